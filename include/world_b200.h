@@ -1,0 +1,198 @@
+/*
+ * world_b200.h -- C ABI of libworld_b200.so, the B200 (sm_100a) DEM step.
+ *
+ * The reference exposes its step only as the C++ class ParticleDynamics
+ * (src/particle_dynamics.h:17-141), statically linked into every driver, plus the
+ * YAML loader load_config (src/sim_config.h:202-205). This header is the drop-in
+ * boundary for that path: plain C types, no exceptions, every call returns an int
+ * status (0 = ok, > 0 = ok with a warning, < 0 = error; wd_last_error() has the
+ * message). One handle per host thread; each handle owns its CUDA stream and its
+ * device buffers. The C++ class mirroring ParticleDynamics member for member is in
+ * include/world_b200/particle_dynamics.hpp; Python reaches the same calls through
+ * ctypes (world_b200/_lib.py).
+ *
+ * Arrays crossing this boundary use the reference's layouts:
+ *   state      float[6n]  AoS [x y z vx vy vz] per grain (src/sim_config.h:14-15)
+ *   positions  float[3n]  AoS [x y z]          (src/particle_dynamics.h:34-37)
+ *   rhs        float[6n]  AoS [v, F/m]          (src/compute_rhs_kernel.cu:207-210)
+ *   grid       float[4*nodes] channel-major [m, m vx, m vy, m vz], node =
+ *              (ix*ny + iy)*nz + iz             (src/density_grid_kernel.h:18-24)
+ * all indexed by the caller's grain id, whatever order the device keeps them in.
+ */
+#ifndef WORLD_B200_H
+#define WORLD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define WD_OK 0
+#define WD_WARN_DEFAULTS 1     /* config file missing: defaults kept (src/sim_config.cpp:157-161) */
+#define WD_WARN_UNKNOWN_KEY 2  /* unknown key ignored (src/sim_config.cpp:47-50) */
+#define WD_ERR_INVALID (-1)    /* bad argument */
+#define WD_ERR_CUDA (-2)       /* CUDA runtime error (the reference aborts: src/cuda_check.h:7-12) */
+#define WD_ERR_IO (-3)         /* state file unreadable or short (the reference exits: src/particle_dynamics.cu:213-229) */
+#define WD_ERR_CONFIG (-4)     /* value that does not parse (the reference throws from std::stof) */
+#define WD_ERR_OOM (-5)        /* device allocation failed */
+#define WD_ERR_CAPACITY (-6)   /* a caller buffer or a fixed capacity is too small */
+
+/* Tangential-history capacity per grain (pair plus wall contacts). */
+#define WD_HIST_CAP 24
+
+typedef struct wd_config wd_config;
+typedef struct wd_sim wd_sim;
+
+/* Message of the last failing call on this thread (never NULL). */
+const char* wd_last_error(void);
+
+/* Library version string. */
+const char* wd_version(void);
+
+/* ---- configuration: SimConfig + load_config (src/sim_config.h:64-205) ----------- */
+
+/* New config holding the reference's built-in defaults (src/sim_config.h:68-199). */
+int wd_config_create(wd_config** out);
+int wd_config_destroy(wd_config* cfg);
+int wd_config_copy(const wd_config* src, wd_config** out);
+
+/* Apply a YAML file on top of cfg with load_config's semantics
+ * (src/sim_config.cpp:153-195): "section:" headers, "key: value", "[a, b]" lists, "#"
+ * comments; unknown keys warn; a missing file warns and keeps cfg. */
+int wd_config_load_yaml(wd_config* cfg, const char* path);
+
+/* Set one "section.key" from its text form, exactly as a YAML line would
+ * (src/sim_config.cpp:54-149). Returns WD_WARN_UNKNOWN_KEY for unknown keys. */
+int wd_config_set(wd_config* cfg, const char* section, const char* key, const char* value);
+
+/* Read one "section.key" back as text (floats as %.9g, lists as "[a, b]"). */
+int wd_config_get(const wd_config* cfg, const char* section, const char* key, char* buf,
+                  size_t buf_len);
+
+/* Host-only: the initial grains cfg's initialization section describes
+ * (initialize_to_cube / two_particles / single_particle / from_file,
+ * src/particle_dynamics.cu:128-235). *n receives the grain count; state (6n) and
+ * material (n) are written only when n <= capacity. No device is touched. */
+int wd_initial_state(const wd_config* cfg, float* state, int32_t* material, int64_t capacity,
+                     int64_t* n);
+
+/* ---- construction: ParticleDynamics(const SimConfig&) (src/particle_dynamics.cu:10-94) */
+
+/* Build the initial state from cfg's initialization section (cube, two_particles,
+ * single_particle or file: src/particle_dynamics.cu:22-30,165-235) and upload it. */
+int wd_create(const wd_config* cfg, wd_sim** out);
+
+/* Build from caller arrays (length n): state AoS6; material ids (NULL: the config's
+ * particle_material); radius (NULL: physics.particle_radius); mass (NULL: from
+ * physics.density when set, else the material table). */
+int wd_create_from_arrays(const wd_config* cfg, int64_t n, const float* state,
+                          const int32_t* material, const float* radius, const float* mass,
+                          wd_sim** out);
+
+int wd_destroy(wd_sim* sim);
+
+/* ---- stepping: take_step() (src/particle_dynamics.cu:264-281) -------------------- */
+
+/* nsteps x take_step(), launched asynchronously on the handle's stream. */
+int wd_step(wd_sim* sim, int64_t nsteps);
+
+/* dt is re-read at every step, as the reference re-applies sim.dt
+ * (src/particle_dynamics.cu:268,276). */
+int wd_set_dt(wd_sim* sim, float dt);
+int wd_get_dt(const wd_sim* sim, float* dt);
+/* Simulated time, float, advanced by dt per step (src/particle_dynamics.cu:280). */
+int wd_get_time(const wd_sim* sim, float* time);
+int wd_set_time(wd_sim* sim, float time);
+int wd_get_n(const wd_sim* sim, int64_t* n);
+/* Picard iterations run in the last step and its final residual max|x_{k+1}-x_k|. */
+int wd_get_picard_stats(const wd_sim* sim, int32_t* iterations, float* residual);
+
+/* ---- state in and out: host_state / device_state / positions / device_rhs -------- */
+
+/* device_state.copy_from_host(host_state) (src/device_vector.h:30-49): state AoS6. */
+int wd_set_state(wd_sim* sim, const float* state);
+/* host_state.copy_from_device(device_state): state AoS6 by grain id. */
+int wd_get_state(wd_sim* sim, float* state);
+/* unpack_state() positions (src/particle_dynamics.cu:109-124): AoS3 by grain id. */
+int wd_get_positions(wd_sim* sim, float* positions);
+/* device_rhs of the last step (src/particle_dynamics.h:42): AoS6 [v, F/m]. */
+int wd_get_rhs(wd_sim* sim, float* rhs);
+/* host_mass / host_material per grain, and per-grain radius. */
+int wd_get_grain_props(const wd_sim* sim, float* radius, float* mass, int32_t* material);
+
+/* Device-pointer variants for zero-copy callers (PyTorch): the same layouts, in
+ * device memory, ordered on the handle's stream. */
+int wd_set_state_device(wd_sim* sim, const float* d_state);
+int wd_get_state_device(wd_sim* sim, float* d_state);
+int wd_get_positions_device(wd_sim* sim, float* d_positions);
+/* Use an external stream (cudaStream_t as void*); NULL restores the own stream. */
+int wd_set_stream(wd_sim* sim, void* stream);
+int wd_get_stream(const wd_sim* sim, void** stream);
+/* Block until all work queued on the handle's stream is done. */
+int wd_synchronize(wd_sim* sim);
+
+/* ---- tangential history (extension: no reference counterpart) ------------------- */
+
+/* Per grain id: count[n], partner[n*WD_HIST_CAP] (grain id, or -1-2a / -2-2a for the
+ * lower / upper wall of axis a), xi[n*WD_HIST_CAP*3] tangential displacement. */
+int wd_get_history(wd_sim* sim, int32_t* count, int32_t* partner, float* xi);
+int wd_set_history(wd_sim* sim, const int32_t* count, const int32_t* partner,
+                   const float* xi);
+
+/* ---- on-demand fields: compute_density_grid / compute_total_energy -------------- */
+
+/* density_grid_nodes() (src/particle_dynamics.cu:283-286). */
+int wd_density_grid_nodes(const wd_sim* sim, int64_t* nodes);
+/* compute_density_grid() (src/particle_dynamics.cu:289-293): writes 4*nodes floats
+ * to grid (host). Deterministic: order-independent fixed-point accumulation. */
+int wd_compute_density_grid(wd_sim* sim, float* grid);
+int wd_compute_density_grid_device(wd_sim* sim, float* d_grid);
+/* compute_total_energy() (src/particle_dynamics.cu:296-308), summed in FP64. Like
+ * the reference it re-runs the neighbor search on the current positions first. */
+int wd_compute_total_energy(wd_sim* sim, double* energy);
+/* Total momentum sum(m v) in FP64 (extension). */
+int wd_compute_momentum(wd_sim* sim, double* momentum3);
+
+/* ---- diagnostics (src/particle_dynamics.cu:311-347) ------------------------------ */
+
+/* is_stable(): every position finite and inside the domain box. */
+int wd_is_stable(wd_sim* sim, int32_t* stable);
+/* compute_max_acceleration(): max |F/m| of the last step's rhs. */
+int wd_compute_max_acceleration(wd_sim* sim, float* max_accel);
+/* grid_overflow_count(): lifetime count of (cell, search) incidents with more than
+ * particles_per_cell grains in a cell (src/find_neighbors_kernel.cu:230-234). No
+ * grain is dropped here: the sorted search has no per-cell capacity. */
+int wd_grid_overflow_count(wd_sim* sim, int64_t* count);
+/* Lifetime count of contacts that found no free history slot (WD_HIST_CAP). */
+int wd_history_overflow_count(wd_sim* sim, int64_t* count);
+/* find_neighbors_wct / compute_rhs_wct / take_step_wct / density_grid_wct
+ * (src/particle_dynamics.cu:350-358): lifetime ms, recorded when
+ * drivers.kernel_timing is true. The contact kernel integrates in its epilogue, so
+ * take_step_wct stays 0 and compute_rhs_wct covers forces plus integration. */
+int wd_timings(wd_sim* sim, float* ms4);
+/* Number of kernels one step launches (for launch accounting). */
+int wd_kernels_per_step(const wd_sim* sim, int64_t* kernels);
+
+/* ---- parity probes: the reference's public device_neighbors buffer
+ * (src/particle_dynamics.h:48-52) and its cell mapping -------------------------- */
+
+/* Cell key of every grain at the current positions, by grain id
+ * (src/find_neighbors_kernel.cu:11-40). */
+int wd_debug_cell_keys(wd_sim* sim, int32_t* keys);
+/* The sorted order of the last neighbor search: cell key and grain id per slot,
+ * ascending by (key, id). */
+int wd_debug_sorted(wd_sim* sim, int32_t* keys, int32_t* ids);
+/* Candidate lists at the current positions, CSR by grain id: offsets[n+1];
+ * cand[offsets[i]..offsets[i+1]) in stencil order, ids ascending inside a cell;
+ * contact[k] = 1 when that pair overlaps. *total receives the candidate count;
+ * cand/contact are written only when it fits in cap. */
+int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* contact,
+                        int64_t cap, int64_t* total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,265 @@
+// wd_device.cuh -- parameters and per-contact arithmetic shared by the sm_100a kernels.
+//
+// The library is compiled with -fmad=false: the only fused multiply-adds are the
+// explicit fmaf() calls below, placed where nvcc contracts the reference's own
+// expressions (e.g. `force[a] += f_pair * normal[a]`). Division and sqrt are the
+// IEEE-rounded ones (-prec-div, -prec-sqrt), so a CPU restatement with the same
+// operation order reproduces these kernels bit for bit.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace wd {
+
+constexpr int kHistCap = 24;          // tangential-history slots per grain
+constexpr uint32_t kNoKey = 0xFFFFFFFFu;
+
+// Lifetime counters kept on the device.
+enum Counter : int {
+    kCntGridOverflow = 0,   // (cell, search) incidents above particles_per_cell
+    kCntHistOverflow = 1,   // contacts without a free history slot
+    kCntUnstable = 2,       // scratch for is_stable
+    kCntMaxAccel = 3,       // scratch for compute_max_acceleration (float bits)
+    kNumCounters = 8,
+};
+
+// Everything a step kernel needs, passed by value (baked into the captured graph).
+struct DevParams {
+    float lo[3], hi[3];        // domain box
+    int grid[3];               // collision grid
+    int ppc;                   // particles_per_cell
+    float gravity;
+    float max_force;           // clamp (+inf: none)
+    float k_n, k_t;
+    float restitution, ln_e, damp_den;
+    float mu;
+    float dt;
+    float wall_lo[3], wall_hi[3];
+    float clamp_overlap;
+    float picard_tol;
+    int history;
+    int n;
+};
+
+// reference src/find_neighbors_kernel.cu:11-22. __float2int_rz is cvt.rzi.s32.f32,
+// the conversion static_cast<int>(float) compiles to.
+__device__ __forceinline__ int cell_axis(float x, float lo, float hi, int g) {
+    const float t = (x - lo) / (hi - lo) * static_cast<float>(g);
+    return min(g - 1, max(0, __float2int_rz(t)));
+}
+
+__device__ __forceinline__ void cell_coords(const DevParams& P, float x, float y, float z,
+                                            int& cx, int& cy, int& cz) {
+    cx = cell_axis(x, P.lo[0], P.hi[0], P.grid[0]);
+    cy = cell_axis(y, P.lo[1], P.hi[1], P.grid[1]);
+    cz = cell_axis(z, P.lo[2], P.hi[2], P.grid[2]);
+}
+
+// reference src/find_neighbors_kernel.cu:27-30 (x slowest, z fastest).
+__device__ __forceinline__ uint32_t flat_cell(const DevParams& P, int x, int y, int z) {
+    return (static_cast<uint32_t>(x) * static_cast<uint32_t>(P.grid[1]) +
+            static_cast<uint32_t>(y)) * static_cast<uint32_t>(P.grid[2]) +
+           static_cast<uint32_t>(z);
+}
+
+// reference src/compute_rhs_kernel.cu:41-47 with logf(e) and the denominator
+// sqrtf(pi^2 + ln^2 e) computed once on the host.
+__device__ __forceinline__ float damping(const DevParams& P, float m) {
+    if (P.restitution <= 0.f) return 2.f * sqrtf(P.k_n * m);
+    if (P.restitution >= 1.f) return 0.f;
+    return ((-2.f * sqrtf(m * P.k_n)) * P.ln_e) / P.damp_den;
+}
+
+// reference src/compute_rhs_kernel.cu:66-78
+__device__ __forceinline__ void viscous_friction(float3& f, float3 vt, float limit, float c) {
+    float vt_sq = vt.x * vt.x;
+    vt_sq = fmaf(vt.y, vt.y, vt_sq);
+    vt_sq = fmaf(vt.z, vt.z, vt_sq);
+    const float v = sqrtf(vt_sq);
+    if (v < 1e-8f) return;
+    const float mag = fminf(limit, c * v);
+    f.x = f.x - (mag * vt.x) / v;
+    f.y = f.y - (mag * vt.y) / v;
+    f.z = f.z - (mag * vt.z) / v;
+}
+
+// Tangential spring with per-pair history (Cundall-Strack), capped at mu |F_n| with
+// the spring reset to the cap on slip. The stored displacement is rotated onto the
+// current tangent plane, advanced by v_t dt, and F_t = -k_t xi. Extension: the
+// reference's friction is the viscous form above.
+struct HistRow {
+    const float4* in;   // old row of this grain (kHistCap entries)
+    int in_count;
+    float4* out;        // new row
+    int out_count;
+};
+
+__device__ __forceinline__ void spring_friction(const DevParams& P, float3& f, float3 vt,
+                                                float3 nrm, float limit, int partner,
+                                                HistRow& h, unsigned long long* counters) {
+    float3 xi = make_float3(0.f, 0.f, 0.f);
+    for (int k = 0; k < h.in_count; ++k) {
+        const float4 e = h.in[k];
+        if (__float_as_int(e.w) == partner) {
+            xi = make_float3(e.x, e.y, e.z);
+            break;
+        }
+    }
+    float xn = xi.x * nrm.x;
+    xn = fmaf(xi.y, nrm.y, xn);
+    xn = fmaf(xi.z, nrm.z, xn);
+    xi.x = fmaf(-xn, nrm.x, xi.x);
+    xi.y = fmaf(-xn, nrm.y, xi.y);
+    xi.z = fmaf(-xn, nrm.z, xi.z);
+    xi.x = fmaf(P.dt, vt.x, xi.x);
+    xi.y = fmaf(P.dt, vt.y, xi.y);
+    xi.z = fmaf(P.dt, vt.z, xi.z);
+    float3 ft = make_float3(-P.k_t * xi.x, -P.k_t * xi.y, -P.k_t * xi.z);
+    float ft_sq = ft.x * ft.x;
+    ft_sq = fmaf(ft.y, ft.y, ft_sq);
+    ft_sq = fmaf(ft.z, ft.z, ft_sq);
+    if (ft_sq > limit * limit) {
+        const float s = limit / sqrtf(ft_sq);
+        ft.x = ft.x * s; ft.y = ft.y * s; ft.z = ft.z * s;
+        xi.x = xi.x * s; xi.y = xi.y * s; xi.z = xi.z * s;
+    }
+    f.x = f.x + ft.x;
+    f.y = f.y + ft.y;
+    f.z = f.z + ft.z;
+    if (h.out_count < kHistCap) {
+        h.out[h.out_count] = make_float4(xi.x, xi.y, xi.z, __int_as_float(partner));
+        ++h.out_count;
+    } else {
+        atomicAdd(&counters[kCntHistOverflow], 1ull);
+    }
+}
+
+// Gravity and the six walls: reference src/compute_rhs_kernel.cu:114-146.
+template <bool HIST>
+__device__ __forceinline__ void wall_forces(const DevParams& P, float3 pos, float3 vel,
+                                            float ri, float mi, float3& f, HistRow& h,
+                                            unsigned long long* counters) {
+    const float k = P.k_n, F = P.max_force;
+    const float c_wall = damping(P, mi);
+    f.z = fmaf(-mi, P.gravity, f.z);
+    const float p3[3] = {pos.x, pos.y, pos.z};
+    const float v3[3] = {vel.x, vel.y, vel.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float3 vt = make_float3(a == 0 ? 0.f : vel.x, a == 1 ? 0.f : vel.y,
+                                      a == 2 ? 0.f : vel.z);
+        float fa = a == 0 ? f.x : (a == 1 ? f.y : f.z);
+        const float dl = (p3[a] - P.wall_lo[a]) - ri;
+        const float fl = fmaxf(0.f, fminf(F, -k * dl));
+        fa = fa + fl;
+        if (a == 0) f.x = fa; else if (a == 1) f.y = fa; else f.z = fa;
+        if (dl < 0.f) {
+            fa = fmaf(-c_wall, v3[a], fa);
+            if (a == 0) f.x = fa; else if (a == 1) f.y = fa; else f.z = fa;
+            if (HIST) {
+                const float3 nrm = make_float3(a == 0 ? 1.f : 0.f, a == 1 ? 1.f : 0.f,
+                                               a == 2 ? 1.f : 0.f);
+                spring_friction(P, f, vt, nrm, P.mu * fl, -1 - 2 * a, h, counters);
+            } else {
+                viscous_friction(f, vt, P.mu * fl, c_wall);
+            }
+        }
+        fa = a == 0 ? f.x : (a == 1 ? f.y : f.z);
+        const float du = (P.wall_hi[a] - p3[a]) - ri;
+        const float fu = fmaxf(0.f, fminf(F, -k * du));
+        fa = fa - fu;
+        if (a == 0) f.x = fa; else if (a == 1) f.y = fa; else f.z = fa;
+        if (du < 0.f) {
+            fa = fmaf(-c_wall, v3[a], fa);
+            if (a == 0) f.x = fa; else if (a == 1) f.y = fa; else f.z = fa;
+            if (HIST) {
+                const float3 nrm = make_float3(a == 0 ? -1.f : 0.f, a == 1 ? -1.f : 0.f,
+                                               a == 2 ? -1.f : 0.f);
+                spring_friction(P, f, vt, nrm, P.mu * fu, -2 - 2 * a, h, counters);
+            } else {
+                viscous_friction(f, vt, P.mu * fu, c_wall);
+            }
+        }
+    }
+}
+
+// Squared centre distance, accumulated as the reference's loop contracts it.
+__device__ __forceinline__ float pair_norm_sq(float4 pi, float4 pj, float3& d) {
+    d = make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z);
+    float ns = d.x * d.x;
+    ns = fmaf(d.y, d.y, ns);
+    ns = fmaf(d.z, d.z, ns);
+    return ns;
+}
+
+// dist = |delta| - r_i - r_j with the larger radius subtracted first: symmetric in
+// (i, j) and equal to the reference's norm - radius - radius for equal radii.
+__device__ __forceinline__ float pair_dist(float norm, float ri, float rj) {
+    const float rmax = fmaxf(ri, rj), rmin = fminf(ri, rj);
+    return (norm - rmax) - rmin;
+}
+
+// Conservative early-out: ns above this can never give dist < 0.
+__device__ __forceinline__ bool maybe_contact(float ns, float ri, float rj) {
+    const float rs = ri + rj;
+    return ns <= rs * rs * 1.001f;
+}
+
+// One pair contact: reference src/compute_rhs_kernel.cu:150-204 (dist < 0 branch).
+template <bool HIST>
+__device__ __forceinline__ void pair_force(const DevParams& P, float3 d, float norm,
+                                           float dist, float3 vel, float mi, float4 vj,
+                                           int partner, float3& f, HistRow& h,
+                                           unsigned long long* counters) {
+    const float3 nrm = make_float3(d.x / norm, d.y / norm, d.z / norm);
+    const float fp = fmaxf(0.f, fminf(P.max_force, -P.k_n * dist));
+    f.x = fmaf(fp, nrm.x, f.x);
+    f.y = fmaf(fp, nrm.y, f.y);
+    f.z = fmaf(fp, nrm.z, f.z);
+    const float mj = vj.w;
+    const float msum = mi + mj;
+    const float mred = (msum > 0.f) ? (mi * mj) / msum : 0.f;
+    const float c = damping(P, mred);
+    const float3 vr = make_float3(vel.x - vj.x, vel.y - vj.y, vel.z - vj.z);
+    float vn = vr.x * nrm.x;
+    vn = fmaf(vr.y, nrm.y, vn);
+    vn = fmaf(vr.z, nrm.z, vn);
+    const float cvn = c * vn;
+    f.x = fmaf(-cvn, nrm.x, f.x);
+    f.y = fmaf(-cvn, nrm.y, f.y);
+    f.z = fmaf(-cvn, nrm.z, f.z);
+    const float3 vt = make_float3(fmaf(-vn, nrm.x, vr.x), fmaf(-vn, nrm.y, vr.y),
+                                  fmaf(-vn, nrm.z, vr.z));
+    if (HIST) {
+        spring_friction(P, f, vt, nrm, P.mu * fp, partner, h, counters);
+    } else {
+        viscous_friction(f, vt, P.mu * fp, c);
+    }
+}
+
+// reference src/energy_kernel.cu:22-27, clamp point generalised to F/k_n.
+__device__ __forceinline__ float contact_energy(float delta, float clamp_d, float F, float k) {
+    if (delta <= 0.f) return 0.f;
+    if (delta <= clamp_d) return 0.5f * k * delta * delta;
+    return 0.5f * F * clamp_d + F * (delta - clamp_d);
+}
+
+// Range of sorted slots covering cells (x, y, z-1 .. z+1): the three runs are
+// consecutive in (key, id) order, so one [lo, hi) spans them in stencil order.
+__device__ __forceinline__ void column_range(const DevParams& P, const int2* __restrict__ table,
+                                             int nx, int ny, int cz, int& lo, int& hi) {
+    const int zlo = max(cz - 1, 0), zhi = min(cz + 1, P.grid[2] - 1);
+    const uint32_t base = flat_cell(P, nx, ny, 0);
+    lo = 0x7fffffff;
+    hi = 0;
+    for (int z = zlo; z <= zhi; ++z) {
+        const int2 e = __ldg(&table[base + static_cast<uint32_t>(z)]);
+        if (e.x >= 0) {
+            lo = min(lo, e.x);
+            hi = max(hi, e.y);
+        }
+    }
+}
+
+}  // namespace wd

@@ -1,0 +1,113 @@
+// wd_kernels.h -- host-side launchers of the sm_100a kernels (wd_search.cu,
+// wd_contact.cu, wd_fields.cu). All launches are asynchronous on the given stream.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "wd_device.cuh"
+
+namespace wd {
+
+constexpr int kBlock = 256;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kBlock * kSortItems;  // keys per radix-sort tile
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+
+inline int blocks_for(int64_t n, int block = kBlock) {
+    return static_cast<int>((n + block - 1) / block);
+}
+
+// Buffers of one neighbor search (sorted by (cell key, grain id)).
+struct SearchBuffers {
+    uint32_t* key_by_id;     // n: cell key of grain id
+    int* slot_of_id;         // n: slot of grain id in the source state arrays
+    uint32_t* keys[2];       // n: radix ping-pong
+    uint32_t* vals[2];       // n
+    uint32_t* key_sorted;    // n: sorted keys of the last search (table bookkeeping)
+    uint32_t* tile_counts;   // kRadix * num_tiles
+    uint32_t* digit_totals;  // kRadix * max_passes
+    int2* table;             // num_cells: [start, end) of each occupied cell
+    int num_tiles;
+    int passes;              // radix passes for the key width
+};
+
+// Picard early exit: kernels return at once when prev_res != nullptr and
+// *prev_res (float bits) < tol. tol <= 0 never skips.
+struct Skip {
+    const uint32_t* prev_res;
+    float tol;
+};
+
+// keys + radix sort + run table. Leaves sorted keys / ids in
+// keys[out_buf] / vals[out_buf], returns out_buf.
+int launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
+                  Skip skip, uint32_t* zero_res, int zero_res_count, cudaStream_t st);
+
+// Gather the source state into sorted order (and the Picard snapshot when given),
+// counting cells above capacity.
+void launch_gather(const DevParams& P, const SearchBuffers& sb, int out_buf,
+                   const float4* posA, const float4* velA, float4* posB, float4* velB,
+                   int* idsB, const float4* nposA, const float4* nvelA, float4* nposB,
+                   float4* nvelB, bool snap_from_state, unsigned long long* counters,
+                   Skip skip, cudaStream_t st);
+
+struct ForceArgs {
+    const float4* pos; const float4* vel; const int* ids;  // sorted step input
+    const int2* table;
+    float4* pos_out; float4* vel_out; int* ids_out;        // integrated state
+    float4* acc_out;                                       // F/m per slot
+    const float4* npos; const float4* nvel;                // Picard x^n, v^n
+    const float4* hist_in; const int* hcnt_in;             // committed history
+    float4* hist_out; int* hcnt_out;                       // new history
+    unsigned long long* counters;
+    uint32_t* res_slot;                                    // Picard residual (bits)
+    int* picard_used;
+    int iter;
+};
+
+void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip,
+                  cudaStream_t st);
+
+// Total energy at the sorted state (after a search): per-block FP64 partials, then
+// a fixed-order final sum into out.
+void launch_energy(const DevParams& P, const float4* pos, const float4* vel, const int* ids,
+                   const int2* table, const float4* hist, const int* hcnt, double* partials,
+                   double* out, cudaStream_t st);
+
+// Candidate probes (CSR by grain id).
+void launch_candidate_count(const DevParams& P, const float4* pos, const int* ids,
+                            const int2* table, int* count_by_id, cudaStream_t st);
+void launch_candidate_fill(const DevParams& P, const float4* pos, const int* ids,
+                           const int2* table, const int64_t* offsets_by_id, int* cand,
+                           uint8_t* contact, cudaStream_t st);
+
+// State conversion between the sorted SoA and the caller's AoS-by-id layouts.
+void launch_state_to_aos(int n, const float4* pos, const float4* vel, const int* ids,
+                         float* out6, cudaStream_t st);
+void launch_positions_to_aos(int n, const float4* pos, const int* ids, float* out3,
+                             cudaStream_t st);
+void launch_rhs_to_aos(int n, const float4* vel_used, const float4* acc, const int* ids,
+                       float* out6, cudaStream_t st);
+void launch_state_from_aos(int n, const float* in6, float4* pos, float4* vel, const int* ids,
+                           cudaStream_t st);
+void launch_cell_keys_by_id(const DevParams& P, const float4* pos, const int* ids,
+                            int32_t* keys, cudaStream_t st);
+
+// CIC deposit: deterministic fixed-point accumulation (see wd_fields.cu).
+void launch_deposit(int n, const float4* pos, const float4* vel, const float* lo,
+                    const float* hi, const int* dgrid, uint32_t* bounds,
+                    unsigned long long* acc, float* out, cudaStream_t st);
+
+// Reductions.
+void launch_momentum(int n, const float4* vel, double* partials, double* out3,
+                     cudaStream_t st);
+void launch_max_accel(int n, const float4* acc, unsigned long long* counters,
+                      cudaStream_t st);
+void launch_stability(const DevParams& P, const float4* pos, unsigned long long* counters,
+                      cudaStream_t st);
+
+int reduction_blocks(int n);
+
+}  // namespace wd

@@ -1,0 +1,445 @@
+// wd_search.cu -- neighbor search for sm_100a: cell keys, stable LSD radix sort of
+// (cell key, grain id), run table, gather into sorted SoA.
+//
+// Replaces the reference's four-pass dense bucketing (src/find_neighbors_kernel.cu:
+// 46-161: atomicCAS marks, atomicAdd compaction, atomicAdd slot fill, flat candidate
+// rows of 27*particles_per_cell ints). Here:
+//   * the key of every grain is computed with the reference's cell mapping and
+//     written by grain id, so the sort input is in id order and a stable LSD sort
+//     yields (key, id) order: deterministic, no per-cell capacity, nothing dropped;
+//   * the run table is a dense [start, end) per cell, but only the cells of the
+//     previous search are cleared (O(n), not the reference's O(cells) memset);
+//   * no candidate list is materialised: the contact kernel walks the sorted runs.
+#include <cstdio>
+
+#include "wd_kernels.h"
+
+namespace wd {
+
+namespace {
+
+__device__ __forceinline__ bool skipped(const Skip& s) {
+    return s.prev_res != nullptr && s.tol > 0.f && __uint_as_float(*s.prev_res) < s.tol;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Pass 0 of a search: key of every grain by id, slot of every id, clear the runs
+// of the previous search, zero the per-pass digit totals.
+__global__ void __launch_bounds__(kBlock)
+k_keys(DevParams P, const float4* __restrict__ pos, const int* __restrict__ ids,
+       uint32_t* __restrict__ key_by_id, int* __restrict__ slot_of_id,
+       const uint32_t* __restrict__ key_sorted, int2* __restrict__ table,
+       uint32_t* __restrict__ digit_totals, int totals_count, uint32_t* __restrict__ zero_res,
+       int zero_res_count, Skip skip) {
+    if (skipped(skip)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < totals_count) digit_totals[s] = 0u;
+    if (zero_res != nullptr && s < zero_res_count) zero_res[s] = 0u;
+    if (s >= P.n) return;
+    const float4 p = pos[s];
+    int cx, cy, cz;
+    cell_coords(P, p.x, p.y, p.z, cx, cy, cz);
+    const int i = ids[s];
+    key_by_id[i] = flat_cell(P, cx, cy, cz);
+    slot_of_id[i] = s;
+    const uint32_t kp = key_sorted[s];
+    if (kp != kNoKey && (s == 0 || key_sorted[s - 1] != kp)) table[kp] = make_int2(-1, -1);
+}
+
+// Radix pass, step 1: digit histogram of one tile (warp-aggregated shared atomics:
+// nearly sorted input puts most keys of a tile on one digit).
+__global__ void __launch_bounds__(kBlock)
+k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift, int num_tiles,
+            uint32_t* __restrict__ counts, uint32_t* __restrict__ totals, Skip skip) {
+    if (skipped(skip)) return;
+    __shared__ uint32_t h[kRadix];
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) h[d] = 0u;
+    __syncthreads();
+    const int base = blockIdx.x * kSortTile;
+    const unsigned lane_lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const int idx = base + k * kBlock + threadIdx.x;
+        const bool valid = idx < n;
+        const uint32_t d = valid ? (keys[idx] >> shift) & (kRadix - 1) : kRadix;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (valid && (peers & lane_lt) == 0u) atomicAdd(&h[d], static_cast<uint32_t>(__popc(peers)));
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+        const uint32_t c = h[d];
+        counts[static_cast<size_t>(d) * num_tiles + blockIdx.x] = c;
+        if (c) atomicAdd(&totals[d], c);
+    }
+}
+
+// Block-wide exclusive scan of one value per thread (256 threads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t warp_sums[kBlock / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kBlock / 32 ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < kBlock / 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kBlock / 32) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = (warp > 0 ? warp_sums[warp - 1] : 0u) + x - v;
+    if (total) *total = warp_sums[kBlock / 32 - 1];
+    __syncthreads();
+    return before;
+}
+
+// Radix pass, step 2: one block per digit turns that digit's per-tile counts into
+// global output offsets (digit base + exclusive scan over tiles).
+__global__ void __launch_bounds__(kBlock)
+k_sort_scan(uint32_t* __restrict__ counts, const uint32_t* __restrict__ totals, int num_tiles,
+            Skip skip) {
+    if (skipped(skip)) return;
+    const int d = blockIdx.x;
+    uint32_t part = 0u;
+    for (int t = threadIdx.x; t < d; t += blockDim.x) part += totals[t];
+    uint32_t base = 0u;
+    block_exclusive_scan(part, &base);
+    uint32_t* col = counts + static_cast<size_t>(d) * num_tiles;
+    const int chunk = (num_tiles + kBlock - 1) / kBlock;
+    const int t0 = threadIdx.x * chunk;
+    uint32_t sum = 0u;
+    for (int t = t0; t < min(t0 + chunk, num_tiles); ++t) sum += col[t];
+    uint32_t run = base + block_exclusive_scan(sum, nullptr);
+    for (int t = t0; t < min(t0 + chunk, num_tiles); ++t) {
+        const uint32_t c = col[t];
+        col[t] = run;
+        run += c;
+    }
+}
+
+// Radix pass, step 3: stable scatter. Each warp ranks its 256 consecutive keys in 8
+// rounds of 32 with __match_any_sync; warps are then offset by the per-digit counts
+// of the warps before them, and the tile by its scanned global offset.
+template <bool IOTA>
+__global__ void __launch_bounds__(kBlock)
+k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+               uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n,
+               int shift, int num_tiles, const uint32_t* __restrict__ offsets, Skip skip) {
+    if (skipped(skip)) return;
+    constexpr int kWarps = kBlock / 32;
+    __shared__ uint32_t wh[kWarps][kRadix];
+    __shared__ uint32_t toff[kRadix];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+        toff[d] = offsets[static_cast<size_t>(d) * num_tiles + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) wh[w][d] = 0u;
+    }
+    __syncthreads();
+    const unsigned lane_lt = lanemask_lt();
+    const int base = blockIdx.x * kSortTile + warp * (32 * kSortItems);
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int idx = base + r * 32 + lane;
+        const bool valid = idx < n;
+        key[r] = valid ? keys_in[idx] : 0u;
+        val[r] = valid ? (IOTA ? static_cast<uint32_t>(idx) : vals_in[idx]) : 0u;
+        const uint32_t d = valid ? (key[r] >> shift) & (kRadix - 1) : kRadix;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned lt = peers & lane_lt;
+        const uint32_t before = valid ? wh[warp][d] : 0u;
+        __syncwarp();
+        if (valid && lt == 0u) wh[warp][d] = before + static_cast<uint32_t>(__popc(peers));
+        __syncwarp();
+        rank[r] = before + static_cast<uint32_t>(__popc(lt));
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+        uint32_t run = 0u;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = wh[w][d];
+            wh[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int idx = base + r * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (key[r] >> shift) & (kRadix - 1);
+            const uint32_t dst = toff[d] + wh[warp][d] + rank[r];
+            keys_out[dst] = key[r];
+            vals_out[dst] = val[r];
+        }
+    }
+}
+
+// Run table: [start, end) of every occupied cell, from key changes in sorted order.
+__global__ void __launch_bounds__(kBlock)
+k_runs(const uint32_t* __restrict__ skey, uint32_t* __restrict__ key_sorted,
+       int2* __restrict__ table, int n, Skip skip) {
+    if (skipped(skip)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t k = skey[s];
+    key_sorted[s] = k;
+    int* e = reinterpret_cast<int*>(&table[k]);
+    if (s == 0 || skey[s - 1] != k) e[0] = s;
+    if (s == n - 1 || skey[s + 1] != k) e[1] = s + 1;
+}
+
+template <bool SNAP, bool SNAP_FROM_STATE>
+__global__ void __launch_bounds__(kBlock)
+k_gather(int n, int ppc, const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid,
+         const int* __restrict__ slot_of_id, const float4* __restrict__ posA,
+         const float4* __restrict__ velA, float4* __restrict__ posB, float4* __restrict__ velB,
+         int* __restrict__ idsB, const float4* __restrict__ nposA,
+         const float4* __restrict__ nvelA, float4* __restrict__ nposB,
+         float4* __restrict__ nvelB, const int2* __restrict__ table,
+         unsigned long long* __restrict__ counters, Skip skip) {
+    if (skipped(skip)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int i = static_cast<int>(sid[s]);
+    const int p = slot_of_id[i];
+    const float4 x = posA[p], v = velA[p];
+    posB[s] = x;
+    velB[s] = v;
+    idsB[s] = i;
+    if (SNAP) {
+        if (SNAP_FROM_STATE) {
+            nposB[s] = x;
+            nvelB[s] = v;
+        } else {
+            nposB[s] = nposA[p];
+            nvelB[s] = nvelA[p];
+        }
+    }
+    const uint32_t k = skey[s];
+    if (s == 0 || skey[s - 1] != k) {
+        const int len = table[k].y - s;
+        if (len > ppc) atomicAdd(&counters[kCntGridOverflow], 1ull);
+    }
+}
+
+// Candidate probes: same traversal as the contact kernel.
+__global__ void __launch_bounds__(kBlock)
+k_cand_count(DevParams P, const float4* __restrict__ pos, const int* __restrict__ ids,
+             const int2* __restrict__ table, int* __restrict__ count_by_id) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n) return;
+    const float4 pi = pos[s];
+    int cx, cy, cz;
+    cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+    int c = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int nx = cx + dx;
+        if (nx < 0 || nx >= P.grid[0]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int ny = cy + dy;
+            if (ny < 0 || ny >= P.grid[1]) continue;
+            int lo, hi;
+            column_range(P, table, nx, ny, cz, lo, hi);
+            if (hi > lo) c += hi - lo - ((s >= lo && s < hi) ? 1 : 0);
+        }
+    }
+    count_by_id[ids[s]] = c;
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_cand_fill(DevParams P, const float4* __restrict__ pos, const int* __restrict__ ids,
+            const int2* __restrict__ table, const int64_t* __restrict__ offsets,
+            int* __restrict__ cand, uint8_t* __restrict__ contact) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n) return;
+    const float4 pi = pos[s];
+    int cx, cy, cz;
+    cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+    int64_t k = offsets[ids[s]];
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int nx = cx + dx;
+        if (nx < 0 || nx >= P.grid[0]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int ny = cy + dy;
+            if (ny < 0 || ny >= P.grid[1]) continue;
+            int lo, hi;
+            column_range(P, table, nx, ny, cz, lo, hi);
+            for (int j = lo; j < hi; ++j) {
+                if (j == s) continue;
+                const float4 pj = pos[j];
+                float3 d;
+                const float ns = pair_norm_sq(pi, pj, d);
+                const float dist = pair_dist(sqrtf(ns), pi.w, pj.w);
+                cand[k] = ids[j];
+                contact[k] = dist < 0.f ? 1 : 0;
+                ++k;
+            }
+        }
+    }
+}
+
+__global__ void k_state_to_aos(int n, const float4* __restrict__ pos,
+                               const float4* __restrict__ vel, const int* __restrict__ ids,
+                               float* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 x = pos[s], v = vel[s];
+    float* o = out + 6 * static_cast<int64_t>(ids[s]);
+    o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = v.x; o[4] = v.y; o[5] = v.z;
+}
+
+__global__ void k_positions_to_aos(int n, const float4* __restrict__ pos,
+                                   const int* __restrict__ ids, float* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 x = pos[s];
+    float* o = out + 3 * static_cast<int64_t>(ids[s]);
+    o[0] = x.x; o[1] = x.y; o[2] = x.z;
+}
+
+__global__ void k_rhs_to_aos(int n, const float4* __restrict__ vel,
+                             const float4* __restrict__ acc, const int* __restrict__ ids,
+                             float* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 v = vel[s], a = acc[s];
+    float* o = out + 6 * static_cast<int64_t>(ids[s]);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = a.x; o[4] = a.y; o[5] = a.z;
+}
+
+__global__ void k_state_from_aos(int n, const float* __restrict__ in, float4* __restrict__ pos,
+                                 float4* __restrict__ vel, const int* __restrict__ ids) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float* q = in + 6 * static_cast<int64_t>(ids[s]);
+    pos[s] = make_float4(q[0], q[1], q[2], pos[s].w);
+    vel[s] = make_float4(q[3], q[4], q[5], vel[s].w);
+}
+
+__global__ void k_cell_keys_by_id(DevParams P, const float4* __restrict__ pos,
+                                  const int* __restrict__ ids, int32_t* __restrict__ keys) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n) return;
+    const float4 p = pos[s];
+    int cx, cy, cz;
+    cell_coords(P, p.x, p.y, p.z, cx, cy, cz);
+    keys[ids[s]] = static_cast<int32_t>(flat_cell(P, cx, cy, cz));
+}
+
+}  // namespace
+
+int launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
+                  Skip skip, uint32_t* zero_res, int zero_res_count, cudaStream_t st) {
+    const int n = P.n;
+    const int nb = blocks_for(n);
+    const int totals = kRadix * sb.passes;
+    const int kb = blocks_for(n > totals ? n : totals);
+    k_keys<<<kb, kBlock, 0, st>>>(P, pos, ids, sb.key_by_id, sb.slot_of_id, sb.key_sorted,
+                                  sb.table, sb.digit_totals, totals, zero_res, zero_res_count,
+                                  skip);
+    int cur = 0;
+    const uint32_t* kin = sb.key_by_id;
+    const uint32_t* vin = nullptr;
+    for (int pass = 0; pass < sb.passes; ++pass) {
+        const int shift = pass * kRadixBits;
+        uint32_t* totals_p = sb.digit_totals + kRadix * pass;
+        k_sort_hist<<<sb.num_tiles, kBlock, 0, st>>>(kin, n, shift, sb.num_tiles, sb.tile_counts,
+                                                     totals_p, skip);
+        k_sort_scan<<<kRadix, kBlock, 0, st>>>(sb.tile_counts, totals_p, sb.num_tiles, skip);
+        if (pass == 0) {
+            k_sort_scatter<true><<<sb.num_tiles, kBlock, 0, st>>>(
+                kin, vin, sb.keys[cur], sb.vals[cur], n, shift, sb.num_tiles, sb.tile_counts,
+                skip);
+        } else {
+            k_sort_scatter<false><<<sb.num_tiles, kBlock, 0, st>>>(
+                kin, vin, sb.keys[cur], sb.vals[cur], n, shift, sb.num_tiles, sb.tile_counts,
+                skip);
+        }
+        kin = sb.keys[cur];
+        vin = sb.vals[cur];
+        cur ^= 1;
+    }
+    const int out = cur ^ 1;
+    k_runs<<<nb, kBlock, 0, st>>>(sb.keys[out], sb.key_sorted, sb.table, n, skip);
+    return out;
+}
+
+void launch_gather(const DevParams& P, const SearchBuffers& sb, int out_buf,
+                   const float4* posA, const float4* velA, float4* posB, float4* velB,
+                   int* idsB, const float4* nposA, const float4* nvelA, float4* nposB,
+                   float4* nvelB, bool snap_from_state, unsigned long long* counters,
+                   Skip skip, cudaStream_t st) {
+    const int nb = blocks_for(P.n);
+    const uint32_t* skey = sb.keys[out_buf];
+    const uint32_t* sid = sb.vals[out_buf];
+    if (nposB == nullptr) {
+        k_gather<false, false><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.slot_of_id,
+                                                      posA, velA, posB, velB, idsB, nullptr,
+                                                      nullptr, nullptr, nullptr, sb.table,
+                                                      counters, skip);
+    } else if (snap_from_state) {
+        k_gather<true, true><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.slot_of_id, posA,
+                                                    velA, posB, velB, idsB, nullptr, nullptr,
+                                                    nposB, nvelB, sb.table, counters, skip);
+    } else {
+        k_gather<true, false><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.slot_of_id,
+                                                     posA, velA, posB, velB, idsB, nposA,
+                                                     nvelA, nposB, nvelB, sb.table, counters,
+                                                     skip);
+    }
+}
+
+void launch_candidate_count(const DevParams& P, const float4* pos, const int* ids,
+                            const int2* table, int* count_by_id, cudaStream_t st) {
+    k_cand_count<<<blocks_for(P.n), kBlock, 0, st>>>(P, pos, ids, table, count_by_id);
+}
+
+void launch_candidate_fill(const DevParams& P, const float4* pos, const int* ids,
+                           const int2* table, const int64_t* offsets_by_id, int* cand,
+                           uint8_t* contact, cudaStream_t st) {
+    k_cand_fill<<<blocks_for(P.n), kBlock, 0, st>>>(P, pos, ids, table, offsets_by_id, cand,
+                                                    contact);
+}
+
+void launch_state_to_aos(int n, const float4* pos, const float4* vel, const int* ids,
+                         float* out6, cudaStream_t st) {
+    k_state_to_aos<<<blocks_for(n), kBlock, 0, st>>>(n, pos, vel, ids, out6);
+}
+
+void launch_positions_to_aos(int n, const float4* pos, const int* ids, float* out3,
+                             cudaStream_t st) {
+    k_positions_to_aos<<<blocks_for(n), kBlock, 0, st>>>(n, pos, ids, out3);
+}
+
+void launch_rhs_to_aos(int n, const float4* vel_used, const float4* acc, const int* ids,
+                       float* out6, cudaStream_t st) {
+    k_rhs_to_aos<<<blocks_for(n), kBlock, 0, st>>>(n, vel_used, acc, ids, out6);
+}
+
+void launch_state_from_aos(int n, const float* in6, float4* pos, float4* vel, const int* ids,
+                           cudaStream_t st) {
+    k_state_from_aos<<<blocks_for(n), kBlock, 0, st>>>(n, in6, pos, vel, ids);
+}
+
+void launch_cell_keys_by_id(const DevParams& P, const float4* pos, const int* ids,
+                            int32_t* keys, cudaStream_t st) {
+    k_cell_keys_by_id<<<blocks_for(P.n), kBlock, 0, st>>>(P, pos, ids, keys);
+}
+
+}  // namespace wd

@@ -1,0 +1,955 @@
+// wd_sim.cu -- the simulation handle behind the C ABI (include/world_b200.h).
+//
+// Replaces class ParticleDynamics (src/particle_dynamics.h:17-141,
+// src/particle_dynamics.cu:10-358). Differences in mechanism, not in meaning:
+//   * state lives on the device as sorted SoA (float4 x,y,z,r / float4 vx,vy,vz,m /
+//     int id); the caller always sees AoS by grain id;
+//   * a step is one CUDA graph launch on the handle's stream (search, gather,
+//     contact+integrate), instead of eleven launches each followed by
+//     cudaDeviceSynchronize (src/kernel.cu:31-38);
+//   * errors come back as status codes; nothing calls exit() or abort().
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/world_b200.h"
+#include "wd_config.h"
+#include "wd_kernels.h"
+
+namespace wd {
+const char* last_error_cstr();
+}
+
+struct wd_config {
+    wd::Config cfg;
+};
+
+namespace {
+
+using wd::DevParams;
+
+constexpr const char* kVersion = "world_b200 0.1.0 (sm_100a)";
+
+int fail(int code, const std::string& msg) {
+    wd::set_last_error(msg);
+    return code;
+}
+
+#define WD_CUDA(call)                                                                   \
+    do {                                                                                \
+        const cudaError_t e_ = (call);                                                  \
+        if (e_ != cudaSuccess) {                                                        \
+            return fail(e_ == cudaErrorMemoryAllocation ? WD_ERR_OOM : WD_ERR_CUDA,     \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));            \
+        }                                                                               \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+int key_bits(uint64_t cells) {
+    int b = 0;
+    uint64_t v = cells > 0 ? cells - 1 : 0;
+    while (v) {
+        ++b;
+        v >>= 1;
+    }
+    return b;
+}
+
+}  // namespace
+
+struct wd_sim {
+    wd::Config cfg;
+    int n = 0;
+    DevParams P{};
+    float dt = 0.f;
+    float time = 0.f;
+    bool picard = false;
+    int picard_iters = 1;
+
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+
+    // sorted SoA: A = state, B = step gather, C = on-demand gather
+    float4 *posA = nullptr, *velA = nullptr, *posB = nullptr, *velB = nullptr;
+    float4 *posC = nullptr, *velC = nullptr;
+    int *idsA = nullptr, *idsB = nullptr, *idsC = nullptr;
+    float4 *npos[2] = {nullptr, nullptr}, *nvel[2] = {nullptr, nullptr};
+    float4* acc = nullptr;
+    float4* hist[2] = {nullptr, nullptr};
+    int* hcnt[2] = {nullptr, nullptr};
+    int hist_cur = 0;
+
+    wd::SearchBuffers sb{};
+    int search_out = 0;
+    uint64_t num_cells = 0;
+
+    unsigned long long* counters = nullptr;
+    uint32_t* picard_res = nullptr;
+    int* picard_used = nullptr;
+    double* partials = nullptr;
+    double* red_out = nullptr;
+
+    uint32_t* dep_bounds = nullptr;
+    unsigned long long* dep_acc = nullptr;
+    float* dep_out = nullptr;
+    int64_t dep_nodes = 0;
+
+    float* staging = nullptr;   // 6n floats
+    int64_t* cand_offsets = nullptr;
+    int* cand_count = nullptr;
+
+    std::vector<float> radius, mass;
+    std::vector<int32_t> material;
+
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graph_dirty = true;
+    int kernels_per_step = 0;
+
+    // kernel_timing: lifetime ms [search, contact+integrate, integrate, deposit]
+    float wct[4] = {0.f, 0.f, 0.f, 0.f};
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<cudaEvent_t> ev_pending;  // triples: t0, t1, t2 per timed step
+};
+
+namespace {
+
+void destroy_graphs(wd_sim* s) {
+    for (auto& g : s->graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    s->graph_dirty = true;
+}
+
+void free_sim(wd_sim* s) {
+    if (!s) return;
+    destroy_graphs(s);
+    void* bufs[] = {s->posA, s->velA, s->posB, s->velB, s->posC, s->velC, s->idsA, s->idsB,
+                    s->idsC, s->npos[0], s->npos[1], s->nvel[0], s->nvel[1], s->acc,
+                    s->hist[0], s->hist[1], s->hcnt[0], s->hcnt[1], s->sb.key_by_id,
+                    s->sb.slot_of_id, s->sb.keys[0], s->sb.keys[1], s->sb.vals[0],
+                    s->sb.vals[1], s->sb.key_sorted, s->sb.tile_counts, s->sb.digit_totals,
+                    s->sb.table, s->counters, s->picard_res, s->picard_used, s->partials,
+                    s->red_out, s->dep_bounds, s->dep_acc, s->dep_out, s->staging,
+                    s->cand_offsets, s->cand_count};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : s->ev_pending) cudaEventDestroy(e);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    delete s;
+}
+
+// Derived physics constants; the same derivation is restated by the oracle.
+DevParams make_params(const wd::Config& c, int n, float dt) {
+    DevParams P{};
+    for (int a = 0; a < 3; ++a) {
+        P.lo[a] = c.dom_lo[a];
+        P.hi[a] = c.dom_hi[a];
+        P.grid[a] = c.grid[a];
+    }
+    P.ppc = c.particles_per_cell;
+    P.gravity = c.gravity;
+    const bool compat_k = !(c.normal_stiffness > 0.f);
+    P.k_n = compat_k ? c.max_force / c.particle_radius : c.normal_stiffness;
+    P.max_force = (!compat_k && !(c.max_force > 0.f)) ? INFINITY : c.max_force;
+    P.k_t = c.tangential_stiffness > 0.f ? c.tangential_stiffness : (2.f / 7.f) * P.k_n;
+    P.restitution = c.restitution;
+    const float pi = 3.14159265358979323846f;
+    P.ln_e = (c.restitution > 0.f && c.restitution < 1.f) ? logf(c.restitution) : 0.f;
+    P.damp_den = sqrtf(fmaf(P.ln_e, P.ln_e, pi * pi));
+    P.mu = c.friction;
+    P.dt = dt;
+    P.wall_lo[0] = c.wall_x_min; P.wall_lo[1] = c.wall_y_min; P.wall_lo[2] = c.floor_z;
+    P.wall_hi[0] = c.wall_x_max; P.wall_hi[1] = c.wall_y_max; P.wall_hi[2] = c.ceiling_z;
+    P.clamp_overlap = compat_k ? c.particle_radius : P.max_force / P.k_n;
+    P.picard_tol = c.picard_tolerance;
+    P.history = c.history ? 1 : 0;
+    P.n = n;
+    return P;
+}
+
+// One take_step() enqueued on st (captured into the step graph).
+void enqueue_step(wd_sim* s, int parity, cudaStream_t st) {
+    const DevParams& P = s->P;
+    const int hin = parity, hout = parity ^ 1;
+    wd::ForceArgs fa{};
+    fa.pos = s->posB; fa.vel = s->velB; fa.ids = s->idsB; fa.table = s->sb.table;
+    fa.pos_out = s->posA; fa.vel_out = s->velA; fa.ids_out = s->idsA; fa.acc_out = s->acc;
+    fa.hist_in = s->hist[hin]; fa.hcnt_in = s->hcnt[hin];
+    fa.hist_out = s->hist[hout]; fa.hcnt_out = s->hcnt[hout];
+    fa.counters = s->counters;
+    const wd::Skip none{nullptr, 0.f};
+    if (!s->picard) {
+        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, none, nullptr, 0, st);
+        s->search_out = out;
+        wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr,
+                          nullptr, nullptr, nullptr, false, s->counters, none, st);
+        wd::launch_force(P, fa, false, none, st);
+        return;
+    }
+    for (int k = 0; k < s->picard_iters; ++k) {
+        const wd::Skip skip{k == 0 ? nullptr : s->picard_res + (k - 1), P.picard_tol};
+        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, skip,
+                                          k == 0 ? s->picard_res : nullptr, s->picard_iters, st);
+        s->search_out = out;
+        const int nb = k & 1;
+        wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB,
+                          k == 0 ? nullptr : s->npos[nb ^ 1], k == 0 ? nullptr : s->nvel[nb ^ 1],
+                          s->npos[nb], s->nvel[nb], k == 0, s->counters, skip, st);
+        fa.npos = s->npos[nb];
+        fa.nvel = s->nvel[nb];
+        fa.res_slot = s->picard_res + k;
+        fa.picard_used = s->picard_used;
+        fa.iter = k;
+        wd::launch_force(P, fa, true, skip, st);
+    }
+}
+
+int build_graphs(wd_sim* s) {
+    destroy_graphs(s);
+    const int count = s->P.history ? 2 : 1;
+    for (int parity = 0; parity < count; ++parity) {
+        cudaGraph_t g = nullptr;
+        WD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(s, parity, s->stream);
+        WD_CUDA(cudaStreamEndCapture(s->stream, &g));
+        size_t nodes = 0;
+        cudaGraphGetNodes(g, nullptr, &nodes);
+        s->kernels_per_step = static_cast<int>(nodes);
+        const cudaError_t e = cudaGraphInstantiate(&s->graph[parity], g, 0);
+        cudaGraphDestroy(g);
+        WD_CUDA(e);
+    }
+    s->graph_dirty = false;
+    return WD_OK;
+}
+
+int flush_timings(wd_sim* s) {
+    if (s->ev_pending.empty()) return WD_OK;
+    WD_CUDA(cudaEventSynchronize(s->ev_pending.back()));
+    for (size_t i = 0; i + 2 < s->ev_pending.size(); i += 3) {
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, s->ev_pending[i], s->ev_pending[i + 1]);
+        cudaEventElapsedTime(&b, s->ev_pending[i + 1], s->ev_pending[i + 2]);
+        s->wct[0] += a;
+        s->wct[1] += b;
+    }
+    for (cudaEvent_t e : s->ev_pending) s->ev_pool.push_back(e);
+    s->ev_pending.clear();
+    return WD_OK;
+}
+
+cudaEvent_t take_event(wd_sim* s) {
+    if (!s->ev_pool.empty()) {
+        cudaEvent_t e = s->ev_pool.back();
+        s->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Timed step (drivers.kernel_timing): direct launches with events around the
+// search and the contact phase; accumulated lazily, no per-step host sync.
+int timed_step(wd_sim* s, int parity) {
+    if (s->ev_pending.size() >= 3 * 256) {
+        const int rc = flush_timings(s);
+        if (rc) return rc;
+    }
+    const DevParams& P = s->P;
+    cudaStream_t st = s->stream;
+    cudaEvent_t e0 = take_event(s), e1 = take_event(s), e2 = take_event(s);
+    if (!s->picard) {
+        WD_CUDA(cudaEventRecord(e0, st));
+        const wd::Skip none{nullptr, 0.f};
+        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, none, nullptr, 0, st);
+        s->search_out = out;
+        wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr,
+                          nullptr, nullptr, nullptr, false, s->counters, none, st);
+        WD_CUDA(cudaEventRecord(e1, st));
+        wd::ForceArgs fa{};
+        fa.pos = s->posB; fa.vel = s->velB; fa.ids = s->idsB; fa.table = s->sb.table;
+        fa.pos_out = s->posA; fa.vel_out = s->velA; fa.ids_out = s->idsA; fa.acc_out = s->acc;
+        fa.hist_in = s->hist[parity]; fa.hcnt_in = s->hcnt[parity];
+        fa.hist_out = s->hist[parity ^ 1]; fa.hcnt_out = s->hcnt[parity ^ 1];
+        fa.counters = s->counters;
+        wd::launch_force(P, fa, false, none, st);
+        WD_CUDA(cudaEventRecord(e2, st));
+    } else {
+        // Picard interleaves search and force per iteration; time the whole step as
+        // contact work and the search share as zero-length.
+        WD_CUDA(cudaEventRecord(e0, st));
+        WD_CUDA(cudaEventRecord(e1, st));
+        enqueue_step(s, parity, st);
+        WD_CUDA(cudaEventRecord(e2, st));
+    }
+    WD_CUDA(cudaGetLastError());
+    s->ev_pending.push_back(e0);
+    s->ev_pending.push_back(e1);
+    s->ev_pending.push_back(e2);
+    return WD_OK;
+}
+
+// Search on the current state into the C buffers (energy, probes).
+int ondemand_search(wd_sim* s) {
+    if (!s->posC) {
+        WD_CUDA(dalloc(&s->posC, s->n));
+        WD_CUDA(dalloc(&s->velC, s->n));
+        WD_CUDA(dalloc(&s->idsC, s->n));
+    }
+    const wd::Skip none{nullptr, 0.f};
+    const int out = wd::launch_search(s->P, s->posA, s->idsA, s->sb, none, nullptr, 0, s->stream);
+    s->search_out = out;
+    wd::launch_gather(s->P, s->sb, out, s->posA, s->velA, s->posC, s->velC, s->idsC, nullptr,
+                      nullptr, nullptr, nullptr, false, s->counters, none, s->stream);
+    WD_CUDA(cudaGetLastError());
+    return WD_OK;
+}
+
+int sync_stream(wd_sim* s) {
+    WD_CUDA(cudaStreamSynchronize(s->stream));
+    WD_CUDA(cudaGetLastError());
+    return WD_OK;
+}
+
+int alloc_sim(wd_sim* s) {
+    const int n = s->n;
+    WD_CUDA(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+    s->stream = s->own_stream;
+    WD_CUDA(dalloc(&s->posA, n)); WD_CUDA(dalloc(&s->velA, n)); WD_CUDA(dalloc(&s->idsA, n));
+    WD_CUDA(dalloc(&s->posB, n)); WD_CUDA(dalloc(&s->velB, n)); WD_CUDA(dalloc(&s->idsB, n));
+    WD_CUDA(dalloc(&s->acc, n));
+    if (s->picard) {
+        for (int b = 0; b < 2; ++b) {
+            WD_CUDA(dalloc(&s->npos[b], n));
+            WD_CUDA(dalloc(&s->nvel[b], n));
+        }
+    }
+    if (s->P.history) {
+        for (int b = 0; b < 2; ++b) {
+            WD_CUDA(dalloc(&s->hist[b], static_cast<size_t>(n) * wd::kHistCap));
+            WD_CUDA(dalloc(&s->hcnt[b], n));
+            WD_CUDA(cudaMemset(s->hcnt[b], 0, sizeof(int) * static_cast<size_t>(n)));
+        }
+    }
+    wd::SearchBuffers& sb = s->sb;
+    WD_CUDA(dalloc(&sb.key_by_id, n));
+    WD_CUDA(dalloc(&sb.slot_of_id, n));
+    for (int b = 0; b < 2; ++b) {
+        WD_CUDA(dalloc(&sb.keys[b], n));
+        WD_CUDA(dalloc(&sb.vals[b], n));
+    }
+    WD_CUDA(dalloc(&sb.key_sorted, n));
+    WD_CUDA(cudaMemset(sb.key_sorted, 0xFF, sizeof(uint32_t) * static_cast<size_t>(n)));
+    sb.num_tiles = static_cast<int>((static_cast<int64_t>(n) + wd::kSortTile - 1) / wd::kSortTile);
+    const int bits = key_bits(s->num_cells);
+    sb.passes = bits > 0 ? (bits + wd::kRadixBits - 1) / wd::kRadixBits : 1;
+    WD_CUDA(dalloc(&sb.tile_counts, static_cast<size_t>(wd::kRadix) * sb.num_tiles));
+    WD_CUDA(dalloc(&sb.digit_totals, static_cast<size_t>(wd::kRadix) * sb.passes));
+    WD_CUDA(dalloc(&sb.table, s->num_cells));
+    WD_CUDA(cudaMemset(sb.table, 0xFF, sizeof(int2) * s->num_cells));
+    WD_CUDA(dalloc(&s->counters, wd::kNumCounters));
+    WD_CUDA(cudaMemset(s->counters, 0, sizeof(unsigned long long) * wd::kNumCounters));
+    WD_CUDA(dalloc(&s->picard_res, s->picard_iters > 0 ? s->picard_iters : 1));
+    WD_CUDA(cudaMemset(s->picard_res, 0, sizeof(uint32_t) * (s->picard_iters > 0 ? s->picard_iters : 1)));
+    WD_CUDA(dalloc(&s->picard_used, 1));
+    WD_CUDA(cudaMemset(s->picard_used, 0, sizeof(int)));
+    WD_CUDA(dalloc(&s->partials, static_cast<size_t>(3) * wd::reduction_blocks(n)));
+    WD_CUDA(dalloc(&s->red_out, 4));
+    WD_CUDA(dalloc(&s->staging, static_cast<size_t>(6) * n));
+    s->dep_nodes = static_cast<int64_t>(s->cfg.dgrid[0]) * s->cfg.dgrid[1] * s->cfg.dgrid[2];
+    return WD_OK;
+}
+
+int upload_initial(wd_sim* s, const float* state) {
+    const int n = s->n;
+    std::vector<float4> pos(n), vel(n);
+    std::vector<int> ids(n);
+    for (int i = 0; i < n; ++i) {
+        const float* q = state + 6 * static_cast<size_t>(i);
+        pos[i] = make_float4(q[0], q[1], q[2], s->radius[i]);
+        vel[i] = make_float4(q[3], q[4], q[5], s->mass[i]);
+        ids[i] = i;
+    }
+    WD_CUDA(cudaMemcpy(s->posA, pos.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    WD_CUDA(cudaMemcpy(s->velA, vel.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    WD_CUDA(cudaMemcpy(s->idsA, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    // B mirrors A until the first step, so get_rhs before a step reads defined data.
+    WD_CUDA(cudaMemcpy(s->posB, s->posA, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
+    WD_CUDA(cudaMemcpy(s->velB, s->velA, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
+    WD_CUDA(cudaMemcpy(s->idsB, s->idsA, sizeof(int) * n, cudaMemcpyDeviceToDevice));
+    WD_CUDA(cudaMemset(s->acc, 0, sizeof(float4) * n));
+    return WD_OK;
+}
+
+int create_impl(const wd::Config& cfg, int64_t n64, const float* state,
+                const int32_t* material, const float* radius, const float* mass,
+                wd_sim** out) {
+    if (!out) return fail(WD_ERR_INVALID, "wd_create: out is NULL");
+    *out = nullptr;
+    if (n64 <= 0 || n64 > (int64_t{1} << 30))
+        return fail(WD_ERR_INVALID, "wd_create: grain count must be in [1, 2^30]");
+    if (!state) return fail(WD_ERR_INVALID, "wd_create: state is NULL");
+    for (int a = 0; a < 3; ++a) {
+        if (cfg.grid[a] <= 0) return fail(WD_ERR_INVALID, "wd_create: collision grid sizes must be > 0");
+        if (cfg.dgrid[a] <= 0) return fail(WD_ERR_INVALID, "wd_create: density grid sizes must be > 0");
+    }
+    const uint64_t cells = static_cast<uint64_t>(cfg.grid[0]) * cfg.grid[1] * cfg.grid[2];
+    if (cells >= (uint64_t{1} << 32))
+        return fail(WD_ERR_INVALID, "wd_create: collision grid exceeds 2^32 cells");
+    if (!(cfg.particle_radius > 0.f) && !radius)
+        return fail(WD_ERR_INVALID, "wd_create: physics.particle_radius must be > 0");
+    if (cfg.picard_iterations < 1 && cfg.time_integrator != "semi_implicit_euler")
+        return fail(WD_ERR_INVALID, "wd_create: picard_iterations must be >= 1");
+
+    wd_sim* s = new wd_sim();
+    s->cfg = cfg;
+    s->n = static_cast<int>(n64);
+    s->dt = cfg.dt;
+    s->picard = cfg.time_integrator != "semi_implicit_euler";
+    s->picard_iters = s->picard ? cfg.picard_iterations : 1;
+    s->num_cells = cells;
+    s->P = make_params(cfg, s->n, s->dt);
+    s->radius.resize(s->n);
+    s->mass.resize(s->n);
+    s->material.resize(s->n);
+    for (int i = 0; i < s->n; ++i) {
+        const int32_t mat = material ? material[i] : cfg.particle_material;
+        s->material[i] = mat;
+        const float r = radius ? radius[i] : cfg.particle_radius;
+        s->radius[i] = r;
+        float m;
+        if (mass) {
+            m = mass[i];
+        } else if (cfg.density > 0.f) {
+            const double rd = r;
+            m = static_cast<float>(static_cast<double>(cfg.density) * 4.0 / 3.0 * 3.14159265358979323846 * rd * rd * rd);
+        } else {
+            if (mat < 0 || static_cast<size_t>(mat) >= cfg.masses.size()) {
+                delete s;
+                return fail(WD_ERR_INVALID, "wd_create: material id " + std::to_string(mat) +
+                                                " has no entry in materials.masses");
+            }
+            m = cfg.masses[mat];
+        }
+        s->mass[i] = m;
+    }
+    int rc = alloc_sim(s);
+    if (rc == WD_OK) rc = upload_initial(s, state);
+    if (rc != WD_OK) {
+        const std::string msg = wd::last_error_cstr();
+        free_sim(s);
+        return fail(rc, msg);
+    }
+    *out = s;
+    return WD_OK;
+}
+
+}  // namespace
+
+// ============================== C ABI ==============================================
+
+extern "C" {
+
+const char* wd_last_error(void) { return wd::last_error_cstr(); }
+const char* wd_version(void) { return kVersion; }
+
+int wd_config_create(wd_config** out) {
+    if (!out) return fail(WD_ERR_INVALID, "wd_config_create: out is NULL");
+    *out = new wd_config();
+    return WD_OK;
+}
+
+int wd_config_destroy(wd_config* cfg) {
+    delete cfg;
+    return WD_OK;
+}
+
+int wd_config_copy(const wd_config* src, wd_config** out) {
+    if (!src || !out) return fail(WD_ERR_INVALID, "wd_config_copy: NULL argument");
+    *out = new wd_config(*src);
+    return WD_OK;
+}
+
+int wd_config_load_yaml(wd_config* cfg, const char* path) {
+    if (!cfg || !path) return fail(WD_ERR_INVALID, "wd_config_load_yaml: NULL argument");
+    std::string err;
+    const int rc = wd::config_load_yaml(cfg->cfg, path, &err);
+    if (rc < 0) return fail(rc, err);
+    if (rc == WD_WARN_DEFAULTS)
+        wd::set_last_error(std::string("load_config: could not open '") + path + "'");
+    return rc;
+}
+
+int wd_config_set(wd_config* cfg, const char* section, const char* key, const char* value) {
+    if (!cfg || !section || !key || !value) return fail(WD_ERR_INVALID, "wd_config_set: NULL argument");
+    std::string err;
+    const int rc = wd::config_set(cfg->cfg, section, key, value, &err);
+    if (rc < 0) return fail(rc, err);
+    if (rc == WD_WARN_UNKNOWN_KEY)
+        wd::set_last_error(std::string("unknown key '") + section + "." + key + "'");
+    return rc;
+}
+
+int wd_config_get(const wd_config* cfg, const char* section, const char* key, char* buf,
+                  size_t buf_len) {
+    if (!cfg || !section || !key || !buf) return fail(WD_ERR_INVALID, "wd_config_get: NULL argument");
+    std::string v;
+    if (wd::config_get(cfg->cfg, section, key, &v) != WD_OK)
+        return fail(WD_ERR_INVALID, std::string("unknown key '") + section + "." + key + "'");
+    if (v.size() + 1 > buf_len) return fail(WD_ERR_CAPACITY, "wd_config_get: buffer too small");
+    std::memcpy(buf, v.c_str(), v.size() + 1);
+    return WD_OK;
+}
+
+int wd_initial_state(const wd_config* cfg, float* state, int32_t* material, int64_t capacity,
+                     int64_t* n) {
+    if (!cfg || !n) return fail(WD_ERR_INVALID, "wd_initial_state: NULL argument");
+    wd::Grains g;
+    std::string err;
+    const int rc = wd::build_initial_grains(cfg->cfg, &g, &err);
+    if (rc < 0) return fail(rc, err);
+    *n = static_cast<int64_t>(g.material.size());
+    if (*n <= capacity) {
+        if (state) std::memcpy(state, g.state.data(), g.state.size() * sizeof(float));
+        if (material) std::memcpy(material, g.material.data(), g.material.size() * sizeof(int32_t));
+    }
+    return WD_OK;
+}
+
+int wd_create(const wd_config* cfg, wd_sim** out) {
+    if (!cfg) return fail(WD_ERR_INVALID, "wd_create: cfg is NULL");
+    wd::Grains g;
+    std::string err;
+    const int rc = wd::build_initial_grains(cfg->cfg, &g, &err);
+    if (rc < 0) return fail(rc, err);
+    if (g.material.empty()) return fail(WD_ERR_INVALID, "wd_create: initialization produced no grains");
+    return create_impl(cfg->cfg, static_cast<int64_t>(g.material.size()), g.state.data(),
+                       g.material.data(), nullptr, nullptr, out);
+}
+
+int wd_create_from_arrays(const wd_config* cfg, int64_t n, const float* state,
+                          const int32_t* material, const float* radius, const float* mass,
+                          wd_sim** out) {
+    if (!cfg) return fail(WD_ERR_INVALID, "wd_create_from_arrays: cfg is NULL");
+    return create_impl(cfg->cfg, n, state, material, radius, mass, out);
+}
+
+int wd_destroy(wd_sim* sim) {
+    if (!sim) return WD_OK;
+    if (sim->stream) cudaStreamSynchronize(sim->stream);
+    free_sim(sim);
+    return WD_OK;
+}
+
+int wd_step(wd_sim* sim, int64_t nsteps) {
+    if (!sim || nsteps < 0) return fail(WD_ERR_INVALID, "wd_step: bad argument");
+    for (int64_t k = 0; k < nsteps; ++k) {
+        const int parity = sim->P.history ? sim->hist_cur : 0;
+        if (sim->cfg.kernel_timing) {
+            const int rc = timed_step(sim, parity);
+            if (rc) return rc;
+        } else {
+            if (sim->graph_dirty) {
+                const int rc = build_graphs(sim);
+                if (rc) return rc;
+            }
+            WD_CUDA(cudaGraphLaunch(sim->graph[parity], sim->stream));
+        }
+        if (sim->P.history) sim->hist_cur ^= 1;
+        sim->time += sim->dt;
+    }
+    return WD_OK;
+}
+
+int wd_set_dt(wd_sim* sim, float dt) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_set_dt: NULL handle");
+    if (dt != sim->dt) {
+        sim->dt = dt;
+        sim->P.dt = dt;
+        sim->graph_dirty = true;
+    }
+    return WD_OK;
+}
+
+int wd_get_dt(const wd_sim* sim, float* dt) {
+    if (!sim || !dt) return fail(WD_ERR_INVALID, "wd_get_dt: NULL argument");
+    *dt = sim->dt;
+    return WD_OK;
+}
+
+int wd_get_time(const wd_sim* sim, float* t) {
+    if (!sim || !t) return fail(WD_ERR_INVALID, "wd_get_time: NULL argument");
+    *t = sim->time;
+    return WD_OK;
+}
+
+int wd_set_time(wd_sim* sim, float t) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_set_time: NULL handle");
+    sim->time = t;
+    return WD_OK;
+}
+
+int wd_get_n(const wd_sim* sim, int64_t* n) {
+    if (!sim || !n) return fail(WD_ERR_INVALID, "wd_get_n: NULL argument");
+    *n = sim->n;
+    return WD_OK;
+}
+
+int wd_get_picard_stats(const wd_sim* sim_c, int32_t* iterations, float* residual) {
+    wd_sim* sim = const_cast<wd_sim*>(sim_c);
+    if (!sim) return fail(WD_ERR_INVALID, "wd_get_picard_stats: NULL handle");
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    int used = 1;
+    float res = 0.f;
+    if (sim->picard) {
+        WD_CUDA(cudaMemcpy(&used, sim->picard_used, sizeof(int), cudaMemcpyDeviceToHost));
+        if (used > 0) {
+            uint32_t bits = 0;
+            WD_CUDA(cudaMemcpy(&bits, sim->picard_res + (used - 1), sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost));
+            std::memcpy(&res, &bits, sizeof(float));
+        }
+    }
+    if (iterations) *iterations = used;
+    if (residual) *residual = res;
+    return WD_OK;
+}
+
+int wd_set_state_device(wd_sim* sim, const float* d_state) {
+    if (!sim || !d_state) return fail(WD_ERR_INVALID, "wd_set_state_device: NULL argument");
+    wd::launch_state_from_aos(sim->n, d_state, sim->posA, sim->velA, sim->idsA, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    return WD_OK;
+}
+
+int wd_set_state(wd_sim* sim, const float* state) {
+    if (!sim || !state) return fail(WD_ERR_INVALID, "wd_set_state: NULL argument");
+    WD_CUDA(cudaMemcpyAsync(sim->staging, state, sizeof(float) * 6 * static_cast<size_t>(sim->n),
+                            cudaMemcpyHostToDevice, sim->stream));
+    return wd_set_state_device(sim, sim->staging);
+}
+
+int wd_get_state_device(wd_sim* sim, float* d_state) {
+    if (!sim || !d_state) return fail(WD_ERR_INVALID, "wd_get_state_device: NULL argument");
+    wd::launch_state_to_aos(sim->n, sim->posA, sim->velA, sim->idsA, d_state, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    return WD_OK;
+}
+
+int wd_get_state(wd_sim* sim, float* state) {
+    if (!sim || !state) return fail(WD_ERR_INVALID, "wd_get_state: NULL argument");
+    int rc = wd_get_state_device(sim, sim->staging);
+    if (rc) return rc;
+    WD_CUDA(cudaMemcpyAsync(state, sim->staging, sizeof(float) * 6 * static_cast<size_t>(sim->n),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_get_positions_device(wd_sim* sim, float* d_pos) {
+    if (!sim || !d_pos) return fail(WD_ERR_INVALID, "wd_get_positions_device: NULL argument");
+    wd::launch_positions_to_aos(sim->n, sim->posA, sim->idsA, d_pos, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    return WD_OK;
+}
+
+int wd_get_positions(wd_sim* sim, float* positions) {
+    if (!sim || !positions) return fail(WD_ERR_INVALID, "wd_get_positions: NULL argument");
+    int rc = wd_get_positions_device(sim, sim->staging);
+    if (rc) return rc;
+    WD_CUDA(cudaMemcpyAsync(positions, sim->staging, sizeof(float) * 3 * static_cast<size_t>(sim->n),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_get_rhs(wd_sim* sim, float* rhs) {
+    if (!sim || !rhs) return fail(WD_ERR_INVALID, "wd_get_rhs: NULL argument");
+    wd::launch_rhs_to_aos(sim->n, sim->velB, sim->acc, sim->idsB, sim->staging, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    WD_CUDA(cudaMemcpyAsync(rhs, sim->staging, sizeof(float) * 6 * static_cast<size_t>(sim->n),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_get_grain_props(const wd_sim* sim, float* radius, float* mass, int32_t* material) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_get_grain_props: NULL handle");
+    const size_t n = static_cast<size_t>(sim->n);
+    if (radius) std::memcpy(radius, sim->radius.data(), n * sizeof(float));
+    if (mass) std::memcpy(mass, sim->mass.data(), n * sizeof(float));
+    if (material) std::memcpy(material, sim->material.data(), n * sizeof(int32_t));
+    return WD_OK;
+}
+
+int wd_set_stream(wd_sim* sim, void* stream) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_set_stream: NULL handle");
+    WD_CUDA(cudaStreamSynchronize(sim->stream));
+    sim->stream = stream ? static_cast<cudaStream_t>(stream) : sim->own_stream;
+    return WD_OK;
+}
+
+int wd_get_stream(const wd_sim* sim, void** stream) {
+    if (!sim || !stream) return fail(WD_ERR_INVALID, "wd_get_stream: NULL argument");
+    *stream = static_cast<void*>(sim->stream);
+    return WD_OK;
+}
+
+int wd_synchronize(wd_sim* sim) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_synchronize: NULL handle");
+    return sync_stream(sim);
+}
+
+int wd_get_history(wd_sim* sim, int32_t* count, int32_t* partner, float* xi) {
+    if (!sim || !count || !partner || !xi) return fail(WD_ERR_INVALID, "wd_get_history: NULL argument");
+    const size_t n = static_cast<size_t>(sim->n);
+    if (!sim->P.history) {
+        std::memset(count, 0, n * sizeof(int32_t));
+        return WD_OK;
+    }
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    std::vector<float4> rows(n * wd::kHistCap);
+    WD_CUDA(cudaMemcpy(count, sim->hcnt[sim->hist_cur], n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    WD_CUDA(cudaMemcpy(rows.data(), sim->hist[sim->hist_cur], rows.size() * sizeof(float4),
+                       cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < wd::kHistCap; ++k) {
+            const float4 e = rows[i * wd::kHistCap + k];
+            const bool live = k < count[i];
+            int32_t p;
+            std::memcpy(&p, &e.w, sizeof(int32_t));
+            partner[i * wd::kHistCap + k] = live ? p : 0;
+            float* x = xi + (i * wd::kHistCap + k) * 3;
+            x[0] = live ? e.x : 0.f;
+            x[1] = live ? e.y : 0.f;
+            x[2] = live ? e.z : 0.f;
+        }
+    return WD_OK;
+}
+
+int wd_set_history(wd_sim* sim, const int32_t* count, const int32_t* partner, const float* xi) {
+    if (!sim || !count || !partner || !xi) return fail(WD_ERR_INVALID, "wd_set_history: NULL argument");
+    if (!sim->P.history) return fail(WD_ERR_INVALID, "wd_set_history: simulation.history is off");
+    const size_t n = static_cast<size_t>(sim->n);
+    std::vector<float4> rows(n * wd::kHistCap);
+    for (size_t i = 0; i < n; ++i) {
+        if (count[i] < 0 || count[i] > wd::kHistCap)
+            return fail(WD_ERR_INVALID, "wd_set_history: count out of range");
+        for (int k = 0; k < wd::kHistCap; ++k) {
+            const float* x = xi + (i * wd::kHistCap + k) * 3;
+            float w;
+            std::memcpy(&w, &partner[i * wd::kHistCap + k], sizeof(float));
+            rows[i * wd::kHistCap + k] = make_float4(x[0], x[1], x[2], w);
+        }
+    }
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    WD_CUDA(cudaMemcpy(sim->hcnt[sim->hist_cur], count, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    WD_CUDA(cudaMemcpy(sim->hist[sim->hist_cur], rows.data(), rows.size() * sizeof(float4),
+                       cudaMemcpyHostToDevice));
+    return WD_OK;
+}
+
+int wd_density_grid_nodes(const wd_sim* sim, int64_t* nodes) {
+    if (!sim || !nodes) return fail(WD_ERR_INVALID, "wd_density_grid_nodes: NULL argument");
+    *nodes = sim->dep_nodes;
+    return WD_OK;
+}
+
+int wd_compute_density_grid_device(wd_sim* sim, float* d_grid) {
+    if (!sim || !d_grid) return fail(WD_ERR_INVALID, "wd_compute_density_grid_device: NULL argument");
+    if (!sim->dep_acc) {
+        WD_CUDA(dalloc(&sim->dep_bounds, 4));
+        WD_CUDA(dalloc(&sim->dep_acc, static_cast<size_t>(4) * sim->dep_nodes));
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (sim->cfg.kernel_timing) {
+        e0 = take_event(sim);
+        e1 = take_event(sim);
+        WD_CUDA(cudaEventRecord(e0, sim->stream));
+    }
+    wd::launch_deposit(sim->n, sim->posA, sim->velA, sim->cfg.dom_lo, sim->cfg.dom_hi,
+                       sim->cfg.dgrid, sim->dep_bounds, sim->dep_acc, d_grid, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    if (e0) {
+        WD_CUDA(cudaEventRecord(e1, sim->stream));
+        WD_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        sim->wct[3] += ms;
+        sim->ev_pool.push_back(e0);
+        sim->ev_pool.push_back(e1);
+    }
+    return WD_OK;
+}
+
+int wd_compute_density_grid(wd_sim* sim, float* grid) {
+    if (!sim || !grid) return fail(WD_ERR_INVALID, "wd_compute_density_grid: NULL argument");
+    if (!sim->dep_out) WD_CUDA(dalloc(&sim->dep_out, static_cast<size_t>(4) * sim->dep_nodes));
+    int rc = wd_compute_density_grid_device(sim, sim->dep_out);
+    if (rc) return rc;
+    WD_CUDA(cudaMemcpyAsync(grid, sim->dep_out, sizeof(float) * 4 * static_cast<size_t>(sim->dep_nodes),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_compute_total_energy(wd_sim* sim, double* energy) {
+    if (!sim || !energy) return fail(WD_ERR_INVALID, "wd_compute_total_energy: NULL argument");
+    int rc = ondemand_search(sim);
+    if (rc) return rc;
+    wd::launch_energy(sim->P, sim->posC, sim->velC, sim->idsC, sim->sb.table,
+                      sim->hist[sim->hist_cur], sim->hcnt[sim->hist_cur], sim->partials,
+                      sim->red_out, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    WD_CUDA(cudaMemcpyAsync(energy, sim->red_out, sizeof(double), cudaMemcpyDeviceToHost, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_compute_momentum(wd_sim* sim, double* momentum3) {
+    if (!sim || !momentum3) return fail(WD_ERR_INVALID, "wd_compute_momentum: NULL argument");
+    wd::launch_momentum(sim->n, sim->velA, sim->partials, sim->red_out, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    WD_CUDA(cudaMemcpyAsync(momentum3, sim->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                            sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_is_stable(wd_sim* sim, int32_t* stable) {
+    if (!sim || !stable) return fail(WD_ERR_INVALID, "wd_is_stable: NULL argument");
+    WD_CUDA(cudaMemsetAsync(sim->counters + wd::kCntUnstable, 0, sizeof(unsigned long long), sim->stream));
+    wd::launch_stability(sim->P, sim->posA, sim->counters, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    unsigned long long flag = 0;
+    WD_CUDA(cudaMemcpyAsync(&flag, sim->counters + wd::kCntUnstable, sizeof(flag),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    *stable = flag ? 0 : 1;
+    return WD_OK;
+}
+
+int wd_compute_max_acceleration(wd_sim* sim, float* max_accel) {
+    if (!sim || !max_accel) return fail(WD_ERR_INVALID, "wd_compute_max_acceleration: NULL argument");
+    WD_CUDA(cudaMemsetAsync(sim->counters + wd::kCntMaxAccel, 0, sizeof(unsigned long long), sim->stream));
+    wd::launch_max_accel(sim->n, sim->acc, sim->counters, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    unsigned long long bits = 0;
+    WD_CUDA(cudaMemcpyAsync(&bits, sim->counters + wd::kCntMaxAccel, sizeof(bits),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    const uint32_t b = static_cast<uint32_t>(bits);
+    std::memcpy(max_accel, &b, sizeof(float));
+    return WD_OK;
+}
+
+static int read_counter(wd_sim* sim, int which, int64_t* out) {
+    unsigned long long v = 0;
+    WD_CUDA(cudaMemcpyAsync(&v, sim->counters + which, sizeof(v), cudaMemcpyDeviceToHost, sim->stream));
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    *out = static_cast<int64_t>(v);
+    return WD_OK;
+}
+
+int wd_grid_overflow_count(wd_sim* sim, int64_t* count) {
+    if (!sim || !count) return fail(WD_ERR_INVALID, "wd_grid_overflow_count: NULL argument");
+    return read_counter(sim, wd::kCntGridOverflow, count);
+}
+
+int wd_history_overflow_count(wd_sim* sim, int64_t* count) {
+    if (!sim || !count) return fail(WD_ERR_INVALID, "wd_history_overflow_count: NULL argument");
+    return read_counter(sim, wd::kCntHistOverflow, count);
+}
+
+int wd_timings(wd_sim* sim, float* ms4) {
+    if (!sim || !ms4) return fail(WD_ERR_INVALID, "wd_timings: NULL argument");
+    int rc = flush_timings(sim);
+    if (rc) return rc;
+    for (int i = 0; i < 4; ++i) ms4[i] = sim->wct[i];
+    return WD_OK;
+}
+
+int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
+    wd_sim* sim = const_cast<wd_sim*>(sim_c);
+    if (!sim || !kernels) return fail(WD_ERR_INVALID, "wd_kernels_per_step: NULL argument");
+    const int per_search = 2 + 3 * sim->sb.passes;  // keys, 3 per radix pass, runs
+    const int per_iter = per_search + 2;            // gather, contact
+    *kernels = static_cast<int64_t>(per_iter) * sim->picard_iters;
+    return WD_OK;
+}
+
+int wd_debug_cell_keys(wd_sim* sim, int32_t* keys) {
+    if (!sim || !keys) return fail(WD_ERR_INVALID, "wd_debug_cell_keys: NULL argument");
+    int32_t* d = reinterpret_cast<int32_t*>(sim->staging);
+    wd::launch_cell_keys_by_id(sim->P, sim->posA, sim->idsA, d, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    WD_CUDA(cudaMemcpyAsync(keys, d, sizeof(int32_t) * static_cast<size_t>(sim->n),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_debug_sorted(wd_sim* sim, int32_t* keys, int32_t* ids) {
+    if (!sim || !keys || !ids) return fail(WD_ERR_INVALID, "wd_debug_sorted: NULL argument");
+    int rc = ondemand_search(sim);
+    if (rc) return rc;
+    const size_t bytes = sizeof(int32_t) * static_cast<size_t>(sim->n);
+    WD_CUDA(cudaMemcpyAsync(keys, sim->sb.keys[sim->search_out], bytes, cudaMemcpyDeviceToHost, sim->stream));
+    WD_CUDA(cudaMemcpyAsync(ids, sim->sb.vals[sim->search_out], bytes, cudaMemcpyDeviceToHost, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* contact,
+                        int64_t cap, int64_t* total) {
+    if (!sim || !offsets || !total) return fail(WD_ERR_INVALID, "wd_debug_candidates: NULL argument");
+    int rc = ondemand_search(sim);
+    if (rc) return rc;
+    const int n = sim->n;
+    if (!sim->cand_count) {
+        WD_CUDA(dalloc(&sim->cand_count, n));
+        WD_CUDA(dalloc(&sim->cand_offsets, static_cast<size_t>(n) + 1));
+    }
+    wd::launch_candidate_count(sim->P, sim->posC, sim->idsC, sim->sb.table, sim->cand_count, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    std::vector<int> counts(n);
+    WD_CUDA(cudaMemcpyAsync(counts.data(), sim->cand_count, sizeof(int) * n, cudaMemcpyDeviceToHost, sim->stream));
+    rc = sync_stream(sim);
+    if (rc) return rc;
+    offsets[0] = 0;
+    for (int i = 0; i < n; ++i) offsets[i + 1] = offsets[i] + counts[i];
+    *total = offsets[n];
+    if (!cand || !contact || *total > cap) return WD_OK;
+    int* d_cand = nullptr;
+    uint8_t* d_contact = nullptr;
+    WD_CUDA(dalloc(&d_cand, static_cast<size_t>(*total)));
+    WD_CUDA(dalloc(&d_contact, static_cast<size_t>(*total)));
+    WD_CUDA(cudaMemcpyAsync(sim->cand_offsets, offsets, sizeof(int64_t) * (n + 1),
+                            cudaMemcpyHostToDevice, sim->stream));
+    wd::launch_candidate_fill(sim->P, sim->posC, sim->idsC, sim->sb.table, sim->cand_offsets,
+                              d_cand, d_contact, sim->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(cand, d_cand, sizeof(int32_t) * static_cast<size_t>(*total),
+                            cudaMemcpyDeviceToHost, sim->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(contact, d_contact, static_cast<size_t>(*total), cudaMemcpyDeviceToHost,
+                            sim->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sim->stream);
+    cudaFree(d_cand);
+    cudaFree(d_contact);
+    WD_CUDA(e);
+    return WD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+"""Initial states and the reference's state file format.
+
+State file (reader: src/particle_dynamics.cu:212-235; writer:
+surrogate/decode_particles.py:355-361): little-endian int32 n, then n*6 float32 laid
+out [x, y, z, vx, vy, vz] per grain. Grains get `initialization.particle_material`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from ._lib import check, lib, ptr
+from .config import SimConfig
+
+
+def initial_state(cfg: SimConfig) -> tuple[np.ndarray, np.ndarray]:
+    """(state[n, 6] float32, material[n] int32) for cfg's initialization section,
+    built by the library's host code exactly as the reference's constructor does."""
+    n = ctypes.c_int64()
+    check(lib.wd_initial_state(cfg.handle, None, None, 0, ctypes.byref(n)))
+    state = np.empty((n.value, 6), np.float32)
+    material = np.empty(n.value, np.int32)
+    check(lib.wd_initial_state(cfg.handle, ptr(state), ptr(material), n.value, ctypes.byref(n)))
+    return state, material
+
+
+def grain_properties(cfg: SimConfig, material: np.ndarray,
+                     radius: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """Per-grain (radius, mass) the library derives when none are given: the global
+    particle_radius, and mass from physics.density (4/3 pi r^3 rho) when it is set,
+    else the materials.masses table."""
+    n = material.size
+    r = np.full(n, np.float32(cfg.physics.particle_radius), np.float32) if radius is None \
+        else np.asarray(radius, np.float32)
+    rho = cfg.physics.density
+    if rho > 0:
+        rd = r.astype(np.float64)
+        m = (np.float64(np.float32(rho)) * 4.0 / 3.0 * np.pi * rd * rd * rd).astype(np.float32)
+    else:
+        table = np.asarray(cfg.masses, np.float32)
+        m = table[material]
+    return r, m
+
+
+def write_state_file(path: str | os.PathLike, state: np.ndarray) -> None:
+    st = np.ascontiguousarray(state, dtype="<f4").reshape(-1, 6)
+    with open(path, "wb") as f:
+        f.write(np.int32(st.shape[0]).astype("<i4").tobytes())
+        f.write(st.tobytes())
+
+
+def read_state_file(path: str | os.PathLike) -> np.ndarray:
+    with open(path, "rb") as f:
+        raw = f.read()
+    if len(raw) < 4:
+        raise ValueError(f"{path}: missing particle count")
+    n = int(np.frombuffer(raw[:4], "<i4")[0])
+    if n <= 0:
+        raise ValueError(f"{path}: bad particle count {n}")
+    body = np.frombuffer(raw[4:], "<f4")
+    if body.size < 6 * n:
+        raise ValueError(f"{path}: short of {6 * n} floats")
+    return body[:6 * n].reshape(n, 6).copy()
