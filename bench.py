@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the world DEM step on B200: grain-steps/s at 2^20 grains, FP32.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Workload (default): granular column collapse at 2^20 grains, lognormal diameters
+(mean 5 mm, log-sigma 0.15, clipped to [0.7 d, 1.4 d]), mu = 0.5 with tangential
+springs and per-pair history, restitution 0.5, k_n = 1e5 N/m, semi-implicit Euler,
+dt = 1e-5 s, 453 x 453 x 226 collision grid, 128^3 CIC grid; synthetic seeded input
+(world_b200/scenes.py). A step is one take_step() over all grains.
+
+value  -- device time of K steps (CUDA events on the library's stream, L2 flushed
+          by a 512 MiB write before every timed step, flush excluded), max over
+          ranks; grains x ranks x K / time.
+e2e    -- the same metric through the C ABI with host buffers: each step
+          wd_set_state() from pinned host memory, wd_step(1), wd_get_positions() to
+          pinned host memory, all inside the timed region.
+roofline -- the contact kernel (forces + integrator, the dominant kernel): its
+          algorithmic bytes per launch over its average event-timed duration,
+          against the measured HBM copy bandwidth.
+cpu_baseline -- the oracle port (C, OpenMP on all host cores) on a bounded sample
+          of the same workload, rank 0 at N = 1 only.
+
+Multi-GPU: one process per GPU (torchrun), each rank advancing its own ensemble
+member of the same workload (seed 12345 + rank); no collective on the data path,
+scaling "weak"; only the timing max-reduction uses NCCL.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grain-steps/s at 2^20 grains FP32"
+UNIT = "grain-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="collapse_1m_sie_mu05")
+    ap.add_argument("--grains", type=int, default=None, help="override the grain count")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--phase-steps", type=int, default=50)
+    return ap.parse_args()
+
+
+def env_int(name: str, default: int) -> int:
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def workload_config(scene, args) -> dict:
+    c = scene.cfg
+    return {
+        "workload": args.workload,
+        "grains": scene.n,
+        "integrator": c.time_integrator,
+        "mu": c.physics.friction,
+        "tangential_history": bool(c.history),
+        "diameters": "lognormal(mean 5 mm, sigma 0.15) clipped [0.7d, 1.4d]"
+        if "1m" in args.workload else "see world_b200/scenes.py",
+        "collision_grid": [c.collision_grid_size_x, c.collision_grid_size_y, c.collision_grid_size_z],
+        "cic_grid": c.density_grid_size_x,
+        "dt": c.dt,
+        "l2": "flushed (512 MiB write) before every timed step, flush not timed",
+    }
+
+
+# ------------------------------------------------------------------ clocks -------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, indices):
+        self.indices = set(indices)
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    idx = int(parts[0])
+                except ValueError:
+                    continue
+                if idx not in self.indices:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured"
+    except (OSError, KeyError, ValueError, TypeError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(workload: str):
+    """DRAM bytes per contact-kernel launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "contact_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        return data.get(workload)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------------ CPU side -----
+def cpu_oracle_rate(scene, seconds: float, max_steps: int, warmup: int = 1):
+    """The oracle port on all host cores: (grain-steps/s, steps, elapsed, threads)."""
+    from oracle.oracle import OracleSim, params_from_config
+    from world_b200.state_io import grain_properties
+    import numpy as np
+    threads = os.cpu_count() or 1
+    from oracle.oracle import lib as oracle_lib
+    oracle_lib().dem_set_num_threads(threads)
+    material = np.full(scene.n, scene.cfg.particle_material, np.int32)
+    radius, mass = grain_properties(scene.cfg, material, scene.radius)
+    sim = OracleSim(params_from_config(scene.cfg), scene.state, radius, mass)
+    for _ in range(max(0, warmup)):
+        sim.step()
+    steps = 0
+    t0 = time.perf_counter()
+    while steps < max_steps and (steps == 0 or time.perf_counter() - t0 < seconds):
+        sim.step()
+        steps += 1
+    elapsed = time.perf_counter() - t0
+    return scene.n * steps / elapsed, steps, elapsed, oracle_lib().dem_num_threads()
+
+
+def run_reference(args) -> int:
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    from world_b200.scenes import scene_for
+    scene = scene_for(args.workload, n=args.grains, seed=12345)
+    budget = min(180.0, max(10.0, 0.5 * args.steps))
+    rate, steps, elapsed, threads = cpu_oracle_rate(scene, budget, args.steps,
+                                                    warmup=min(args.warmup, 1))
+    sample = (f"{steps} of {args.steps} requested steps of the full {scene.n}-grain workload "
+              f"({elapsed:.1f} s, bounded at {budget:.0f} s); the reference has no CPU step, so "
+              "this is its algorithm restated in C (oracle/dem_oracle.c)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": steps, "warmup": min(args.warmup, 1),
+        "ms_per_step": 1e3 * elapsed / max(steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded column collapse)",
+        "config": workload_config(scene, args),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU side -----
+def run_ours(args) -> int:
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from world_b200 import ParticleDynamics
+    from world_b200._lib import check, lib, ptr
+    from world_b200.scenes import scene_for
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local))
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    scene = scene_for(args.workload, n=args.grains, seed=12345 + rank)
+    sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
+    sim.set_kernel_timing(False)
+    n = sim.n
+    stream = torch.cuda.ExternalStream(sim.stream_ptr())
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    sim.advance(args.warmup)
+    sim.synchronize()
+    barrier()
+
+    sampler = ClockSampler(range(world) if world > 1 else [local]) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    barrier()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        ev[k][0].record(stream)
+        sim.take_step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    local_ms = sum(a.elapsed_time(b) for a, b in ev)
+    total_ms = max_over_ranks(local_ms)
+    value = n * world * args.steps / (total_ms / 1e3)
+
+    # per-phase timing of the same workload for the roofline (direct launches)
+    sim.set_kernel_timing(True)
+    t0 = sim._timings()
+    for k in range(args.phase_steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        sim.take_step()
+    sim.synchronize()
+    t1 = sim._timings()
+    sim.set_kernel_timing(False)
+    search_ms = float(t1[0] - t0[0]) / args.phase_steps
+    contact_ms = float(t1[1] - t0[1]) / args.phase_steps
+    cnt, _, _ = sim.get_history()
+    entries = int(cnt.astype(np.int64).sum())
+    # contact kernel, algorithmic bytes per launch: read x,r / v,m / id (36 B) and
+    # write x,r / v,m / id / a (52 B) per grain; history rows read and written
+    # (16 B per entry each way) plus the per-grain counts (4 B each way)
+    hist_bytes = (2 * 16 * entries + 8 * n) if scene.cfg.history else 0
+    contact_bytes = 88 * n + hist_bytes
+    achieved = contact_bytes / (contact_ms / 1e3) / 1e9
+    peak, peak_kind = measured_hbm_peak()
+
+    # e2e through the C ABI with pinned host buffers
+    h_state = torch.from_numpy(np.ascontiguousarray(scene.state.reshape(-1))).pin_memory()
+    h_pos = torch.empty(3 * n, dtype=torch.float32).pin_memory()
+    sim.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    check(lib.wd_get_state(sim.handle, ptr(h_state)))
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        check(lib.wd_set_state(sim.handle, ptr(h_state)))
+        check(lib.wd_step(sim.handle, 1))
+        check(lib.wd_get_positions(sim.handle, ptr(h_pos)))
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = n * world * args.e2e_steps / (e2e_ms / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, steps, elapsed, threads = cpu_oracle_rate(scene, args.cpu_seconds, 10_000)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{steps} steps of the same {n}-grain workload on {threads} host "
+                         f"threads ({elapsed:.1f} s), oracle/dem_oracle.c with OpenMP"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
+            "config": workload_config(scene, args),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic(args.workload),
+                         "kernel": "k_force (contact forces + integrator)",
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "algorithmic_bytes_per_launch": contact_bytes,
+                         "kernel_ms": contact_ms, "search_ms": search_ms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+                    "d2h_bytes_per_step": 12 * n, "steps": args.e2e_steps},
+            "clocks": clocks,
+            "gpu_launches": sim.kernels_per_step() * args.steps,
+            "history_entries_per_grain": entries / n,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    del flush
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main() -> int:
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -173,6 +173,10 @@ int wd_history_overflow_count(wd_sim* sim, int64_t* count);
  * drivers.kernel_timing is true. The contact kernel integrates in its epilogue, so
  * take_step_wct stays 0 and compute_rhs_wct covers forces plus integration. */
 int wd_timings(wd_sim* sim, float* ms4);
+/* Switch drivers.kernel_timing at run time (the reference fixes it at construction,
+ * src/sim_config.h:165): 1 = direct launches with events per phase, 0 = one graph
+ * launch per step. */
+int wd_set_kernel_timing(wd_sim* sim, int32_t enabled);
 /* Number of kernels one step launches (for launch accounting). */
 int wd_kernels_per_step(const wd_sim* sim, int64_t* kernels);
 

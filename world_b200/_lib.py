@@ -91,6 +91,7 @@ SIGNATURES = {
     "wd_grid_overflow_count": ([_p, _i64], c_int),
     "wd_history_overflow_count": ([_p, _i64], c_int),
     "wd_timings": ([_p, _f], c_int),
+    "wd_set_kernel_timing": ([_p, c_int32], c_int),
     "wd_kernels_per_step": ([_p, _i64], c_int),
     "wd_debug_cell_keys": ([_p, _p], c_int),
     "wd_debug_sorted": ([_p, _p, _p], c_int),

@@ -881,6 +881,12 @@ int wd_timings(wd_sim* sim, float* ms4) {
     return WD_OK;
 }
 
+int wd_set_kernel_timing(wd_sim* sim, int32_t enabled) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_set_kernel_timing: NULL handle");
+    sim->cfg.kernel_timing = enabled != 0;
+    return WD_OK;
+}
+
 int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
     wd_sim* sim = const_cast<wd_sim*>(sim_c);
     if (!sim || !kernels) return fail(WD_ERR_INVALID, "wd_kernels_per_step: NULL argument");

@@ -243,6 +243,14 @@ class ParticleDynamics:
     def density_grid_wct(self) -> float:
         return float(self._timings()[3])
 
+    def set_kernel_timing(self, enabled: bool) -> None:
+        check(lib.wd_set_kernel_timing(self._h, 1 if enabled else 0))
+
+    def stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        check(lib.wd_get_stream(self._h, ctypes.byref(s)))
+        return int(s.value or 0)
+
     def kernels_per_step(self) -> int:
         v = ctypes.c_int64()
         check(lib.wd_kernels_per_step(self._h, ctypes.byref(v)))

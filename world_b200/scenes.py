@@ -1,0 +1,186 @@
+"""Seeded synthetic scenes for the benchmark workloads.
+
+No dataset ships with the reference, so these generators stand in for its runs, with
+the shapes, sizes and value distributions of the workloads they name:
+
+* column_collapse(n, ...): granular column collapse. Grains on a simple-cubic lattice
+  inside a cylinder of radius R and height 4R, centred in a walled box; the lattice
+  spacing is the smallest one whose first n sites (ordered by z, then y, then x) all
+  fit; each site is jittered uniformly by +-0.05 d per axis. At n = 32,768 and
+  d = 5 mm the box is 1.0 x 1.0 x 0.5 m and R = 0.1 m; larger n scales R and the box
+  by (n / 32768)^(1/3). Diameters: "uniform" in [0.9 d, 1.1 d], "lognormal" with
+  arithmetic mean d and log-sigma 0.15 clipped to [0.7 d, 1.4 d], or "mono".
+* dense_box(n, ...): grains at volume fraction 0.55 in a 2 x 2 x 1 m box on a
+  jittered body-centred-cubic lattice (simple cubic tops out at 0.524), velocities
+  N(0, 0.5 m/s) per component.
+
+Each returns (SimConfig, state[n, 6], radius[n]); masses come from physics.density
+(2500 kg/m^3) inside the library. The collision cell is the larger of 1.1 d and the
+largest contact distance (2 r_max), so the 27-cell stencil sees every contact.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from .config import SimConfig
+
+D_REF = 5e-3          # mean diameter d (m)
+N_REF = 32768         # grains of the 1.0 x 1.0 x 0.5 m reference column
+
+
+@dataclass
+class Scene:
+    cfg: SimConfig
+    state: np.ndarray    # (n, 6) float32
+    radius: np.ndarray   # (n,) float32
+    name: str
+
+    @property
+    def n(self) -> int:
+        return int(self.state.shape[0])
+
+
+def _diameters(rng: np.random.Generator, n: int, d: float, kind: str) -> np.ndarray:
+    if kind == "mono":
+        return np.full(n, d, np.float64)
+    if kind == "uniform":
+        return rng.uniform(0.9 * d, 1.1 * d, n)
+    if kind == "lognormal":
+        sigma = 0.15
+        mu = math.log(d) - 0.5 * sigma * sigma
+        return np.clip(rng.lognormal(mu, sigma, n), 0.7 * d, 1.4 * d)
+    raise ValueError(f"unknown diameter distribution '{kind}'")
+
+
+def _cylinder_sites(n: int, spacing: float, radius_xy: float, z0: float) -> np.ndarray | None:
+    k = int(math.floor(radius_xy / spacing))
+    ax = np.arange(-k, k + 1, dtype=np.float64) * spacing
+    yy, xx = np.meshgrid(ax, ax, indexing="ij")          # rows: y, cols: x
+    inside = (xx * xx + yy * yy) <= radius_xy * radius_xy
+    layer = np.stack([xx[inside], yy[inside]], axis=1)    # (y, x) order within a layer
+    per_layer = layer.shape[0]
+    if per_layer == 0:
+        return None
+    layers = -(-n // per_layer)
+    z = z0 + np.arange(layers, dtype=np.float64) * spacing
+    sites = np.concatenate([np.column_stack([layer, np.full(per_layer, zz)]) for zz in z])
+    return sites[:n]
+
+
+def _apply_common(cfg: SimConfig, box: tuple[float, float, float], d_max: float, d_mean: float,
+                  *, mu: float, restitution: float, k_n: float, density: float, dt: float,
+                  history: bool, integrator: str, picard_iterations: int, picard_tol: float,
+                  cic: int, cell_factor: float = 1.1) -> None:
+    lx, ly, lz = box
+    cfg.domain.x_min, cfg.domain.x_max = -0.5 * lx, 0.5 * lx
+    cfg.domain.y_min, cfg.domain.y_max = -0.5 * ly, 0.5 * ly
+    cfg.domain.z_min, cfg.domain.z_max = 0.0, lz
+    ph = cfg.physics
+    ph.wall_x_min, ph.wall_x_max = -0.5 * lx, 0.5 * lx
+    ph.wall_y_min, ph.wall_y_max = -0.5 * ly, 0.5 * ly
+    ph.floor_z, ph.ceiling_z = 0.0, lz
+    ph.gravity = 9.81
+    ph.particle_radius = 0.5 * d_mean
+    ph.normal_stiffness = k_n
+    ph.max_force = k_n * 0.5 * d_mean          # clamp at one mean radius of overlap
+    ph.restitution = restitution
+    ph.friction = mu
+    ph.density = density
+    cfg.history = history and mu > 0
+    cfg.dt = dt
+    cell = max(cell_factor * d_mean, d_max)
+    cfg.collision_grid_size_x = max(1, int(math.floor(lx / cell)))
+    cfg.collision_grid_size_y = max(1, int(math.floor(ly / cell)))
+    cfg.collision_grid_size_z = max(1, int(math.floor(lz / cell)))
+    cfg.particles_per_cell = 16
+    cfg.density_grid_size_x = cic
+    cfg.density_grid_size_y = cic
+    cfg.density_grid_size_z = cic
+    cfg.time_integrator = integrator
+    cfg.picard_iterations = picard_iterations
+    cfg.picard_tolerance = picard_tol
+    cfg.kernel_timing = False
+
+
+def column_collapse(n: int = N_REF, *, diameters: str = "uniform", seed: int = 12345,
+                    mu: float = 0.5, restitution: float = 0.5, k_n: float = 1e5,
+                    density: float = 2500.0, dt: float = 1e-5, history: bool = True,
+                    integrator: str = "semi_implicit_euler", picard_iterations: int = 8,
+                    picard_tol: float = 1e-6, cic: int = 64, d: float = D_REF) -> Scene:
+    rng = np.random.default_rng(seed)
+    scale = (n / N_REF) ** (1.0 / 3.0)
+    R = 0.1 * scale
+    H = 4.0 * R
+    box = (1.0 * scale, 1.0 * scale, 0.5 * scale)
+    diam = _diameters(rng, n, d, diameters)
+    d_max = float(diam.max())
+    # smallest spacing (>= d_max) whose first n sites fit in the cylinder
+    spacing = max((math.pi * R * R * H / n) ** (1.0 / 3.0), d_max * 1.001)
+    while True:
+        sites = _cylinder_sites(n, spacing, R - 0.5 * d_max, 0.5 * spacing + 0.5 * d_max)
+        if sites is not None and sites[-1, 2] + 0.5 * d_max <= box[2]:
+            break
+        spacing *= 0.995
+        if spacing < d_max:
+            raise ValueError("column does not fit the box")
+    jitter = rng.uniform(-0.05 * d, 0.05 * d, size=(n, 3))
+    pos = sites + jitter
+    state = np.zeros((n, 6), np.float32)
+    state[:, :3] = pos.astype(np.float32)
+    cfg = SimConfig()
+    _apply_common(cfg, box, d_max, d, mu=mu, restitution=restitution, k_n=k_n, density=density,
+                  dt=dt, history=history, integrator=integrator,
+                  picard_iterations=picard_iterations, picard_tol=picard_tol, cic=cic)
+    return Scene(cfg, state, (0.5 * diam).astype(np.float32),
+                 f"column_collapse n={n} d={diameters} mu={mu} {integrator}")
+
+
+def dense_box(n: int = 1 << 24, *, phi: float = 0.55, seed: int = 2024, mu: float = 0.5,
+              restitution: float = 0.5, k_n: float = 1e5, density: float = 2500.0,
+              dt: float = 1e-5, history: bool = True, cic: int = 64) -> Scene:
+    rng = np.random.default_rng(seed)
+    box = (2.0, 2.0, 1.0)
+    vol = box[0] * box[1] * box[2]
+    d = (6.0 * phi * vol / (math.pi * n)) ** (1.0 / 3.0)
+    a = (2.0 * (math.pi / 6.0) * d ** 3 / phi) ** (1.0 / 3.0)   # BCC: 2 sites per a^3
+    nx, ny, nz = (int(math.floor((L - d) / a)) for L in box)
+    base = np.stack(np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij"),
+                    axis=-1).reshape(-1, 3)[:, ::-1].astype(np.float64)   # (x, y, z), z-major
+    corner = base * a
+    centre = corner + 0.5 * a
+    sites = np.empty((2 * base.shape[0], 3))
+    sites[0::2] = corner
+    sites[1::2] = centre
+    sites = sites[:n]
+    if sites.shape[0] < n:
+        raise ValueError("box too small for the requested grains")
+    lo = np.array([-0.5 * box[0], -0.5 * box[1], 0.0]) + 0.5 * d + 0.02 * a
+    pos = lo + sites + rng.uniform(-0.02 * d, 0.02 * d, size=(n, 3))
+    state = np.zeros((n, 6), np.float32)
+    state[:, :3] = pos.astype(np.float32)
+    state[:, 3:] = rng.normal(0.0, 0.5, size=(n, 3)).astype(np.float32)
+    cfg = SimConfig()
+    _apply_common(cfg, box, d, d, mu=mu, restitution=restitution, k_n=k_n, density=density,
+                  dt=dt, history=history, integrator="semi_implicit_euler",
+                  picard_iterations=8, picard_tol=1e-6, cic=cic)
+    return Scene(cfg, state, np.full(n, 0.5 * d, np.float32), f"dense_box n={n} phi={phi}")
+
+
+def scene_for(workload: str, n: int | None = None, seed: int | None = None) -> Scene:
+    """Named workloads used by bench.py and the tests."""
+    kw = {} if seed is None else {"seed": seed}
+    if workload == "collapse_32k":
+        return column_collapse(n or N_REF, diameters="uniform", cic=64, **kw)
+    if workload == "collapse_1m_sie_mu05":
+        return column_collapse(n or (1 << 20), diameters="lognormal", mu=0.5, cic=128, **kw)
+    if workload == "collapse_1m_sie_mu0":
+        return column_collapse(n or (1 << 20), diameters="lognormal", mu=0.0, cic=128, **kw)
+    if workload == "collapse_1m_picard_mu05":
+        return column_collapse(n or (1 << 20), diameters="lognormal", mu=0.5, cic=128,
+                               integrator="backward_euler_picard", **kw)
+    if workload == "dense_16m":
+        return dense_box(n or (1 << 24), **kw)
+    raise ValueError(f"unknown workload '{workload}'")
