@@ -407,6 +407,18 @@ int dem_compute_rhs(const dem_params* p, int64_t n, const float* state,
     return 0;
 }
 
+/* rhs = [v, F/m] at the state the forces were evaluated on (before the update),
+ * as the reference's device_rhs holds it (src/compute_rhs_kernel.cu:207-210). */
+static void record_rhs(float* rhs_out, const float* state, const float* acc, int64_t n) {
+    if (!rhs_out) return;
+    for (int64_t i = 0; i < n; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            rhs_out[6 * i + a] = state[6 * i + 3 + a];
+            rhs_out[6 * i + 3 + a] = acc[3 * i + a];
+        }
+    }
+}
+
 int dem_step(const dem_params* p, int64_t n, float* state, const float* radius,
              const float* mass, int32_t* hcnt, int32_t* hpart, float* hxi,
              float* rhs_out, int32_t* picard_used, float* picard_residual,
@@ -427,6 +439,7 @@ int dem_step(const dem_params* p, int64_t n, float* state, const float* radius,
     if (p->integrator == 0) {
         /* reference src/semi_implicit_euler_kernel.cu:4-16 */
         ovf += rhs_pass(p, n, state, radius, mass, &h, acc);
+        record_rhs(rhs_out, state, acc, n);
         for (int64_t i = 0; i < n; ++i) {
             float* s = state + 6 * i;
             for (int a = 0; a < 3; ++a) s[3 + a] = fmaf(dt, acc[3 * i + a], s[3 + a]);
@@ -442,6 +455,7 @@ int dem_step(const dem_params* p, int64_t n, float* state, const float* radius,
         for (int32_t k = 0; k < p->picard_iterations; ++k) {
             h.overflow = 0;
             ovf += rhs_pass(p, n, state, radius, mass, &h, acc);
+            record_rhs(rhs_out, state, acc, n);
             float res = 0.f;
             for (int64_t i = 0; i < n; ++i) {
                 float* s = state + 6 * i;
@@ -466,14 +480,6 @@ int dem_step(const dem_params* p, int64_t n, float* state, const float* radius,
         memcpy(hpart, npart, sizeof(int32_t) * (size_t)n * DEM_HIST_CAP);
         memcpy(hxi, nxi, sizeof(float) * (size_t)n * DEM_HIST_CAP * 3);
         free(ncnt); free(npart); free(nxi);
-    }
-    if (rhs_out) {
-        for (int64_t i = 0; i < n; ++i) {
-            for (int a = 0; a < 3; ++a) {
-                rhs_out[6 * i + a] = state[6 * i + 3 + a];
-                rhs_out[6 * i + 3 + a] = acc[3 * i + a];
-            }
-        }
     }
     free(acc);
     if (picard_used) *picard_used = used;

@@ -1,0 +1,81 @@
+"""The C ABI: every entry point include/world_b200.h declares is exported by
+libworld_b200.so, and argument errors come back as statuses (no device calls)."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT, gpu_present
+from world_b200 import _lib
+from world_b200._lib import check, lib
+
+HEADER = os.path.join(ROOT, "include", "world_b200.h")
+
+
+def declared_symbols() -> list[str]:
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(wd_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_surface():
+    names = declared_symbols()
+    for required in ("wd_create", "wd_step", "wd_get_state", "wd_set_state",
+                     "wd_compute_density_grid", "wd_compute_total_energy", "wd_config_load_yaml"):
+        assert required in names
+    assert len(names) >= 40
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (wd_[a-z0-9_]+)\b", out))
+    missing = [s for s in declared_symbols() if s not in exported]
+    assert not missing, f"declared but not exported: {missing}"
+    for s in declared_symbols():
+        assert hasattr(lib, s)
+
+
+def test_python_binding_covers_the_header():
+    missing = [s for s in declared_symbols() if s not in _lib.SIGNATURES]
+    assert not missing, f"no ctypes signature for: {missing}"
+
+
+def test_null_arguments_are_invalid_not_crashes():
+    assert lib.wd_step(None, 1) == -1
+    assert "bad argument" in _lib.last_error()
+    assert lib.wd_get_state(None, None) == -1
+    assert lib.wd_config_create(None) == -1
+    assert lib.wd_compute_total_energy(None, None) == -1
+    assert lib.wd_destroy(None) == 0
+
+
+def test_config_get_unknown_key_and_small_buffer():
+    cfg = ctypes.c_void_p()
+    check(lib.wd_config_create(ctypes.byref(cfg)))
+    buf = ctypes.create_string_buffer(64)
+    assert lib.wd_config_get(cfg, b"physics", b"nope", buf, 64) == -1
+    assert "unknown key" in _lib.last_error()
+    tiny = ctypes.create_string_buffer(2)
+    assert lib.wd_config_get(cfg, b"initialization", b"type", tiny, 2) == -6
+    lib.wd_config_destroy(cfg)
+
+
+def test_version_string():
+    assert b"sm_100a" in lib.wd_version()
+
+
+@pytest.mark.skipif(gpu_present(), reason="checks the no-device error path")
+def test_create_without_a_device_returns_a_cuda_status():
+    cfg = ctypes.c_void_p()
+    check(lib.wd_config_create(ctypes.byref(cfg)))
+    sim = ctypes.c_void_p()
+    rc = lib.wd_create(cfg, ctypes.byref(sim))
+    assert rc in (-2, -5)
+    assert _lib.last_error()
+    assert not sim.value
+    lib.wd_config_destroy(cfg)

@@ -1,0 +1,154 @@
+"""The ParticleDynamics / C-ABI surface on the GPU: state in and out, dt changes,
+graph and timed launch paths, checkpoint / resume of the tangential history,
+PyTorch zero-copy, diagnostics and their error paths."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from world_b200 import ParticleDynamics, SimConfig, WorldError
+from world_b200._lib import check, lib, ptr
+from world_b200.state_io import initial_state
+
+pytestmark = pytest.mark.gpu
+
+
+def jitter_cfg(**kw):
+    cfg = SimConfig()
+    cfg.init_jitter = 0.3
+    for k, v in kw.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+def test_state_round_trip_and_positions():
+    sim = ParticleDynamics(jitter_cfg())
+    rng = np.random.default_rng(0)
+    st = sim.get_state().reshape(-1, 6)
+    st[:, 3:] = rng.normal(0, 0.1, (sim.n, 3)).astype(np.float32)
+    sim.set_state(st)
+    assert np.array_equal(sim.get_state(), st.reshape(-1))
+    assert np.array_equal(sim.get_positions(), st[:, :3].reshape(-1))
+    sim.advance(10)
+    st2 = sim.get_state()
+    sim.set_state(st2)                  # set after the order has been permuted
+    assert np.array_equal(sim.get_state(), st2)
+
+
+def test_graph_and_timed_paths_are_identical():
+    a = ParticleDynamics(jitter_cfg(kernel_timing=True))
+    b = ParticleDynamics(jitter_cfg(kernel_timing=False))
+    a.advance(120)
+    b.advance(120)
+    assert np.array_equal(a.get_state(), b.get_state())
+    t = a._timings()
+    assert t[0] > 0 and t[1] > 0
+
+
+def test_dt_change_applies_to_next_step(oracle_for):
+    cfg = jitter_cfg(kernel_timing=False)
+    st, _ = initial_state(cfg)
+    sim = ParticleDynamics(cfg)
+    orc = oracle_for(cfg, st)
+    sim.advance(20)
+    orc.step(20)
+    sim.dt = 5e-5
+    orc.p.dt = np.float32(5e-5)
+    sim.advance(20)
+    orc.step(20)
+    assert np.array_equal(sim.get_state(), orc.state)
+    assert sim.time == pytest.approx(20 * 1e-4 + 20 * 5e-5, rel=1e-5)
+
+
+def test_history_checkpoint_resume_is_bit_identical():
+    cfg = jitter_cfg(history=True, kernel_timing=False)
+    a = ParticleDynamics(cfg)
+    a.advance(60)
+    state = a.get_state()
+    hist = a.get_history()
+    assert hist[0].sum() > 0
+    a.advance(60)
+    b = ParticleDynamics(cfg)
+    b.set_state(state)
+    b.set_history(*hist)
+    b.advance(60)
+    assert np.array_equal(a.get_state(), b.get_state())
+
+
+def test_set_history_needs_history_mode():
+    sim = ParticleDynamics(jitter_cfg())
+    cnt, part, xi = sim.get_history()
+    assert cnt.sum() == 0
+    with pytest.raises(WorldError):
+        sim.set_history(cnt, part, xi)
+
+
+def test_torch_zero_copy_and_external_stream():
+    torch = pytest.importorskip("torch")
+    sim = ParticleDynamics(jitter_cfg(kernel_timing=False))
+    t = sim.state_tensor()
+    assert np.array_equal(t.cpu().numpy(), sim.get_state())
+    t[3::6] += 0.25
+    sim.set_state_tensor(t)
+    assert np.array_equal(sim.get_state(), t.cpu().numpy())
+    s = torch.cuda.Stream()
+    check(lib.wd_set_stream(sim.handle, ctypes.c_void_p(s.cuda_stream)))
+    ref = ParticleDynamics(jitter_cfg(kernel_timing=False))
+    ref.set_state(t.cpu().numpy())
+    sim.advance(30)
+    ref.advance(30)
+    assert np.array_equal(sim.get_state(), ref.get_state())
+    check(lib.wd_set_stream(sim.handle, None))
+    dev = torch.empty(3 * sim.n, dtype=torch.float32, device="cuda")
+    check(lib.wd_get_positions_device(sim.handle, ptr(dev)))
+    sim.synchronize()
+    assert np.array_equal(dev.cpu().numpy(), sim.get_positions())
+
+
+def test_is_stable_detects_escape_and_nan():
+    sim = ParticleDynamics()
+    assert sim.is_stable()
+    st = sim.get_state()
+    st[0] = 5.0
+    sim.set_state(st)
+    assert not sim.is_stable()
+    st[0] = np.nan
+    sim.set_state(st)
+    assert not sim.is_stable()
+
+
+def test_max_acceleration_matches_rhs():
+    sim = ParticleDynamics(jitter_cfg())
+    sim.advance(50)
+    a = sim.get_rhs().reshape(-1, 6)[:, 3:]
+    sq = (a[:, 0] * a[:, 0] + a[:, 1] * a[:, 1]).astype(np.float32) + a[:, 2] * a[:, 2]
+    assert sim.compute_max_acceleration() == np.sqrt(sq.astype(np.float32)).max()
+
+
+def test_picard_stats_and_launch_count():
+    cfg = jitter_cfg(time_integrator="backward_euler_picard", picard_iterations=6,
+                     picard_tolerance=1e-7, kernel_timing=False)
+    sim = ParticleDynamics(cfg)
+    sim.advance(5)
+    used, res = sim.picard_stats()
+    assert 1 <= used < 6 and res < 1e-7
+    # 32^3 cells -> 15-bit keys -> 2 radix passes of 8 bits; per iteration: keys,
+    # 3 kernels per pass, runs, gather, contact
+    assert sim.kernels_per_step() == 6 * (4 + 3 * 2)
+
+
+def test_create_errors_are_statuses(tmp_path):
+    cfg = SimConfig()
+    cfg.init_type = "file"
+    cfg.init_state_path = str(tmp_path / "missing.bin")
+    with pytest.raises(WorldError) as e:
+        ParticleDynamics(cfg)
+    assert e.value.status == -3
+    cfg = SimConfig()
+    cfg.particle_material = 7          # no such entry in materials.masses
+    with pytest.raises(WorldError):
+        ParticleDynamics(cfg)
+    with pytest.raises(ValueError):
+        ParticleDynamics(SimConfig(), state=np.zeros((4, 6), np.float32), radius=np.ones(3, np.float32))
