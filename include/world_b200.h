@@ -180,6 +180,25 @@ int wd_set_kernel_timing(wd_sim* sim, int32_t enabled);
 /* Number of kernels one step launches (for launch accounting). */
 int wd_kernels_per_step(const wd_sim* sim, int64_t* kernels);
 
+/* ---- allocation-free CIC deposit (no counterpart in the reference) ---------------
+ * For callers that cannot call cudaMalloc: processes whose device memory is owned by
+ * another framework's allocator (an ML runtime that reserves the GPU's memory up
+ * front, PyTorch's caching allocator holding the pool) and loops that must not
+ * allocate while they run. Same field as wd_compute_density_grid, from caller-owned
+ * device arrays: d_state AoS6 per grain, d_mass per grain (0 skips the grain), the
+ * node-centred grid [lo, hi] with size[a] nodes per axis, d_grid = 4*nodes floats.
+ * The scratch (64-bit accumulators and channel bounds) is one static device array
+ * sized for WD_NOALLOC_MAX_NODES nodes (8 MiB), held by every GPU that loads the
+ * library until the process exits; larger grids return WD_ERR_CAPACITY. The first
+ * call on each device looks that array up (cudaGetSymbolAddress) and should come
+ * before any stream capture. Every call shares the array and clears it first, so
+ * calls that overlap on the GPU (different streams or threads) race. Work is queued
+ * on `stream` (cudaStream_t as void*, NULL = default stream). */
+#define WD_NOALLOC_MAX_NODES (64 * 64 * 64)
+int wd_deposit_grid_noalloc(const float* d_state, const float* d_mass, int64_t n,
+                            const float* lo3, const float* hi3, const int32_t* size3,
+                            float* d_grid, void* stream);
+
 /* ---- parity probes: the reference's public device_neighbors buffer
  * (src/particle_dynamics.h:48-52) and its cell mapping -------------------------- */
 

@@ -16,6 +16,7 @@ WD_OK = 0
 WD_WARN_DEFAULTS = 1
 WD_WARN_UNKNOWN_KEY = 2
 WD_HIST_CAP = 24
+WD_NOALLOC_MAX_NODES = 64 * 64 * 64
 
 _STATUS_NAMES = {
     -1: "WD_ERR_INVALID", -2: "WD_ERR_CUDA", -3: "WD_ERR_IO", -4: "WD_ERR_CONFIG",
@@ -93,6 +94,7 @@ SIGNATURES = {
     "wd_timings": ([_p, _f], c_int),
     "wd_set_kernel_timing": ([_p, c_int32], c_int),
     "wd_kernels_per_step": ([_p, _i64], c_int),
+    "wd_deposit_grid_noalloc": ([_p, _p, c_int64, _p, _p, _p, _p, _p], c_int),
     "wd_debug_cell_keys": ([_p, _p], c_int),
     "wd_debug_sorted": ([_p, _p, _p], c_int),
     "wd_debug_candidates": ([_p, _p, _p, _p, c_int64, _i64], c_int),

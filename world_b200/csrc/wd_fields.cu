@@ -175,3 +175,199 @@ void launch_deposit(int n, const float4* pos, const float4* vel, const float* lo
 }
 
 }  // namespace wd
+
+// ---------------------------------------------------------------------------------
+// Allocation-free variant of the deposit for callers that cannot call cudaMalloc
+// (device memory owned by another framework's allocator, or a loop that must not
+// allocate). Inputs are the caller's own device arrays in the reference's AoS
+// layout; the scratch is the static array below, one per device, never freed.
+// ---------------------------------------------------------------------------------
+#include <mutex>
+#include <string>
+
+#include "../../include/world_b200.h"
+#include "wd_config.h"
+
+namespace {
+
+constexpr long long kNoAllocNodes = WD_NOALLOC_MAX_NODES;
+// 4 channels of 64-bit accumulators, then 2 words holding the four 32-bit bounds.
+static __device__ __align__(256) unsigned long long g_deposit_scratch[4 * kNoAllocNodes + 2];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+void* g_scratch_addr[kMaxDevices] = {};
+
+__global__ void __launch_bounds__(wd::kBlock)
+k_deposit_bounds_aos(int n, const float* __restrict__ state, const float* __restrict__ mass,
+                     uint32_t* __restrict__ bounds) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t b[4] = {0u, 0u, 0u, 0u};
+    if (s < n) {
+        const float m = mass[s];
+        if (m != 0.f) {
+            const float* q = state + 6 * static_cast<int64_t>(s);
+            b[0] = __float_as_uint(fabsf(m));
+            b[1] = __float_as_uint(fabsf(m * q[3]));
+            b[2] = __float_as_uint(fabsf(m * q[4]));
+            b[3] = __float_as_uint(fabsf(m * q[5]));
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        uint32_t x = b[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(0xffffffffu, x, o));
+        if ((threadIdx.x & 31) == 0 && x) atomicMax(&bounds[c], x);
+    }
+}
+
+// Same contributions, scale and per-warp combining as k_deposit; integer sums make
+// the field independent of the order grains arrive in.
+__global__ void __launch_bounds__(wd::kBlock)
+k_deposit_aos(int n, const float* __restrict__ state, const float* __restrict__ mass,
+              wd::DepositGeom g, const uint32_t* __restrict__ bounds,
+              unsigned long long* __restrict__ acc) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nodes = static_cast<int64_t>(g.size[0]) * g.size[1] * g.size[2];
+    double scale[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) scale[c] = wd::channel_scale(n, bounds[c]);
+    bool active = s < n;
+    float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float m = 0.f;
+    if (active) {
+        const float* q = state + 6 * static_cast<int64_t>(s);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) p[a] = q[a];
+        m = mass[s];
+        active = m != 0.f;
+    }
+    int ix[2] = {0, 0}, iy[2] = {0, 0}, iz[2] = {0, 0};
+    float wx[2] = {0.f, 0.f}, wy[2] = {0.f, 0.f}, wz[2] = {0.f, 0.f};
+    const float mom[3] = {m * p[3], m * p[4], m * p[5]};
+    if (active) {
+        wd::axis_weights(p[0], g.lo[0], g.hi[0], g.size[0], ix[0], ix[1], wx[0], wx[1]);
+        wd::axis_weights(p[1], g.lo[1], g.hi[1], g.size[1], iy[0], iy[1], wy[0], wy[1]);
+        wd::axis_weights(p[2], g.lo[2], g.hi[2], g.size[2], iz[0], iz[1], wz[0], wz[1]);
+    }
+#pragma unroll
+    for (int cx = 0; cx < 2; ++cx)
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+            for (int cz = 0; cz < 2; ++cz) {
+                const float w = wx[cx] * wy[cy] * wz[cz];
+                const bool live = active && w != 0.f;
+                const long long node =
+                    live ? (static_cast<long long>(ix[cx]) * g.size[1] + iy[cy]) * g.size[2] + iz[cz]
+                         : -1ll;
+                long long q[4] = {0, 0, 0, 0};
+                if (live) {
+                    q[0] = __double2ll_rn(static_cast<double>(m * w) * scale[0]);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        q[a + 1] = __double2ll_rn(static_cast<double>(mom[a] * w) * scale[a + 1]);
+                }
+                const unsigned peers = __match_any_sync(0xffffffffu, node);
+                const int leader = __ffs(peers) - 1;
+                const int lane = threadIdx.x & 31;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    long long sum = 0;
+                    unsigned rest = peers;
+                    while (rest) {
+                        const int src = __ffs(rest) - 1;
+                        rest &= rest - 1u;
+                        sum += __shfl_sync(peers, q[c], src);
+                    }
+                    q[c] = sum;
+                }
+                if (live && lane == leader) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (q[c] != 0)
+                            atomicAdd(&acc[c * nodes + node], static_cast<unsigned long long>(q[c]));
+                }
+            }
+}
+
+// Device address of this device's scratch array, looked up once per device.
+cudaError_t scratch_for_current_device(unsigned long long** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_deposit_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_addr[dev] = p;
+    }
+    *out = static_cast<unsigned long long*>(g_scratch_addr[dev]);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int wd_deposit_grid_noalloc(const float* d_state, const float* d_mass, int64_t n,
+                                       const float* lo3, const float* hi3, const int32_t* size3,
+                                       float* d_grid, void* stream_v) {
+    if (!lo3 || !hi3 || !size3 || !d_grid || (n > 0 && (!d_state || !d_mass))) {
+        wd::set_last_error("wd_deposit_grid_noalloc: NULL argument");
+        return WD_ERR_INVALID;
+    }
+    if (n < 0 || n > (int64_t{1} << 30)) {
+        wd::set_last_error("wd_deposit_grid_noalloc: grain count must be in [0, 2^30]");
+        return WD_ERR_INVALID;
+    }
+    for (int a = 0; a < 3; ++a) {
+        if (size3[a] < 1) {
+            wd::set_last_error("wd_deposit_grid_noalloc: grid sizes must be >= 1");
+            return WD_ERR_INVALID;
+        }
+    }
+    const int64_t nodes = static_cast<int64_t>(size3[0]) * size3[1] * size3[2];
+    if (nodes > kNoAllocNodes) {
+        wd::set_last_error("wd_deposit_grid_noalloc: grid of " + std::to_string(nodes) +
+                           " nodes exceeds the fixed scratch of " +
+                           std::to_string(kNoAllocNodes) + " nodes (64^3)");
+        return WD_ERR_CAPACITY;
+    }
+    unsigned long long* scratch = nullptr;
+    cudaError_t e = scratch_for_current_device(&scratch);
+    if (e != cudaSuccess) {
+        wd::set_last_error(std::string("wd_deposit_grid_noalloc: cudaGetSymbolAddress: ") +
+                           cudaGetErrorString(e));
+        return WD_ERR_CUDA;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream_v);
+    unsigned long long* acc = scratch;
+    uint32_t* bounds = reinterpret_cast<uint32_t*>(scratch + 4 * kNoAllocNodes);
+    wd::DepositGeom g;
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = lo3[a];
+        g.hi[a] = hi3[a];
+        g.size[a] = size3[a];
+    }
+    // the array keeps the previous call's sums: clear what this call reads
+    e = cudaMemsetAsync(bounds, 0, 4 * sizeof(uint32_t), st);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(acc, 0, static_cast<size_t>(4 * nodes) * sizeof(unsigned long long), st);
+    if (e == cudaSuccess && n > 0) {
+        const int ni = static_cast<int>(n);
+        k_deposit_bounds_aos<<<wd::blocks_for(ni), wd::kBlock, 0, st>>>(ni, d_state, d_mass, bounds);
+        k_deposit_aos<<<wd::blocks_for(ni), wd::kBlock, 0, st>>>(ni, d_state, d_mass, g, bounds, acc);
+    }
+    if (e == cudaSuccess) {
+        wd::k_deposit_finish<<<static_cast<int>((4 * nodes + wd::kBlock - 1) / wd::kBlock), wd::kBlock, 0,
+                               st>>>(static_cast<int>(n), nodes, bounds, acc, d_grid);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        wd::set_last_error(std::string("wd_deposit_grid_noalloc: ") + cudaGetErrorString(e));
+        return WD_ERR_CUDA;
+    }
+    return WD_OK;
+}
