@@ -135,8 +135,9 @@ def test_picard_stats_and_launch_count():
     used, res = sim.picard_stats()
     assert 1 <= used < 6 and res < 1e-7
     # 32^3 cells -> 15-bit keys -> 2 radix passes of 8 bits; per iteration: keys,
-    # 3 kernels per pass, runs, gather, contact
-    assert sim.kernels_per_step() == 6 * (4 + 3 * 2)
+    # mover scan, by-id, 3 kernels per radix pass, 3 mover-path kernels, runs,
+    # gather, contact (the idle path of each search returns at once)
+    assert sim.kernels_per_step() == 6 * (9 + 3 * 2)
 
 
 def test_create_errors_are_statuses(tmp_path):

@@ -19,18 +19,34 @@ inline int blocks_for(int64_t n, int block = kBlock) {
     return static_cast<int>((n + block - 1) / block);
 }
 
+// Incremental search: at most this many grains may change cell between searches
+// for the mover path (one-block bitonic sort); more falls back to the radix sort.
+constexpr int kMoverCap = 8192;
+constexpr int kMoverThreads = 1024;
+
 // Buffers of one neighbor search (sorted by (cell key, grain id)).
 struct SearchBuffers {
-    uint32_t* key_by_id;     // n: cell key of grain id
-    int* slot_of_id;         // n: slot of grain id in the source state arrays
-    uint32_t* keys[2];       // n: radix ping-pong
-    uint32_t* vals[2];       // n
-    uint32_t* key_sorted;    // n: sorted keys of the last search (table bookkeeping)
+    uint32_t* key_by_id;     // n: cell key of grain id (radix path)
+    int* slot_of_id;         // n: slot of grain id in the source state arrays (radix path)
+    uint32_t* keys[2];       // n: radix ping-pong; keys[out] = sorted keys
+    uint32_t* vals[2];       // n: vals[out] = grain id of each sorted position
+    uint32_t* table_keys;    // n: sorted keys of the search that last wrote the table
+    uint32_t* slot_keys;     // n: key of each state slot at the last step search
+    uint32_t* newkey;        // n: key of each state slot now
+    uint32_t* moved;         // n/32 words: bit set when a slot's key changed
+    int* blk_cnt;            // movers per 256-slot block
+    int* blk_off;            // exclusive prefix of blk_cnt
+    int* ctrl;               // [0] mover count, [1] 1 = radix path this search
+    unsigned long long* mv_key;  // kMoverCap: (key << 32 | id) of each mover
+    uint32_t* mv_slot;       // kMoverCap: its state slot
+    int* src;                // n: state slot of each sorted position
     uint32_t* tile_counts;   // kRadix * num_tiles
     uint32_t* digit_totals;  // kRadix * max_passes
     int2* table;             // num_cells: [start, end) of each occupied cell
     int num_tiles;
+    int num_blocks;          // ceil(n / kBlock)
     int passes;              // radix passes for the key width
+    int out;                 // index of the radix output buffers
 };
 
 // Picard early exit: kernels return at once when prev_res != nullptr and
@@ -40,10 +56,19 @@ struct Skip {
     float tol;
 };
 
-// keys + radix sort + run table. Leaves sorted keys / ids in
-// keys[out_buf] / vals[out_buf], returns out_buf.
+// Cell keys, sort by (key, id), run table. Leaves sorted keys / ids in
+// keys[sb.out] / vals[sb.out] and the source slot of each position in sb.src;
+// returns sb.out. step_search: the sorted order becomes the state's slot order
+// (the contact kernel writes the state back in it), so slot_keys is updated and
+// the next search can re-sort only the grains that changed cell.
 int launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
-                  Skip skip, uint32_t* zero_res, int zero_res_count, cudaStream_t st);
+                  Skip skip, uint32_t* zero_res, int zero_res_count, bool step_search,
+                  cudaStream_t st);
+
+// One-time kernel attributes (the mover sort's shared memory); call before capture.
+cudaError_t search_prepare();
+// Kernels one search launches for a given number of radix passes.
+int search_kernels(int passes);
 
 // Gather the source state into sorted order (and the Picard snapshot when given),
 // counting cells above capacity.

@@ -1,12 +1,17 @@
-// wd_search.cu -- neighbor search for sm_100a: cell keys, stable LSD radix sort of
-// (cell key, grain id), run table, gather into sorted SoA.
+// wd_search.cu -- neighbor search for sm_100a: cell keys, ordering by (cell key,
+// grain id), run table, gather into sorted SoA.
 //
 // Replaces the reference's four-pass dense bucketing (src/find_neighbors_kernel.cu:
 // 46-161: atomicCAS marks, atomicAdd compaction, atomicAdd slot fill, flat candidate
 // rows of 27*particles_per_cell ints). Here:
-//   * the key of every grain is computed with the reference's cell mapping and
-//     written by grain id, so the sort input is in id order and a stable LSD sort
-//     yields (key, id) order: deterministic, no per-cell capacity, nothing dropped;
+//   * the key of every grain is the reference's cell mapping; grains are ordered by
+//     (key, grain id): deterministic, no per-cell capacity, nothing dropped;
+//   * between steps few grains change cell, so the search re-sorts only those
+//     ("movers": one-block bitonic sort) and merges them into the still-sorted rest
+//     by binary search; the first search, or one with more than kMoverCap movers,
+//     runs a stable LSD radix sort of all keys instead. The choice is made on the
+//     device, so both paths sit in the same CUDA graph and the idle one returns at
+//     once. Both produce the same order;
 //   * the run table is a dense [start, end) per cell, but only the cells of the
 //     previous search are cleared (O(n), not the reference's O(cells) memset);
 //   * no candidate list is materialised: the contact kernel walks the sorted runs.
@@ -28,35 +33,134 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
-// Pass 0 of a search: key of every grain by id, slot of every id, clear the runs
-// of the previous search, zero the per-pass digit totals.
+// Movers among slots [0, q): block prefix plus the bits of the words before q.
+__device__ __forceinline__ int movers_before(const uint32_t* __restrict__ bits,
+                                             const int* __restrict__ blk_off, int q) {
+    const int b = q / kBlock;
+    int c = blk_off[b];
+    const int w0 = b * (kBlock / 32), wq = q >> 5;
+    for (int w = w0; w < wq; ++w) c += __popc(bits[w]);
+    const int r = q & 31;
+    if (r) c += __popc(bits[wq] & ((1u << r) - 1u));
+    return c;
+}
+
+// Search pass 1: key of every state slot, mover bits and per-block mover counts;
+// clear the runs of the previous search; zero the radix digit totals.
 __global__ void __launch_bounds__(kBlock)
-k_keys(DevParams P, const float4* __restrict__ pos, const int* __restrict__ ids,
-       uint32_t* __restrict__ key_by_id, int* __restrict__ slot_of_id,
-       const uint32_t* __restrict__ key_sorted, int2* __restrict__ table,
-       uint32_t* __restrict__ digit_totals, int totals_count, uint32_t* __restrict__ zero_res,
-       int zero_res_count, Skip skip) {
+k_keys(DevParams P, const float4* __restrict__ pos, uint32_t* __restrict__ newkey,
+       uint32_t* __restrict__ moved, int* __restrict__ blk_cnt, int num_blocks,
+       const uint32_t* __restrict__ slot_keys, const uint32_t* __restrict__ table_keys,
+       int2* __restrict__ table, uint32_t* __restrict__ digit_totals, int totals_count,
+       uint32_t* __restrict__ zero_res, int zero_res_count, Skip skip) {
     if (skipped(skip)) return;
+    __shared__ int warp_movers[kBlock / 32];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < totals_count) digit_totals[s] = 0u;
     if (zero_res != nullptr && s < zero_res_count) zero_res[s] = 0u;
-    if (s >= P.n) return;
-    const float4 p = pos[s];
-    int cx, cy, cz;
-    cell_coords(P, p.x, p.y, p.z, cx, cy, cz);
+    bool mv = false;
+    if (s < P.n) {
+        const float4 p = pos[s];
+        int cx, cy, cz;
+        cell_coords(P, p.x, p.y, p.z, cx, cy, cz);
+        const uint32_t key = flat_cell(P, cx, cy, cz);
+        newkey[s] = key;
+        mv = key != slot_keys[s];
+        const uint32_t kp = table_keys[s];
+        if (kp != kNoKey && (s == 0 || table_keys[s - 1] != kp)) table[kp] = make_int2(-1, -1);
+    }
+    const unsigned ballot = __ballot_sync(0xffffffffu, mv);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        if (s < P.n) moved[s >> 5] = ballot;
+        warp_movers[warp] = __popc(ballot);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && blockIdx.x < num_blocks) {
+        int c = 0;
+#pragma unroll
+        for (int w = 0; w < kBlock / 32; ++w) c += warp_movers[w];
+        blk_cnt[blockIdx.x] = c;
+    }
+}
+
+// Block-wide exclusive scan of one value per thread (THREADS threads).
+template <int THREADS>
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t warp_sums[THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < THREADS / 32 ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < THREADS / 32) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = (warp > 0 ? warp_sums[warp - 1] : 0u) + x - v;
+    if (total) *total = warp_sums[THREADS / 32 - 1];
+    __syncthreads();
+    return before;
+}
+
+// Search pass 2 (one block): block offsets of the movers, their count, and the path:
+// ctrl[1] = 1 selects the radix sort (more movers than the bitonic sort holds).
+__global__ void __launch_bounds__(kMoverThreads)
+k_scan_movers(const int* __restrict__ blk_cnt, int* __restrict__ blk_off, int num_blocks,
+              int* __restrict__ ctrl, int force_radix, Skip skip) {
+    if (skipped(skip)) return;
+    const int chunk = (num_blocks + kMoverThreads - 1) / kMoverThreads;
+    const int b0 = threadIdx.x * chunk;
+    uint32_t sum = 0u;
+    for (int b = b0; b < min(b0 + chunk, num_blocks); ++b) sum += static_cast<uint32_t>(blk_cnt[b]);
+    uint32_t total = 0u;
+    uint32_t run = block_exclusive_scan<kMoverThreads>(sum, &total);
+    for (int b = b0; b < min(b0 + chunk, num_blocks); ++b) {
+        const int c = blk_cnt[b];
+        blk_off[b] = static_cast<int>(run);
+        run += static_cast<uint32_t>(c);
+    }
+    if (threadIdx.x == 0) {
+        blk_off[num_blocks] = static_cast<int>(total);
+        ctrl[0] = static_cast<int>(total);
+        ctrl[1] = (force_radix || total > static_cast<uint32_t>(kMoverCap)) ? 1 : 0;
+    }
+}
+
+__device__ __forceinline__ bool radix_idle(const int* ctrl) { return ctrl != nullptr && ctrl[1] == 0; }
+__device__ __forceinline__ bool mover_idle(const int* ctrl) { return ctrl[1] != 0; }
+
+// Radix path: key and slot of every grain by id, so the sort input is in id order
+// and a stable sort yields (key, id) order.
+__global__ void __launch_bounds__(kBlock)
+k_by_id(int n, const int* __restrict__ ids, const uint32_t* __restrict__ newkey,
+        uint32_t* __restrict__ key_by_id, int* __restrict__ slot_of_id,
+        const int* __restrict__ ctrl, Skip skip) {
+    if (skipped(skip) || radix_idle(ctrl)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
     const int i = ids[s];
-    key_by_id[i] = flat_cell(P, cx, cy, cz);
+    key_by_id[i] = newkey[s];
     slot_of_id[i] = s;
-    const uint32_t kp = key_sorted[s];
-    if (kp != kNoKey && (s == 0 || key_sorted[s - 1] != kp)) table[kp] = make_int2(-1, -1);
 }
 
 // Radix pass, step 1: digit histogram of one tile (warp-aggregated shared atomics:
 // nearly sorted input puts most keys of a tile on one digit).
 __global__ void __launch_bounds__(kBlock)
 k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift, int num_tiles,
-            uint32_t* __restrict__ counts, uint32_t* __restrict__ totals, Skip skip) {
-    if (skipped(skip)) return;
+            uint32_t* __restrict__ counts, uint32_t* __restrict__ totals,
+            const int* __restrict__ ctrl, Skip skip) {
+    if (skipped(skip) || radix_idle(ctrl)) return;
     __shared__ uint32_t h[kRadix];
     for (int d = threadIdx.x; d < kRadix; d += blockDim.x) h[d] = 0u;
     __syncthreads();
@@ -78,51 +182,23 @@ k_sort_hist(const uint32_t* __restrict__ keys, int n, int shift, int num_tiles,
     }
 }
 
-// Block-wide exclusive scan of one value per thread (256 threads).
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
-    __shared__ uint32_t warp_sums[kBlock / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_sums[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = lane < kBlock / 32 ? warp_sums[lane] : 0u;
-#pragma unroll
-        for (int o = 1; o < kBlock / 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < kBlock / 32) warp_sums[lane] = w;
-    }
-    __syncthreads();
-    const uint32_t before = (warp > 0 ? warp_sums[warp - 1] : 0u) + x - v;
-    if (total) *total = warp_sums[kBlock / 32 - 1];
-    __syncthreads();
-    return before;
-}
-
 // Radix pass, step 2: one block per digit turns that digit's per-tile counts into
 // global output offsets (digit base + exclusive scan over tiles).
 __global__ void __launch_bounds__(kBlock)
 k_sort_scan(uint32_t* __restrict__ counts, const uint32_t* __restrict__ totals, int num_tiles,
-            Skip skip) {
-    if (skipped(skip)) return;
+            const int* __restrict__ ctrl, Skip skip) {
+    if (skipped(skip) || radix_idle(ctrl)) return;
     const int d = blockIdx.x;
     uint32_t part = 0u;
     for (int t = threadIdx.x; t < d; t += blockDim.x) part += totals[t];
     uint32_t base = 0u;
-    block_exclusive_scan(part, &base);
+    block_exclusive_scan<kBlock>(part, &base);
     uint32_t* col = counts + static_cast<size_t>(d) * num_tiles;
     const int chunk = (num_tiles + kBlock - 1) / kBlock;
     const int t0 = threadIdx.x * chunk;
     uint32_t sum = 0u;
     for (int t = t0; t < min(t0 + chunk, num_tiles); ++t) sum += col[t];
-    uint32_t run = base + block_exclusive_scan(sum, nullptr);
+    uint32_t run = base + block_exclusive_scan<kBlock>(sum, nullptr);
     for (int t = t0; t < min(t0 + chunk, num_tiles); ++t) {
         const uint32_t c = col[t];
         col[t] = run;
@@ -137,8 +213,9 @@ template <bool IOTA>
 __global__ void __launch_bounds__(kBlock)
 k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n,
-               int shift, int num_tiles, const uint32_t* __restrict__ offsets, Skip skip) {
-    if (skipped(skip)) return;
+               int shift, int num_tiles, const uint32_t* __restrict__ offsets,
+               const int* __restrict__ ctrl, Skip skip) {
+    if (skipped(skip) || radix_idle(ctrl)) return;
     constexpr int kWarps = kBlock / 32;
     __shared__ uint32_t wh[kWarps][kRadix];
     __shared__ uint32_t toff[kRadix];
@@ -190,15 +267,121 @@ k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict_
     }
 }
 
-// Run table: [start, end) of every occupied cell, from key changes in sorted order.
+// Mover path, 1: one (key << 32 | id, slot) record per mover, in slot order.
 __global__ void __launch_bounds__(kBlock)
-k_runs(const uint32_t* __restrict__ skey, uint32_t* __restrict__ key_sorted,
-       int2* __restrict__ table, int n, Skip skip) {
+k_movers(int n, const uint32_t* __restrict__ newkey, const int* __restrict__ ids,
+         const uint32_t* __restrict__ moved, const int* __restrict__ blk_off,
+         unsigned long long* __restrict__ mv_key, uint32_t* __restrict__ mv_slot,
+         const int* __restrict__ ctrl, Skip skip) {
+    if (skipped(skip) || mover_idle(ctrl)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n || !((moved[s >> 5] >> (s & 31)) & 1u)) return;
+    const int m = movers_before(moved, blk_off, s);
+    mv_key[m] = (static_cast<unsigned long long>(newkey[s]) << 32) | static_cast<uint32_t>(ids[s]);
+    mv_slot[m] = static_cast<uint32_t>(s);
+}
+
+// Mover path, 2: bitonic sort of the mover records by (key, id) in one block.
+__global__ void __launch_bounds__(kMoverThreads)
+k_sort_movers(unsigned long long* __restrict__ mv_key, uint32_t* __restrict__ mv_slot,
+              const int* __restrict__ ctrl, Skip skip) {
+    if (skipped(skip) || mover_idle(ctrl)) return;
+    const int m = ctrl[0];
+    if (m <= 1) return;
+    extern __shared__ unsigned long long smem[];
+    unsigned long long* k = smem;
+    uint32_t* v = reinterpret_cast<uint32_t*>(smem + kMoverCap);
+    int p = 1;
+    while (p < m) p <<= 1;
+    for (int i = threadIdx.x; i < p; i += blockDim.x) {
+        k[i] = i < m ? mv_key[i] : ~0ull;
+        v[i] = i < m ? mv_slot[i] : 0u;
+    }
+    __syncthreads();
+    for (int size = 2; size <= p; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < p; i += blockDim.x) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const unsigned long long a = k[i], b = k[j];
+                    if ((a > b) == up) {
+                        k[i] = b;
+                        k[j] = a;
+                        const uint32_t t = v[i];
+                        v[i] = v[j];
+                        v[j] = t;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        mv_key[i] = k[i];
+        mv_slot[i] = v[i];
+    }
+}
+
+// Mover path, 3: final position of every grain. A stayer keeps its rank among
+// stayers and moves up by the movers sorted below it; a mover's position is its rank
+// among movers plus the stayers below it (a binary search over the previous order,
+// which is sorted by (key, id), minus the movers in that prefix).
+__global__ void __launch_bounds__(kBlock)
+k_merge(int n, const uint32_t* __restrict__ newkey, const uint32_t* __restrict__ slot_keys,
+        const int* __restrict__ ids, const uint32_t* __restrict__ moved,
+        const int* __restrict__ blk_off, const unsigned long long* __restrict__ mv_key,
+        const uint32_t* __restrict__ mv_slot, uint32_t* __restrict__ skey,
+        uint32_t* __restrict__ sid, int* __restrict__ src, const int* __restrict__ ctrl,
+        Skip skip) {
+    if (skipped(skip) || mover_idle(ctrl)) return;
+    const int m = ctrl[0];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n && !((moved[t >> 5] >> (t & 31)) & 1u)) {
+        const uint32_t k = newkey[t];
+        const uint32_t id = static_cast<uint32_t>(ids[t]);
+        const unsigned long long x = (static_cast<unsigned long long>(k) << 32) | id;
+        int lo = 0, hi = m;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (mv_key[mid] < x) lo = mid + 1; else hi = mid;
+        }
+        const int pos = t - movers_before(moved, blk_off, t) + lo;
+        skey[pos] = k;
+        sid[pos] = id;
+        src[pos] = t;
+    }
+    if (t < m) {
+        const unsigned long long x = mv_key[t];
+        int lo = 0, hi = n;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const unsigned long long y =
+                (static_cast<unsigned long long>(slot_keys[mid]) << 32) | static_cast<uint32_t>(ids[mid]);
+            if (y < x) lo = mid + 1; else hi = mid;
+        }
+        const int pos = t + lo - movers_before(moved, blk_off, lo);
+        skey[pos] = static_cast<uint32_t>(x >> 32);
+        sid[pos] = static_cast<uint32_t>(x & 0xffffffffu);
+        src[pos] = static_cast<int>(mv_slot[t]);
+    }
+}
+
+// Run table: [start, end) of every occupied cell, from key changes in sorted order.
+// Step searches also record the new slot keys; the radix path resolves the source
+// slot of each position here.
+__global__ void __launch_bounds__(kBlock)
+k_runs(const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid,
+       uint32_t* __restrict__ table_keys, uint32_t* __restrict__ slot_keys,
+       int2* __restrict__ table, int n, int* __restrict__ src,
+       const int* __restrict__ slot_of_id, const int* __restrict__ ctrl, Skip skip) {
     if (skipped(skip)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const uint32_t k = skey[s];
-    key_sorted[s] = k;
+    table_keys[s] = k;
+    if (slot_keys) slot_keys[s] = k;
+    if (ctrl[1]) src[s] = slot_of_id[sid[s]];
     int* e = reinterpret_cast<int*>(&table[k]);
     if (s == 0 || skey[s - 1] != k) e[0] = s;
     if (s == n - 1 || skey[s + 1] != k) e[1] = s + 1;
@@ -207,7 +390,7 @@ k_runs(const uint32_t* __restrict__ skey, uint32_t* __restrict__ key_sorted,
 template <bool SNAP, bool SNAP_FROM_STATE>
 __global__ void __launch_bounds__(kBlock)
 k_gather(int n, int ppc, const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid,
-         const int* __restrict__ slot_of_id, const float4* __restrict__ posA,
+         const int* __restrict__ src, const float4* __restrict__ posA,
          const float4* __restrict__ velA, float4* __restrict__ posB, float4* __restrict__ velB,
          int* __restrict__ idsB, const float4* __restrict__ nposA,
          const float4* __restrict__ nvelA, float4* __restrict__ nposB,
@@ -216,12 +399,11 @@ k_gather(int n, int ppc, const uint32_t* __restrict__ skey, const uint32_t* __re
     if (skipped(skip)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const int i = static_cast<int>(sid[s]);
-    const int p = slot_of_id[i];
+    const int p = src[s];
     const float4 x = posA[p], v = velA[p];
     posB[s] = x;
     velB[s] = v;
-    idsB[s] = i;
+    idsB[s] = static_cast<int>(sid[s]);
     if (SNAP) {
         if (SNAP_FROM_STATE) {
             nposB[s] = x;
@@ -238,7 +420,6 @@ k_gather(int n, int ppc, const uint32_t* __restrict__ skey, const uint32_t* __re
     }
 }
 
-// Candidate probes: same traversal as the contact kernel.
 __global__ void __launch_bounds__(kBlock)
 k_cand_count(DevParams P, const float4* __restrict__ pos, const int* __restrict__ ids,
              const int2* __restrict__ table, int* __restrict__ count_by_id) {
@@ -345,14 +526,19 @@ __global__ void k_cell_keys_by_id(DevParams P, const float4* __restrict__ pos,
 }  // namespace
 
 int launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
-                  Skip skip, uint32_t* zero_res, int zero_res_count, cudaStream_t st) {
+                  Skip skip, uint32_t* zero_res, int zero_res_count, bool step_search,
+                  cudaStream_t st) {
     const int n = P.n;
     const int nb = blocks_for(n);
     const int totals = kRadix * sb.passes;
     const int kb = blocks_for(n > totals ? n : totals);
-    k_keys<<<kb, kBlock, 0, st>>>(P, pos, ids, sb.key_by_id, sb.slot_of_id, sb.key_sorted,
-                                  sb.table, sb.digit_totals, totals, zero_res, zero_res_count,
-                                  skip);
+    k_keys<<<kb, kBlock, 0, st>>>(P, pos, sb.newkey, sb.moved, sb.blk_cnt, sb.num_blocks,
+                                  sb.slot_keys, sb.table_keys, sb.table, sb.digit_totals, totals,
+                                  zero_res, zero_res_count, skip);
+    k_scan_movers<<<1, kMoverThreads, 0, st>>>(sb.blk_cnt, sb.blk_off, sb.num_blocks, sb.ctrl, 0,
+                                               skip);
+    // radix path (idle unless ctrl[1])
+    k_by_id<<<nb, kBlock, 0, st>>>(n, ids, sb.newkey, sb.key_by_id, sb.slot_of_id, sb.ctrl, skip);
     int cur = 0;
     const uint32_t* kin = sb.key_by_id;
     const uint32_t* vin = nullptr;
@@ -360,25 +546,41 @@ int launch_search(const DevParams& P, const float4* pos, const int* ids, SearchB
         const int shift = pass * kRadixBits;
         uint32_t* totals_p = sb.digit_totals + kRadix * pass;
         k_sort_hist<<<sb.num_tiles, kBlock, 0, st>>>(kin, n, shift, sb.num_tiles, sb.tile_counts,
-                                                     totals_p, skip);
-        k_sort_scan<<<kRadix, kBlock, 0, st>>>(sb.tile_counts, totals_p, sb.num_tiles, skip);
+                                                     totals_p, sb.ctrl, skip);
+        k_sort_scan<<<kRadix, kBlock, 0, st>>>(sb.tile_counts, totals_p, sb.num_tiles, sb.ctrl, skip);
         if (pass == 0) {
             k_sort_scatter<true><<<sb.num_tiles, kBlock, 0, st>>>(
                 kin, vin, sb.keys[cur], sb.vals[cur], n, shift, sb.num_tiles, sb.tile_counts,
-                skip);
+                sb.ctrl, skip);
         } else {
             k_sort_scatter<false><<<sb.num_tiles, kBlock, 0, st>>>(
                 kin, vin, sb.keys[cur], sb.vals[cur], n, shift, sb.num_tiles, sb.tile_counts,
-                skip);
+                sb.ctrl, skip);
         }
         kin = sb.keys[cur];
         vin = sb.vals[cur];
         cur ^= 1;
     }
     const int out = cur ^ 1;
-    k_runs<<<nb, kBlock, 0, st>>>(sb.keys[out], sb.key_sorted, sb.table, n, skip);
+    sb.out = out;
+    // mover path (idle when ctrl[1])
+    k_movers<<<nb, kBlock, 0, st>>>(n, sb.newkey, ids, sb.moved, sb.blk_off, sb.mv_key, sb.mv_slot,
+                                    sb.ctrl, skip);
+    k_sort_movers<<<1, kMoverThreads, kMoverCap * 12, st>>>(sb.mv_key, sb.mv_slot, sb.ctrl, skip);
+    k_merge<<<nb, kBlock, 0, st>>>(n, sb.newkey, sb.slot_keys, ids, sb.moved, sb.blk_off, sb.mv_key,
+                                   sb.mv_slot, sb.keys[out], sb.vals[out], sb.src, sb.ctrl, skip);
+    k_runs<<<nb, kBlock, 0, st>>>(sb.keys[out], sb.vals[out], sb.table_keys,
+                                  step_search ? sb.slot_keys : nullptr, sb.table, n, sb.src,
+                                  sb.slot_of_id, sb.ctrl, skip);
     return out;
 }
+
+cudaError_t search_prepare() {
+    return cudaFuncSetAttribute(k_sort_movers, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kMoverCap * 12);
+}
+
+int search_kernels(int passes) { return 2 + 1 + 3 * passes + 3 + 1; }
 
 void launch_gather(const DevParams& P, const SearchBuffers& sb, int out_buf,
                    const float4* posA, const float4* velA, float4* posB, float4* velB,
@@ -389,19 +591,17 @@ void launch_gather(const DevParams& P, const SearchBuffers& sb, int out_buf,
     const uint32_t* skey = sb.keys[out_buf];
     const uint32_t* sid = sb.vals[out_buf];
     if (nposB == nullptr) {
-        k_gather<false, false><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.slot_of_id,
-                                                      posA, velA, posB, velB, idsB, nullptr,
-                                                      nullptr, nullptr, nullptr, sb.table,
-                                                      counters, skip);
+        k_gather<false, false><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.src, posA, velA,
+                                                      posB, velB, idsB, nullptr, nullptr, nullptr,
+                                                      nullptr, sb.table, counters, skip);
     } else if (snap_from_state) {
-        k_gather<true, true><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.slot_of_id, posA,
-                                                    velA, posB, velB, idsB, nullptr, nullptr,
-                                                    nposB, nvelB, sb.table, counters, skip);
+        k_gather<true, true><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.src, posA, velA, posB,
+                                                    velB, idsB, nullptr, nullptr, nposB, nvelB,
+                                                    sb.table, counters, skip);
     } else {
-        k_gather<true, false><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.slot_of_id,
-                                                     posA, velA, posB, velB, idsB, nposA,
-                                                     nvelA, nposB, nvelB, sb.table, counters,
-                                                     skip);
+        k_gather<true, false><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.src, posA, velA,
+                                                     posB, velB, idsB, nposA, nvelA, nposB, nvelB,
+                                                     sb.table, counters, skip);
     }
 }
 

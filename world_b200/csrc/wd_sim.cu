@@ -137,7 +137,9 @@ void free_sim(wd_sim* s) {
                     s->idsC, s->npos[0], s->npos[1], s->nvel[0], s->nvel[1], s->acc,
                     s->hist[0], s->hist[1], s->hcnt[0], s->hcnt[1], s->sb.key_by_id,
                     s->sb.slot_of_id, s->sb.keys[0], s->sb.keys[1], s->sb.vals[0],
-                    s->sb.vals[1], s->sb.key_sorted, s->sb.tile_counts, s->sb.digit_totals,
+                    s->sb.vals[1], s->sb.table_keys, s->sb.slot_keys, s->sb.newkey, s->sb.moved,
+                    s->sb.blk_cnt, s->sb.blk_off, s->sb.ctrl, s->sb.mv_key, s->sb.mv_slot,
+                    s->sb.src, s->sb.tile_counts, s->sb.digit_totals,
                     s->sb.table, s->counters, s->picard_res, s->picard_used, s->partials,
                     s->red_out, s->dep_bounds, s->dep_acc, s->dep_out, s->staging,
                     s->cand_offsets, s->cand_count};
@@ -190,7 +192,7 @@ void enqueue_step(wd_sim* s, int parity, cudaStream_t st) {
     fa.counters = s->counters;
     const wd::Skip none{nullptr, 0.f};
     if (!s->picard) {
-        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, none, nullptr, 0, st);
+        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, none, nullptr, 0, true, st);
         s->search_out = out;
         wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr,
                           nullptr, nullptr, nullptr, false, s->counters, none, st);
@@ -200,7 +202,8 @@ void enqueue_step(wd_sim* s, int parity, cudaStream_t st) {
     for (int k = 0; k < s->picard_iters; ++k) {
         const wd::Skip skip{k == 0 ? nullptr : s->picard_res + (k - 1), P.picard_tol};
         const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, skip,
-                                          k == 0 ? s->picard_res : nullptr, s->picard_iters, st);
+                                          k == 0 ? s->picard_res : nullptr, s->picard_iters, true,
+                                          st);
         s->search_out = out;
         const int nb = k & 1;
         wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB,
@@ -273,7 +276,7 @@ int timed_step(wd_sim* s, int parity) {
     if (!s->picard) {
         WD_CUDA(cudaEventRecord(e0, st));
         const wd::Skip none{nullptr, 0.f};
-        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, none, nullptr, 0, st);
+        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, none, nullptr, 0, true, st);
         s->search_out = out;
         wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr,
                           nullptr, nullptr, nullptr, false, s->counters, none, st);
@@ -309,7 +312,8 @@ int ondemand_search(wd_sim* s) {
         WD_CUDA(dalloc(&s->idsC, s->n));
     }
     const wd::Skip none{nullptr, 0.f};
-    const int out = wd::launch_search(s->P, s->posA, s->idsA, s->sb, none, nullptr, 0, s->stream);
+    const int out =
+        wd::launch_search(s->P, s->posA, s->idsA, s->sb, none, nullptr, 0, false, s->stream);
     s->search_out = out;
     wd::launch_gather(s->P, s->sb, out, s->posA, s->velA, s->posC, s->velC, s->idsC, nullptr,
                       nullptr, nullptr, nullptr, false, s->counters, none, s->stream);
@@ -350,8 +354,21 @@ int alloc_sim(wd_sim* s) {
         WD_CUDA(dalloc(&sb.keys[b], n));
         WD_CUDA(dalloc(&sb.vals[b], n));
     }
-    WD_CUDA(dalloc(&sb.key_sorted, n));
-    WD_CUDA(cudaMemset(sb.key_sorted, 0xFF, sizeof(uint32_t) * static_cast<size_t>(n)));
+    WD_CUDA(dalloc(&sb.table_keys, n));
+    WD_CUDA(cudaMemset(sb.table_keys, 0xFF, sizeof(uint32_t) * static_cast<size_t>(n)));
+    WD_CUDA(dalloc(&sb.slot_keys, n));
+    WD_CUDA(cudaMemset(sb.slot_keys, 0xFF, sizeof(uint32_t) * static_cast<size_t>(n)));
+    WD_CUDA(dalloc(&sb.newkey, n));
+    WD_CUDA(dalloc(&sb.moved, (static_cast<size_t>(n) + 31) / 32));
+    sb.num_blocks = wd::blocks_for(n);
+    WD_CUDA(dalloc(&sb.blk_cnt, sb.num_blocks));
+    WD_CUDA(dalloc(&sb.blk_off, static_cast<size_t>(sb.num_blocks) + 1));
+    WD_CUDA(dalloc(&sb.ctrl, 2));
+    WD_CUDA(cudaMemset(sb.ctrl, 0, 2 * sizeof(int)));
+    WD_CUDA(dalloc(&sb.mv_key, wd::kMoverCap));
+    WD_CUDA(dalloc(&sb.mv_slot, wd::kMoverCap));
+    WD_CUDA(dalloc(&sb.src, n));
+    WD_CUDA(wd::search_prepare());
     sb.num_tiles = static_cast<int>((static_cast<int64_t>(n) + wd::kSortTile - 1) / wd::kSortTile);
     const int bits = key_bits(s->num_cells);
     sb.passes = bits > 0 ? (bits + wd::kRadixBits - 1) / wd::kRadixBits : 1;
@@ -890,8 +907,7 @@ int wd_set_kernel_timing(wd_sim* sim, int32_t enabled) {
 int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
     wd_sim* sim = const_cast<wd_sim*>(sim_c);
     if (!sim || !kernels) return fail(WD_ERR_INVALID, "wd_kernels_per_step: NULL argument");
-    const int per_search = 2 + 3 * sim->sb.passes;  // keys, 3 per radix pass, runs
-    const int per_iter = per_search + 2;            // gather, contact
+    const int per_iter = wd::search_kernels(sim->sb.passes) + 2;  // + gather, contact
     *kernels = static_cast<int64_t>(per_iter) * sim->picard_iters;
     return WD_OK;
 }
