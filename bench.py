@@ -58,6 +58,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--phase-steps", type=int, default=50)
+    ap.add_argument("--direct", action="store_true",
+                    help="launch each step's kernels directly instead of as one CUDA graph "
+                         "(for per-kernel profilers, which cannot see inside graphs with "
+                         "conditional nodes)")
     return ap.parse_args()
 
 
@@ -243,7 +247,7 @@ def run_ours(args) -> int:
 
     scene = scene_for(args.workload, n=args.grains, seed=12345 + rank)
     sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
-    sim.set_kernel_timing(False)
+    sim.set_kernel_timing(args.direct)
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -258,6 +262,7 @@ def run_ours(args) -> int:
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     torch.cuda.synchronize()
+    radix0, radix_each = sim.radix_search_count()
     barrier()
     for k in range(args.steps):
         flush.fill_(float(k))
@@ -268,6 +273,8 @@ def run_ours(args) -> int:
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop() if sampler else None
+    radix_searches = sim.radix_search_count()[0] - radix0
+    launches = sim.kernels_per_step() * args.steps + radix_searches * radix_each
     local_ms = sum(a.elapsed_time(b) for a, b in ev)
     total_ms = max_over_ranks(local_ms)
     value = n * world * args.steps / (total_ms / 1e3)
@@ -281,7 +288,7 @@ def run_ours(args) -> int:
         sim.take_step()
     sim.synchronize()
     t1 = sim._timings()
-    sim.set_kernel_timing(False)
+    sim.set_kernel_timing(args.direct)
     search_ms = float(t1[0] - t0[0]) / args.phase_steps
     contact_ms = float(t1[1] - t0[1]) / args.phase_steps
     cnt, _, _ = sim.get_history()
@@ -337,7 +344,8 @@ def run_ours(args) -> int:
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
                     "d2h_bytes_per_step": 12 * n, "steps": args.e2e_steps},
             "clocks": clocks,
-            "gpu_launches": sim.kernels_per_step() * args.steps,
+            "gpu_launches": launches,
+            "radix_searches_timed": radix_searches,
             "history_entries_per_grain": entries / n,
         }
         print(json.dumps(line), flush=True)

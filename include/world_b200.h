@@ -177,7 +177,11 @@ int wd_timings(wd_sim* sim, float* ms4);
  * src/sim_config.h:165): 1 = direct launches with events per phase, 0 = one graph
  * launch per step. */
 int wd_set_kernel_timing(wd_sim* sim, int32_t enabled);
-/* Number of kernels one step launches (for launch accounting). */
+/* Lifetime count of neighbor searches that ran the full radix sort (first search, or
+ * more grains changing cell than the incremental path takes); *kernels_each
+ * receives the kernels such a search adds. */
+int wd_radix_search_count(wd_sim* sim, int64_t* count, int32_t* kernels_each);
+/* Kernels one step launches on the incremental search path (launch accounting). */
 int wd_kernels_per_step(const wd_sim* sim, int64_t* kernels);
 
 /* ---- allocation-free CIC deposit (no counterpart in the reference) ---------------

@@ -134,10 +134,20 @@ def test_picard_stats_and_launch_count():
     sim.advance(5)
     used, res = sim.picard_stats()
     assert 1 <= used < 6 and res < 1e-7
-    # 32^3 cells -> 15-bit keys -> 2 radix passes of 8 bits; per iteration: keys,
-    # mover scan, by-id, 3 kernels per radix pass, 3 mover-path kernels, runs,
-    # gather, contact (the idle path of each search returns at once)
-    assert sim.kernels_per_step() == 6 * (9 + 3 * 2)
+    # per iteration on the incremental path: keys, mover kernel, merge, gather,
+    # contact; a search on the radix path adds by-id + 3 kernels per pass
+    # (32^3 cells -> 15-bit keys -> 2 passes of 8 bits)
+    assert sim.kernels_per_step() == 6 * 5
+    radix, each = sim.radix_search_count()
+    assert radix == 0 and each == 1 + 3 * 2      # 1000 grains always fit the mover path
+    big = SimConfig()
+    big.cube_length_x = big.cube_length_y = big.cube_length_z = 0.65   # 32^3 grains
+    big.init_jitter = 0.25
+    big.kernel_timing = False
+    sim = ParticleDynamics(big)
+    sim.advance(3)
+    radix, _ = sim.radix_search_count()
+    assert radix == 1        # only the first search (every grain is new) sorts them all
 
 
 def test_create_errors_are_statuses(tmp_path):

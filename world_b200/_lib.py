@@ -93,6 +93,7 @@ SIGNATURES = {
     "wd_history_overflow_count": ([_p, _i64], c_int),
     "wd_timings": ([_p, _f], c_int),
     "wd_set_kernel_timing": ([_p, c_int32], c_int),
+    "wd_radix_search_count": ([_p, _i64, _i32], c_int),
     "wd_kernels_per_step": ([_p, _i64], c_int),
     "wd_deposit_grid_noalloc": ([_p, _p, c_int64, _p, _p, _p, _p, _p], c_int),
     "wd_debug_cell_keys": ([_p, _p], c_int),

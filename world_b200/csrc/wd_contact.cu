@@ -41,12 +41,13 @@ k_force(DevParams P, ForceArgs A, Skip skip) {
         HistRow h;
         if (HIST) {
             h.in = A.hist_in + static_cast<int64_t>(id) * kHistCap;
-            h.in_count = A.hcnt_in[id];
+            h.in_count = A.hcnt_in[s];
             h.out = A.hist_out + static_cast<int64_t>(id) * kHistCap;
             h.out_count = 0;
         }
         wall_forces<HIST>(P, pos, vel, ri, mi, f, h, A.counters);
 
+        const float cut = contact_cutoff_sq(ri, P.rmax);
         int cx, cy, cz;
         cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
         for (int dx = -1; dx <= 1; ++dx) {
@@ -62,7 +63,7 @@ k_force(DevParams P, ForceArgs A, Skip skip) {
                     const float4 pj = __ldg(&A.pos[j]);
                     float3 d;
                     const float ns = pair_norm_sq(pi, pj, d);
-                    if (!maybe_contact(ns, ri, pj.w)) continue;
+                    if (ns > cut) continue;
                     const float norm = sqrtf(ns);
                     const float dist = pair_dist(norm, ri, pj.w);
                     if (!(dist < 0.f)) continue;
@@ -72,7 +73,7 @@ k_force(DevParams P, ForceArgs A, Skip skip) {
                 }
             }
         }
-        if (HIST) A.hcnt_out[id] = h.out_count;
+        if (HIST) A.hcnt_out[s] = h.out_count;
 
         const float3 a = make_float3(f.x / mi, f.y / mi, f.z / mi);
         float3 v1, x1;
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(kBlock)
 k_energy(DevParams P, const float4* __restrict__ pos, const float4* __restrict__ vel,
          const int* __restrict__ ids, const int2* __restrict__ table,
          const float4* __restrict__ hist, const int* __restrict__ hcnt,
-         double* __restrict__ partials) {
+         const int* __restrict__ src, double* __restrict__ partials) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double e = 0.0;
     if (s < P.n) {
@@ -173,7 +174,7 @@ k_energy(DevParams P, const float4* __restrict__ pos, const float4* __restrict__
             }
         }
         if (HIST) {
-            const int c = hcnt[id];
+            const int c = hcnt[src[s]];
             for (int q = 0; q < c; ++q) {
                 const float4 x = hist[static_cast<int64_t>(id) * kHistCap + q];
                 const int partner = __float_as_int(x.w);
@@ -265,11 +266,13 @@ void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip
 int reduction_blocks(int n) { return blocks_for(n > 0 ? n : 1); }
 
 void launch_energy(const DevParams& P, const float4* pos, const float4* vel, const int* ids,
-                   const int2* table, const float4* hist, const int* hcnt, double* partials,
-                   double* out, cudaStream_t st) {
+                   const int2* table, const float4* hist, const int* hcnt, const int* src,
+                   double* partials, double* out, cudaStream_t st) {
     const int nb = reduction_blocks(P.n);
-    if (P.history) k_energy<true><<<nb, kBlock, 0, st>>>(P, pos, vel, ids, table, hist, hcnt, partials);
-    else k_energy<false><<<nb, kBlock, 0, st>>>(P, pos, vel, ids, table, hist, hcnt, partials);
+    if (P.history)
+        k_energy<true><<<nb, kBlock, 0, st>>>(P, pos, vel, ids, table, hist, hcnt, src, partials);
+    else
+        k_energy<false><<<nb, kBlock, 0, st>>>(P, pos, vel, ids, table, hist, hcnt, src, partials);
     k_sum_partials<<<1, kBlock, 0, st>>>(partials, nb, nb, 1, out);
 }
 

@@ -21,6 +21,7 @@ enum Counter : int {
     kCntHistOverflow = 1,   // contacts without a free history slot
     kCntUnstable = 2,       // scratch for is_stable
     kCntMaxAccel = 3,       // scratch for compute_max_acceleration (float bits)
+    kCntRadixSearches = 4,  // searches that took the full radix-sort path
     kNumCounters = 8,
 };
 
@@ -38,6 +39,7 @@ struct DevParams {
     float wall_lo[3], wall_hi[3];
     float clamp_overlap;
     float picard_tol;
+    float rmax;                // largest grain radius (conservative candidate cutoff)
     int history;
     int n;
 };
@@ -204,6 +206,13 @@ __device__ __forceinline__ float pair_dist(float norm, float ri, float rj) {
 __device__ __forceinline__ bool maybe_contact(float ns, float ri, float rj) {
     const float rs = ri + rj;
     return ns <= rs * rs * 1.001f;
+}
+
+// Per-grain form with the scene's largest radius: one compare per candidate, still
+// conservative (the exact dist < 0 test decides).
+__device__ __forceinline__ float contact_cutoff_sq(float ri, float rmax) {
+    const float rs = ri + rmax;
+    return rs * rs * 1.001f;
 }
 
 // One pair contact: reference src/compute_rhs_kernel.cu:150-204 (dist < 0 branch).

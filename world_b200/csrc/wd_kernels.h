@@ -56,27 +56,41 @@ struct Skip {
     float tol;
 };
 
-// Cell keys, sort by (key, id), run table. Leaves sorted keys / ids in
-// keys[sb.out] / vals[sb.out] and the source slot of each position in sb.src;
-// returns sb.out. step_search: the sorted order becomes the state's slot order
-// (the contact kernel writes the state back in it), so slot_keys is updated and
-// the next search can re-sort only the grains that changed cell.
-int launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
-                  Skip skip, uint32_t* zero_res, int zero_res_count, bool step_search,
-                  cudaStream_t st);
+// A search orders the state slots by (cell key, grain id) into keys[out] (sorted
+// keys), vals[out] (grain ids) and src (source slot of each position). It has three
+// parts, split so a CUDA graph can put the radix path under a conditional node:
+//   head  -- keys of every slot, mover bits, and the one-block mover kernel, which
+//            picks the path (ctrl[1]) and sets `cond` when use_cond;
+//   radix -- stable LSD radix sort of all keys (runs when ctrl[1]);
+//   merge -- merges the sorted movers into the still-sorted rest (idle when ctrl[1]).
+void launch_search_head(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
+                        Skip skip, uint32_t* zero_res, int zero_res_count, bool use_cond,
+                        cudaGraphConditionalHandle cond, unsigned long long* counters,
+                        cudaStream_t st);
+void launch_search_radix(const DevParams& P, const int* ids, SearchBuffers& sb, Skip skip,
+                         cudaStream_t st);
+void launch_search_merge(const DevParams& P, const int* ids, SearchBuffers& sb, Skip skip,
+                         cudaStream_t st);
+// All three parts in stream order (outside graph capture).
+void launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
+                   Skip skip, uint32_t* zero_res, int zero_res_count,
+                   unsigned long long* counters, cudaStream_t st);
 
-// One-time kernel attributes (the mover sort's shared memory); call before capture.
+// One-time kernel attributes (the mover kernel's shared memory); call before capture.
 cudaError_t search_prepare();
-// Kernels one search launches for a given number of radix passes.
-int search_kernels(int passes);
+// Index of the radix output buffers for a number of passes.
+int radix_output(int passes);
 
 // Gather the source state into sorted order (and the Picard snapshot when given),
-// counting cells above capacity.
-void launch_gather(const DevParams& P, const SearchBuffers& sb, int out_buf,
-                   const float4* posA, const float4* velA, float4* posB, float4* velB,
-                   int* idsB, const float4* nposA, const float4* nvelA, float4* nposB,
-                   float4* nvelB, bool snap_from_state, unsigned long long* counters,
-                   Skip skip, cudaStream_t st);
+// fused with the run table. History counts travel with the state in slot order:
+// cnt_dst[p] = cnt_src[src[p]] (both NULL without history). step_search: the sorted
+// order becomes the state's slot order, so the slot keys are recorded for the next
+// search's mover test.
+void launch_gather(const DevParams& P, SearchBuffers& sb, const float4* posA,
+                   const float4* velA, float4* posB, float4* velB, int* idsB,
+                   const float4* nposA, const float4* nvelA, float4* nposB, float4* nvelB,
+                   bool snap_from_state, const int* cnt_src, int* cnt_dst, bool step_search,
+                   unsigned long long* counters, Skip skip, cudaStream_t st);
 
 struct ForceArgs {
     const float4* pos; const float4* vel; const int* ids;  // sorted step input
@@ -84,8 +98,10 @@ struct ForceArgs {
     float4* pos_out; float4* vel_out; int* ids_out;        // integrated state
     float4* acc_out;                                       // F/m per slot
     const float4* npos; const float4* nvel;                // Picard x^n, v^n
-    const float4* hist_in; const int* hcnt_in;             // committed history
-    float4* hist_out; int* hcnt_out;                       // new history
+    const float4* hist_in;                                 // committed rows, by grain id
+    const int* hcnt_in;                                    // their counts, by sorted slot
+    float4* hist_out;                                      // new rows, by grain id
+    int* hcnt_out;                                         // new counts, by sorted slot
     unsigned long long* counters;
     uint32_t* res_slot;                                    // Picard residual (bits)
     int* picard_used;
@@ -96,10 +112,11 @@ void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip
                   cudaStream_t st);
 
 // Total energy at the sorted state (after a search): per-block FP64 partials, then
-// a fixed-order final sum into out.
+// a fixed-order final sum into out. hcnt is in state-slot order; src maps each
+// sorted position to its state slot.
 void launch_energy(const DevParams& P, const float4* pos, const float4* vel, const int* ids,
-                   const int2* table, const float4* hist, const int* hcnt, double* partials,
-                   double* out, cudaStream_t st);
+                   const int2* table, const float4* hist, const int* hcnt, const int* src,
+                   double* partials, double* out, cudaStream_t st);
 
 // Candidate probes (CSR by grain id).
 void launch_candidate_count(const DevParams& P, const float4* pos, const int* ids,

@@ -113,30 +113,6 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
     return before;
 }
 
-// Search pass 2 (one block): block offsets of the movers, their count, and the path:
-// ctrl[1] = 1 selects the radix sort (more movers than the bitonic sort holds).
-__global__ void __launch_bounds__(kMoverThreads)
-k_scan_movers(const int* __restrict__ blk_cnt, int* __restrict__ blk_off, int num_blocks,
-              int* __restrict__ ctrl, int force_radix, Skip skip) {
-    if (skipped(skip)) return;
-    const int chunk = (num_blocks + kMoverThreads - 1) / kMoverThreads;
-    const int b0 = threadIdx.x * chunk;
-    uint32_t sum = 0u;
-    for (int b = b0; b < min(b0 + chunk, num_blocks); ++b) sum += static_cast<uint32_t>(blk_cnt[b]);
-    uint32_t total = 0u;
-    uint32_t run = block_exclusive_scan<kMoverThreads>(sum, &total);
-    for (int b = b0; b < min(b0 + chunk, num_blocks); ++b) {
-        const int c = blk_cnt[b];
-        blk_off[b] = static_cast<int>(run);
-        run += static_cast<uint32_t>(c);
-    }
-    if (threadIdx.x == 0) {
-        blk_off[num_blocks] = static_cast<int>(total);
-        ctrl[0] = static_cast<int>(total);
-        ctrl[1] = (force_radix || total > static_cast<uint32_t>(kMoverCap)) ? 1 : 0;
-    }
-}
-
 __device__ __forceinline__ bool radix_idle(const int* ctrl) { return ctrl != nullptr && ctrl[1] == 0; }
 __device__ __forceinline__ bool mover_idle(const int* ctrl) { return ctrl[1] != 0; }
 
@@ -267,35 +243,69 @@ k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict_
     }
 }
 
-// Mover path, 1: one (key << 32 | id, slot) record per mover, in slot order.
-__global__ void __launch_bounds__(kBlock)
-k_movers(int n, const uint32_t* __restrict__ newkey, const int* __restrict__ ids,
-         const uint32_t* __restrict__ moved, const int* __restrict__ blk_off,
-         unsigned long long* __restrict__ mv_key, uint32_t* __restrict__ mv_slot,
-         const int* __restrict__ ctrl, Skip skip) {
-    if (skipped(skip) || mover_idle(ctrl)) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n || !((moved[s >> 5] >> (s & 31)) & 1u)) return;
-    const int m = movers_before(moved, blk_off, s);
-    mv_key[m] = (static_cast<unsigned long long>(newkey[s]) << 32) | static_cast<uint32_t>(ids[s]);
-    mv_slot[m] = static_cast<uint32_t>(s);
-}
-
-// Mover path, 2: bitonic sort of the mover records by (key, id) in one block.
+// Search pass 2, one block: mover offsets per 256-slot block, the mover count and
+// the path. When the movers fit kMoverCap they are compacted from the bit mask (only
+// blocks that have movers are read) and sorted by (key << 32 | id) with a bitonic
+// network in shared memory; otherwise ctrl[1] selects the radix sort, and when the
+// search runs inside a CUDA graph the radix path's conditional node is switched on.
 __global__ void __launch_bounds__(kMoverThreads)
-k_sort_movers(unsigned long long* __restrict__ mv_key, uint32_t* __restrict__ mv_slot,
-              const int* __restrict__ ctrl, Skip skip) {
-    if (skipped(skip) || mover_idle(ctrl)) return;
-    const int m = ctrl[0];
-    if (m <= 1) return;
+k_movers(int n, const int* __restrict__ blk_cnt, int* __restrict__ blk_off, int num_blocks,
+         const uint32_t* __restrict__ moved, const uint32_t* __restrict__ newkey,
+         const int* __restrict__ ids, unsigned long long* __restrict__ mv_key,
+         uint32_t* __restrict__ mv_slot, int* __restrict__ ctrl, int use_cond,
+         cudaGraphConditionalHandle cond, unsigned long long* __restrict__ counters, Skip skip) {
+    if (skipped(skip)) return;
     extern __shared__ unsigned long long smem[];
     unsigned long long* k = smem;
     uint32_t* v = reinterpret_cast<uint32_t*>(smem + kMoverCap);
+    __shared__ int s_full;
+    const int chunk = (num_blocks + kMoverThreads - 1) / kMoverThreads;
+    const int b0 = min(static_cast<int>(threadIdx.x) * chunk, num_blocks);
+    const int b1 = min(b0 + chunk, num_blocks);
+    uint32_t sum = 0u;
+    for (int b = b0; b < b1; ++b) sum += static_cast<uint32_t>(blk_cnt[b]);
+    uint32_t total = 0u;
+    const uint32_t first = block_exclusive_scan<kMoverThreads>(sum, &total);
+    uint32_t run = first;
+    for (int b = b0; b < b1; ++b) {
+        blk_off[b] = static_cast<int>(run);
+        run += static_cast<uint32_t>(blk_cnt[b]);
+    }
+    const int m = static_cast<int>(total);
+    const int full = total > static_cast<uint32_t>(kMoverCap) ? 1 : 0;
+    if (threadIdx.x == 0) {
+        blk_off[num_blocks] = m;
+        ctrl[0] = m;
+        ctrl[1] = full;
+        if (use_cond) cudaGraphSetConditional(cond, static_cast<unsigned>(full));
+        if (full) atomicAdd(&counters[kCntRadixSearches], 1ull);
+        s_full = full;
+    }
+    __syncthreads();
+    if (s_full || m == 0) return;
+    // compaction in slot order
+    run = first;
+    for (int b = b0; b < b1; ++b) {
+        if (blk_cnt[b] == 0) continue;
+        const int w0 = b * (kBlock / 32);
+        for (int w = w0; w < w0 + kBlock / 32 && 32 * w < n; ++w) {
+            uint32_t bits = moved[w];
+            while (bits) {
+                const int lane = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                const int slot = 32 * w + lane;
+                k[run] = (static_cast<unsigned long long>(newkey[slot]) << 32) |
+                         static_cast<uint32_t>(ids[slot]);
+                v[run] = static_cast<uint32_t>(slot);
+                ++run;
+            }
+        }
+    }
     int p = 1;
     while (p < m) p <<= 1;
-    for (int i = threadIdx.x; i < p; i += blockDim.x) {
-        k[i] = i < m ? mv_key[i] : ~0ull;
-        v[i] = i < m ? mv_slot[i] : 0u;
+    for (int i = m + static_cast<int>(threadIdx.x); i < p; i += blockDim.x) {
+        k[i] = ~0ull;
+        v[i] = 0u;
     }
     __syncthreads();
     for (int size = 2; size <= p; size <<= 1) {
@@ -304,9 +314,9 @@ k_sort_movers(unsigned long long* __restrict__ mv_key, uint32_t* __restrict__ mv
                 const int j = i ^ stride;
                 if (j > i) {
                     const bool up = (i & size) == 0;
-                    const unsigned long long a = k[i], b = k[j];
-                    if ((a > b) == up) {
-                        k[i] = b;
+                    const unsigned long long a = k[i], c = k[j];
+                    if ((a > c) == up) {
+                        k[i] = c;
                         k[j] = a;
                         const uint32_t t = v[i];
                         v[i] = v[j];
@@ -323,7 +333,7 @@ k_sort_movers(unsigned long long* __restrict__ mv_key, uint32_t* __restrict__ mv
     }
 }
 
-// Mover path, 3: final position of every grain. A stayer keeps its rank among
+// Mover path, merge: final position of every grain. A stayer keeps its rank among
 // stayers and moves up by the movers sorted below it; a mover's position is its rank
 // among movers plus the stayers below it (a binary search over the previous order,
 // which is sorted by (key, id), minus the movers in that prefix).
@@ -338,16 +348,16 @@ k_merge(int n, const uint32_t* __restrict__ newkey, const uint32_t* __restrict__
     const int m = ctrl[0];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n && !((moved[t >> 5] >> (t & 31)) & 1u)) {
-        const uint32_t k = newkey[t];
+        const uint32_t key = newkey[t];
         const uint32_t id = static_cast<uint32_t>(ids[t]);
-        const unsigned long long x = (static_cast<unsigned long long>(k) << 32) | id;
+        const unsigned long long x = (static_cast<unsigned long long>(key) << 32) | id;
         int lo = 0, hi = m;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
             if (mv_key[mid] < x) lo = mid + 1; else hi = mid;
         }
         const int pos = t - movers_before(moved, blk_off, t) + lo;
-        skey[pos] = k;
+        skey[pos] = key;
         sid[pos] = id;
         src[pos] = t;
     }
@@ -367,43 +377,31 @@ k_merge(int n, const uint32_t* __restrict__ newkey, const uint32_t* __restrict__
     }
 }
 
-// Run table: [start, end) of every occupied cell, from key changes in sorted order.
-// Step searches also record the new slot keys; the radix path resolves the source
-// slot of each position here.
-__global__ void __launch_bounds__(kBlock)
-k_runs(const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid,
-       uint32_t* __restrict__ table_keys, uint32_t* __restrict__ slot_keys,
-       int2* __restrict__ table, int n, int* __restrict__ src,
-       const int* __restrict__ slot_of_id, const int* __restrict__ ctrl, Skip skip) {
-    if (skipped(skip)) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const uint32_t k = skey[s];
-    table_keys[s] = k;
-    if (slot_keys) slot_keys[s] = k;
-    if (ctrl[1]) src[s] = slot_of_id[sid[s]];
-    int* e = reinterpret_cast<int*>(&table[k]);
-    if (s == 0 || skey[s - 1] != k) e[0] = s;
-    if (s == n - 1 || skey[s + 1] != k) e[1] = s + 1;
-}
-
+// Gather into sorted order, fused with the run table: each position copies its grain
+// from its source state slot (the radix path resolves the slot from the grain id),
+// the first and last position of every run write the cell's [start, end), step
+// searches record the new slot keys, and a run longer than particles_per_cell (its
+// first key equals the key ppc positions later) is counted as an overflow.
 template <bool SNAP, bool SNAP_FROM_STATE>
 __global__ void __launch_bounds__(kBlock)
 k_gather(int n, int ppc, const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid,
-         const int* __restrict__ src, const float4* __restrict__ posA,
+         const int* __restrict__ src, const int* __restrict__ slot_of_id,
+         const int* __restrict__ ctrl, const float4* __restrict__ posA,
          const float4* __restrict__ velA, float4* __restrict__ posB, float4* __restrict__ velB,
          int* __restrict__ idsB, const float4* __restrict__ nposA,
          const float4* __restrict__ nvelA, float4* __restrict__ nposB,
-         float4* __restrict__ nvelB, const int2* __restrict__ table,
-         unsigned long long* __restrict__ counters, Skip skip) {
+         float4* __restrict__ nvelB, const int* __restrict__ cnt_src, int* __restrict__ cnt_dst,
+         int2* __restrict__ table, uint32_t* __restrict__ table_keys,
+         uint32_t* __restrict__ slot_keys, unsigned long long* __restrict__ counters, Skip skip) {
     if (skipped(skip)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const int p = src[s];
+    const uint32_t id = sid[s];
+    const int p = ctrl[1] ? slot_of_id[id] : src[s];
     const float4 x = posA[p], v = velA[p];
     posB[s] = x;
     velB[s] = v;
-    idsB[s] = static_cast<int>(sid[s]);
+    idsB[s] = static_cast<int>(id);
     if (SNAP) {
         if (SNAP_FROM_STATE) {
             nposB[s] = x;
@@ -413,13 +411,19 @@ k_gather(int n, int ppc, const uint32_t* __restrict__ skey, const uint32_t* __re
             nvelB[s] = nvelA[p];
         }
     }
+    if (cnt_dst) cnt_dst[s] = cnt_src[p];
     const uint32_t k = skey[s];
+    table_keys[s] = k;
+    if (slot_keys) slot_keys[s] = k;
+    int* e = reinterpret_cast<int*>(&table[k]);
     if (s == 0 || skey[s - 1] != k) {
-        const int len = table[k].y - s;
-        if (len > ppc) atomicAdd(&counters[kCntGridOverflow], 1ull);
+        e[0] = s;
+        if (s + ppc < n && skey[s + ppc] == k) atomicAdd(&counters[kCntGridOverflow], 1ull);
     }
+    if (s == n - 1 || skey[s + 1] != k) e[1] = s + 1;
 }
 
+// Candidate probes: the same traversal as the contact kernel.
 __global__ void __launch_bounds__(kBlock)
 k_cand_count(DevParams P, const float4* __restrict__ pos, const int* __restrict__ ids,
              const int2* __restrict__ table, int* __restrict__ count_by_id) {
@@ -525,20 +529,27 @@ __global__ void k_cell_keys_by_id(DevParams P, const float4* __restrict__ pos,
 
 }  // namespace
 
-int launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
-                  Skip skip, uint32_t* zero_res, int zero_res_count, bool step_search,
-                  cudaStream_t st) {
+void launch_search_head(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
+                        Skip skip, uint32_t* zero_res, int zero_res_count, bool use_cond,
+                        cudaGraphConditionalHandle cond, unsigned long long* counters,
+                        cudaStream_t st) {
     const int n = P.n;
-    const int nb = blocks_for(n);
     const int totals = kRadix * sb.passes;
     const int kb = blocks_for(n > totals ? n : totals);
     k_keys<<<kb, kBlock, 0, st>>>(P, pos, sb.newkey, sb.moved, sb.blk_cnt, sb.num_blocks,
                                   sb.slot_keys, sb.table_keys, sb.table, sb.digit_totals, totals,
                                   zero_res, zero_res_count, skip);
-    k_scan_movers<<<1, kMoverThreads, 0, st>>>(sb.blk_cnt, sb.blk_off, sb.num_blocks, sb.ctrl, 0,
-                                               skip);
-    // radix path (idle unless ctrl[1])
-    k_by_id<<<nb, kBlock, 0, st>>>(n, ids, sb.newkey, sb.key_by_id, sb.slot_of_id, sb.ctrl, skip);
+    k_movers<<<1, kMoverThreads, kMoverCap * 12, st>>>(n, sb.blk_cnt, sb.blk_off, sb.num_blocks,
+                                                       sb.moved, sb.newkey, ids, sb.mv_key,
+                                                       sb.mv_slot, sb.ctrl, use_cond ? 1 : 0,
+                                                       cond, counters, skip);
+}
+
+void launch_search_radix(const DevParams& P, const int* ids, SearchBuffers& sb, Skip skip,
+                         cudaStream_t st) {
+    const int n = P.n;
+    k_by_id<<<blocks_for(n), kBlock, 0, st>>>(n, ids, sb.newkey, sb.key_by_id, sb.slot_of_id,
+                                              sb.ctrl, skip);
     int cur = 0;
     const uint32_t* kin = sb.key_by_id;
     const uint32_t* vin = nullptr;
@@ -561,47 +572,55 @@ int launch_search(const DevParams& P, const float4* pos, const int* ids, SearchB
         vin = sb.vals[cur];
         cur ^= 1;
     }
-    const int out = cur ^ 1;
-    sb.out = out;
-    // mover path (idle when ctrl[1])
-    k_movers<<<nb, kBlock, 0, st>>>(n, sb.newkey, ids, sb.moved, sb.blk_off, sb.mv_key, sb.mv_slot,
-                                    sb.ctrl, skip);
-    k_sort_movers<<<1, kMoverThreads, kMoverCap * 12, st>>>(sb.mv_key, sb.mv_slot, sb.ctrl, skip);
-    k_merge<<<nb, kBlock, 0, st>>>(n, sb.newkey, sb.slot_keys, ids, sb.moved, sb.blk_off, sb.mv_key,
-                                   sb.mv_slot, sb.keys[out], sb.vals[out], sb.src, sb.ctrl, skip);
-    k_runs<<<nb, kBlock, 0, st>>>(sb.keys[out], sb.vals[out], sb.table_keys,
-                                  step_search ? sb.slot_keys : nullptr, sb.table, n, sb.src,
-                                  sb.slot_of_id, sb.ctrl, skip);
-    return out;
+}
+
+void launch_search_merge(const DevParams& P, const int* ids, SearchBuffers& sb, Skip skip,
+                         cudaStream_t st) {
+    const int n = P.n;
+    k_merge<<<blocks_for(n), kBlock, 0, st>>>(n, sb.newkey, sb.slot_keys, ids, sb.moved, sb.blk_off,
+                                              sb.mv_key, sb.mv_slot, sb.keys[sb.out],
+                                              sb.vals[sb.out], sb.src, sb.ctrl, skip);
+}
+
+void launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
+                   Skip skip, uint32_t* zero_res, int zero_res_count,
+                   unsigned long long* counters, cudaStream_t st) {
+    launch_search_head(P, pos, ids, sb, skip, zero_res, zero_res_count, false, 0, counters, st);
+    launch_search_radix(P, ids, sb, skip, st);
+    launch_search_merge(P, ids, sb, skip, st);
 }
 
 cudaError_t search_prepare() {
-    return cudaFuncSetAttribute(k_sort_movers, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(k_movers, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kMoverCap * 12);
 }
 
-int search_kernels(int passes) { return 2 + 1 + 3 * passes + 3 + 1; }
+int radix_output(int passes) { return (passes - 1) & 1; }
 
-void launch_gather(const DevParams& P, const SearchBuffers& sb, int out_buf,
-                   const float4* posA, const float4* velA, float4* posB, float4* velB,
-                   int* idsB, const float4* nposA, const float4* nvelA, float4* nposB,
-                   float4* nvelB, bool snap_from_state, unsigned long long* counters,
-                   Skip skip, cudaStream_t st) {
+void launch_gather(const DevParams& P, SearchBuffers& sb, const float4* posA,
+                   const float4* velA, float4* posB, float4* velB, int* idsB,
+                   const float4* nposA, const float4* nvelA, float4* nposB, float4* nvelB,
+                   bool snap_from_state, const int* cnt_src, int* cnt_dst, bool step_search,
+                   unsigned long long* counters, Skip skip, cudaStream_t st) {
     const int nb = blocks_for(P.n);
-    const uint32_t* skey = sb.keys[out_buf];
-    const uint32_t* sid = sb.vals[out_buf];
+    const uint32_t* skey = sb.keys[sb.out];
+    const uint32_t* sid = sb.vals[sb.out];
+    uint32_t* slot_keys = step_search ? sb.slot_keys : nullptr;
     if (nposB == nullptr) {
-        k_gather<false, false><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.src, posA, velA,
-                                                      posB, velB, idsB, nullptr, nullptr, nullptr,
-                                                      nullptr, sb.table, counters, skip);
+        k_gather<false, false><<<nb, kBlock, 0, st>>>(
+            P.n, P.ppc, skey, sid, sb.src, sb.slot_of_id, sb.ctrl, posA, velA, posB, velB, idsB,
+            nullptr, nullptr, nullptr, nullptr, cnt_src, cnt_dst, sb.table, sb.table_keys,
+            slot_keys, counters, skip);
     } else if (snap_from_state) {
-        k_gather<true, true><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.src, posA, velA, posB,
-                                                    velB, idsB, nullptr, nullptr, nposB, nvelB,
-                                                    sb.table, counters, skip);
+        k_gather<true, true><<<nb, kBlock, 0, st>>>(
+            P.n, P.ppc, skey, sid, sb.src, sb.slot_of_id, sb.ctrl, posA, velA, posB, velB, idsB,
+            nullptr, nullptr, nposB, nvelB, cnt_src, cnt_dst, sb.table, sb.table_keys, slot_keys,
+            counters, skip);
     } else {
-        k_gather<true, false><<<nb, kBlock, 0, st>>>(P.n, P.ppc, skey, sid, sb.src, posA, velA,
-                                                     posB, velB, idsB, nposA, nvelA, nposB, nvelB,
-                                                     sb.table, counters, skip);
+        k_gather<true, false><<<nb, kBlock, 0, st>>>(
+            P.n, P.ppc, skey, sid, sb.src, sb.slot_of_id, sb.ctrl, posA, velA, posB, velB, idsB,
+            nposA, nvelA, nposB, nvelB, cnt_src, cnt_dst, sb.table, sb.table_keys, slot_keys,
+            counters, skip);
     }
 }
 

@@ -77,6 +77,7 @@ struct wd_sim {
 
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t aux_stream = nullptr;   // captures the radix path's conditional body
 
     // sorted SoA: A = state, B = step gather, C = on-demand gather
     float4 *posA = nullptr, *velA = nullptr, *posB = nullptr, *velB = nullptr;
@@ -85,11 +86,12 @@ struct wd_sim {
     float4 *npos[2] = {nullptr, nullptr}, *nvel[2] = {nullptr, nullptr};
     float4* acc = nullptr;
     float4* hist[2] = {nullptr, nullptr};
-    int* hcnt[2] = {nullptr, nullptr};
+    int* hcnt_slot = nullptr;                     // committed counts, state slot order
+    int* hcnt_g = nullptr;                        // gathered counts (semi-implicit Euler)
+    int* hcnt_snap[2] = {nullptr, nullptr};       // step-start counts, permuted (Picard)
     int hist_cur = 0;
 
     wd::SearchBuffers sb{};
-    int search_out = 0;
     uint64_t num_cells = 0;
 
     unsigned long long* counters = nullptr;
@@ -135,7 +137,8 @@ void free_sim(wd_sim* s) {
     destroy_graphs(s);
     void* bufs[] = {s->posA, s->velA, s->posB, s->velB, s->posC, s->velC, s->idsA, s->idsB,
                     s->idsC, s->npos[0], s->npos[1], s->nvel[0], s->nvel[1], s->acc,
-                    s->hist[0], s->hist[1], s->hcnt[0], s->hcnt[1], s->sb.key_by_id,
+                    s->hist[0], s->hist[1], s->hcnt_slot, s->hcnt_g, s->hcnt_snap[0],
+                    s->hcnt_snap[1], s->sb.key_by_id,
                     s->sb.slot_of_id, s->sb.keys[0], s->sb.keys[1], s->sb.vals[0],
                     s->sb.vals[1], s->sb.table_keys, s->sb.slot_keys, s->sb.newkey, s->sb.moved,
                     s->sb.blk_cnt, s->sb.blk_off, s->sb.ctrl, s->sb.mv_key, s->sb.mv_slot,
@@ -148,6 +151,7 @@ void free_sim(wd_sim* s) {
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : s->ev_pending) cudaEventDestroy(e);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    if (s->aux_stream) cudaStreamDestroy(s->aux_stream);
     delete s;
 }
 
@@ -180,35 +184,92 @@ DevParams make_params(const wd::Config& c, int n, float dt) {
     return P;
 }
 
-// One take_step() enqueued on st (captured into the step graph).
-void enqueue_step(wd_sim* s, int parity, cudaStream_t st) {
+// One neighbor search. Inside graph capture the radix path goes into an IF
+// conditional node that the mover kernel switches on only when it is needed, so
+// the common step launches no idle radix kernels; outside capture every kernel is
+// launched and the idle path returns at once.
+cudaError_t enqueue_search(wd_sim* s, wd::Skip skip, uint32_t* zero_res, int zero_res_count,
+                           bool capture, cudaStream_t st) {
     const DevParams& P = s->P;
-    const int hin = parity, hout = parity ^ 1;
+    if (!capture) {
+        wd::launch_search(P, s->posA, s->idsA, s->sb, skip, zero_res, zero_res_count, s->counters, st);
+        return cudaGetLastError();
+    }
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle cond;
+    e = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    wd::launch_search_head(P, s->posA, s->idsA, s->sb, skip, zero_res, zero_res_count, true, cond,
+                           s->counters, st);
+    e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(s->aux_stream, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return e;
+    wd::launch_search_radix(P, s->idsA, s->sb, skip, s->aux_stream);
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(s->aux_stream, &captured);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return e;
+    wd::launch_search_merge(P, s->idsA, s->sb, skip, st);
+    return cudaGetLastError();
+}
+
+// One take_step() enqueued on st (captured into the step graph when `capture`).
+// History rows are indexed by grain id and ping-pong by step parity; their counts
+// travel with the state in slot order (committed in hcnt_slot, gathered into hcnt_g,
+// or for Picard into the permuted step-start snapshots hcnt_snap). `mid`, when given,
+// is recorded between the search and the contact kernel (semi-implicit Euler only).
+cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
+                         cudaEvent_t mid = nullptr) {
+    const DevParams& P = s->P;
+    const bool hist = P.history != 0;
     wd::ForceArgs fa{};
     fa.pos = s->posB; fa.vel = s->velB; fa.ids = s->idsB; fa.table = s->sb.table;
     fa.pos_out = s->posA; fa.vel_out = s->velA; fa.ids_out = s->idsA; fa.acc_out = s->acc;
-    fa.hist_in = s->hist[hin]; fa.hcnt_in = s->hcnt[hin];
-    fa.hist_out = s->hist[hout]; fa.hcnt_out = s->hcnt[hout];
+    fa.hist_in = s->hist[parity];
+    fa.hist_out = s->hist[parity ^ 1];
+    fa.hcnt_out = s->hcnt_slot;
     fa.counters = s->counters;
     const wd::Skip none{nullptr, 0.f};
     if (!s->picard) {
-        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, none, nullptr, 0, true, st);
-        s->search_out = out;
-        wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr,
-                          nullptr, nullptr, nullptr, false, s->counters, none, st);
+        cudaError_t e = enqueue_search(s, none, nullptr, 0, capture, st);
+        if (e != cudaSuccess) return e;
+        wd::launch_gather(P, s->sb, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr, nullptr,
+                          nullptr, nullptr, false, hist ? s->hcnt_slot : nullptr,
+                          hist ? s->hcnt_g : nullptr, true, s->counters, none, st);
+        if (mid) cudaEventRecord(mid, st);
+        fa.hcnt_in = s->hcnt_g;
         wd::launch_force(P, fa, false, none, st);
-        return;
+        return cudaGetLastError();
     }
     for (int k = 0; k < s->picard_iters; ++k) {
         const wd::Skip skip{k == 0 ? nullptr : s->picard_res + (k - 1), P.picard_tol};
-        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, skip,
-                                          k == 0 ? s->picard_res : nullptr, s->picard_iters, true,
-                                          st);
-        s->search_out = out;
+        cudaError_t e = enqueue_search(s, skip, k == 0 ? s->picard_res : nullptr, s->picard_iters,
+                                       capture, st);
+        if (e != cudaSuccess) return e;
         const int nb = k & 1;
-        wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB,
+        const int* cnt_src = k == 0 ? s->hcnt_slot : s->hcnt_snap[nb ^ 1];
+        wd::launch_gather(P, s->sb, s->posA, s->velA, s->posB, s->velB, s->idsB,
                           k == 0 ? nullptr : s->npos[nb ^ 1], k == 0 ? nullptr : s->nvel[nb ^ 1],
-                          s->npos[nb], s->nvel[nb], k == 0, s->counters, skip, st);
+                          s->npos[nb], s->nvel[nb], k == 0, hist ? cnt_src : nullptr,
+                          hist ? s->hcnt_snap[nb] : nullptr, true, s->counters, skip, st);
+        fa.hcnt_in = s->hcnt_snap[nb];
         fa.npos = s->npos[nb];
         fa.nvel = s->nvel[nb];
         fa.res_slot = s->picard_res + k;
@@ -216,6 +277,7 @@ void enqueue_step(wd_sim* s, int parity, cudaStream_t st) {
         fa.iter = k;
         wd::launch_force(P, fa, true, skip, st);
     }
+    return cudaGetLastError();
 }
 
 int build_graphs(wd_sim* s) {
@@ -224,8 +286,13 @@ int build_graphs(wd_sim* s) {
     for (int parity = 0; parity < count; ++parity) {
         cudaGraph_t g = nullptr;
         WD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        enqueue_step(s, parity, s->stream);
-        WD_CUDA(cudaStreamEndCapture(s->stream, &g));
+        const cudaError_t ce = enqueue_step(s, parity, s->stream, true);
+        const cudaError_t ee = cudaStreamEndCapture(s->stream, &g);
+        if (ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            WD_CUDA(ce);
+        }
+        WD_CUDA(ee);
         size_t nodes = 0;
         cudaGraphGetNodes(g, nullptr, &nodes);
         s->kernels_per_step = static_cast<int>(nodes);
@@ -264,39 +331,19 @@ cudaEvent_t take_event(wd_sim* s) {
 }
 
 // Timed step (drivers.kernel_timing): direct launches with events around the
-// search and the contact phase; accumulated lazily, no per-step host sync.
+// search and the contact phase; accumulated lazily, no per-step host sync. Picard
+// interleaves search and contact per iteration, so its whole step counts as contact.
 int timed_step(wd_sim* s, int parity) {
     if (s->ev_pending.size() >= 3 * 256) {
         const int rc = flush_timings(s);
         if (rc) return rc;
     }
-    const DevParams& P = s->P;
     cudaStream_t st = s->stream;
     cudaEvent_t e0 = take_event(s), e1 = take_event(s), e2 = take_event(s);
-    if (!s->picard) {
-        WD_CUDA(cudaEventRecord(e0, st));
-        const wd::Skip none{nullptr, 0.f};
-        const int out = wd::launch_search(P, s->posA, s->idsA, s->sb, none, nullptr, 0, true, st);
-        s->search_out = out;
-        wd::launch_gather(P, s->sb, out, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr,
-                          nullptr, nullptr, nullptr, false, s->counters, none, st);
-        WD_CUDA(cudaEventRecord(e1, st));
-        wd::ForceArgs fa{};
-        fa.pos = s->posB; fa.vel = s->velB; fa.ids = s->idsB; fa.table = s->sb.table;
-        fa.pos_out = s->posA; fa.vel_out = s->velA; fa.ids_out = s->idsA; fa.acc_out = s->acc;
-        fa.hist_in = s->hist[parity]; fa.hcnt_in = s->hcnt[parity];
-        fa.hist_out = s->hist[parity ^ 1]; fa.hcnt_out = s->hcnt[parity ^ 1];
-        fa.counters = s->counters;
-        wd::launch_force(P, fa, false, none, st);
-        WD_CUDA(cudaEventRecord(e2, st));
-    } else {
-        // Picard interleaves search and force per iteration; time the whole step as
-        // contact work and the search share as zero-length.
-        WD_CUDA(cudaEventRecord(e0, st));
-        WD_CUDA(cudaEventRecord(e1, st));
-        enqueue_step(s, parity, st);
-        WD_CUDA(cudaEventRecord(e2, st));
-    }
+    WD_CUDA(cudaEventRecord(e0, st));
+    if (s->picard) WD_CUDA(cudaEventRecord(e1, st));
+    WD_CUDA(enqueue_step(s, parity, st, false, s->picard ? nullptr : e1));
+    WD_CUDA(cudaEventRecord(e2, st));
     WD_CUDA(cudaGetLastError());
     s->ev_pending.push_back(e0);
     s->ev_pending.push_back(e1);
@@ -312,11 +359,10 @@ int ondemand_search(wd_sim* s) {
         WD_CUDA(dalloc(&s->idsC, s->n));
     }
     const wd::Skip none{nullptr, 0.f};
-    const int out =
-        wd::launch_search(s->P, s->posA, s->idsA, s->sb, none, nullptr, 0, false, s->stream);
-    s->search_out = out;
-    wd::launch_gather(s->P, s->sb, out, s->posA, s->velA, s->posC, s->velC, s->idsC, nullptr,
-                      nullptr, nullptr, nullptr, false, s->counters, none, s->stream);
+    wd::launch_search(s->P, s->posA, s->idsA, s->sb, none, nullptr, 0, s->counters, s->stream);
+    wd::launch_gather(s->P, s->sb, s->posA, s->velA, s->posC, s->velC, s->idsC, nullptr, nullptr,
+                      nullptr, nullptr, false, nullptr, nullptr, false, s->counters, none,
+                      s->stream);
     WD_CUDA(cudaGetLastError());
     return WD_OK;
 }
@@ -330,6 +376,7 @@ int sync_stream(wd_sim* s) {
 int alloc_sim(wd_sim* s) {
     const int n = s->n;
     WD_CUDA(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+    WD_CUDA(cudaStreamCreateWithFlags(&s->aux_stream, cudaStreamNonBlocking));
     s->stream = s->own_stream;
     WD_CUDA(dalloc(&s->posA, n)); WD_CUDA(dalloc(&s->velA, n)); WD_CUDA(dalloc(&s->idsA, n));
     WD_CUDA(dalloc(&s->posB, n)); WD_CUDA(dalloc(&s->velB, n)); WD_CUDA(dalloc(&s->idsB, n));
@@ -341,10 +388,14 @@ int alloc_sim(wd_sim* s) {
         }
     }
     if (s->P.history) {
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < 2; ++b)
             WD_CUDA(dalloc(&s->hist[b], static_cast<size_t>(n) * wd::kHistCap));
-            WD_CUDA(dalloc(&s->hcnt[b], n));
-            WD_CUDA(cudaMemset(s->hcnt[b], 0, sizeof(int) * static_cast<size_t>(n)));
+        WD_CUDA(dalloc(&s->hcnt_slot, n));
+        WD_CUDA(cudaMemset(s->hcnt_slot, 0, sizeof(int) * static_cast<size_t>(n)));
+        WD_CUDA(dalloc(&s->hcnt_g, n));
+        if (s->picard) {
+            WD_CUDA(dalloc(&s->hcnt_snap[0], n));
+            WD_CUDA(dalloc(&s->hcnt_snap[1], n));
         }
     }
     wd::SearchBuffers& sb = s->sb;
@@ -372,6 +423,7 @@ int alloc_sim(wd_sim* s) {
     sb.num_tiles = static_cast<int>((static_cast<int64_t>(n) + wd::kSortTile - 1) / wd::kSortTile);
     const int bits = key_bits(s->num_cells);
     sb.passes = bits > 0 ? (bits + wd::kRadixBits - 1) / wd::kRadixBits : 1;
+    sb.out = wd::radix_output(sb.passes);
     WD_CUDA(dalloc(&sb.tile_counts, static_cast<size_t>(wd::kRadix) * sb.num_tiles));
     WD_CUDA(dalloc(&sb.digit_totals, static_cast<size_t>(wd::kRadix) * sb.passes));
     WD_CUDA(dalloc(&sb.table, s->num_cells));
@@ -462,6 +514,9 @@ int create_impl(const wd::Config& cfg, int64_t n64, const float* state,
         }
         s->mass[i] = m;
     }
+    float rmax = 0.f;
+    for (int i = 0; i < s->n; ++i) rmax = fmaxf(rmax, s->radius[i]);
+    s->P.rmax = rmax;
     int rc = alloc_sim(s);
     if (rc == WD_OK) rc = upload_initial(s, state);
     if (rc != WD_OK) {
@@ -737,7 +792,11 @@ int wd_get_history(wd_sim* sim, int32_t* count, int32_t* partner, float* xi) {
     int rc = sync_stream(sim);
     if (rc) return rc;
     std::vector<float4> rows(n * wd::kHistCap);
-    WD_CUDA(cudaMemcpy(count, sim->hcnt[sim->hist_cur], n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    // counts live in state-slot order: map them back to grain ids
+    std::vector<int32_t> slot_count(n), slot_id(n);
+    WD_CUDA(cudaMemcpy(slot_count.data(), sim->hcnt_slot, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    WD_CUDA(cudaMemcpy(slot_id.data(), sim->idsA, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < n; ++k) count[slot_id[k]] = slot_count[k];
     WD_CUDA(cudaMemcpy(rows.data(), sim->hist[sim->hist_cur], rows.size() * sizeof(float4),
                        cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < n; ++i)
@@ -772,7 +831,10 @@ int wd_set_history(wd_sim* sim, const int32_t* count, const int32_t* partner, co
     }
     int rc = sync_stream(sim);
     if (rc) return rc;
-    WD_CUDA(cudaMemcpy(sim->hcnt[sim->hist_cur], count, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    std::vector<int32_t> slot_count(n), slot_id(n);
+    WD_CUDA(cudaMemcpy(slot_id.data(), sim->idsA, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < n; ++k) slot_count[k] = count[slot_id[k]];
+    WD_CUDA(cudaMemcpy(sim->hcnt_slot, slot_count.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
     WD_CUDA(cudaMemcpy(sim->hist[sim->hist_cur], rows.data(), rows.size() * sizeof(float4),
                        cudaMemcpyHostToDevice));
     return WD_OK;
@@ -826,7 +888,7 @@ int wd_compute_total_energy(wd_sim* sim, double* energy) {
     int rc = ondemand_search(sim);
     if (rc) return rc;
     wd::launch_energy(sim->P, sim->posC, sim->velC, sim->idsC, sim->sb.table,
-                      sim->hist[sim->hist_cur], sim->hcnt[sim->hist_cur], sim->partials,
+                      sim->hist[sim->hist_cur], sim->hcnt_slot, sim->sb.src, sim->partials,
                       sim->red_out, sim->stream);
     WD_CUDA(cudaGetLastError());
     WD_CUDA(cudaMemcpyAsync(energy, sim->red_out, sizeof(double), cudaMemcpyDeviceToHost, sim->stream));
@@ -890,6 +952,12 @@ int wd_history_overflow_count(wd_sim* sim, int64_t* count) {
     return read_counter(sim, wd::kCntHistOverflow, count);
 }
 
+int wd_radix_search_count(wd_sim* sim, int64_t* count, int32_t* kernels_each) {
+    if (!sim || !count) return fail(WD_ERR_INVALID, "wd_radix_search_count: NULL argument");
+    if (kernels_each) *kernels_each = 1 + 3 * sim->sb.passes;
+    return read_counter(sim, wd::kCntRadixSearches, count);
+}
+
 int wd_timings(wd_sim* sim, float* ms4) {
     if (!sim || !ms4) return fail(WD_ERR_INVALID, "wd_timings: NULL argument");
     int rc = flush_timings(sim);
@@ -907,8 +975,9 @@ int wd_set_kernel_timing(wd_sim* sim, int32_t enabled) {
 int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
     wd_sim* sim = const_cast<wd_sim*>(sim_c);
     if (!sim || !kernels) return fail(WD_ERR_INVALID, "wd_kernels_per_step: NULL argument");
-    const int per_iter = wd::search_kernels(sim->sb.passes) + 2;  // + gather, contact
-    *kernels = static_cast<int64_t>(per_iter) * sim->picard_iters;
+    // keys, mover kernel, merge, gather, contact per search; a search that takes the
+    // radix path adds 1 + 3 per pass (wd_radix_search_count)
+    *kernels = static_cast<int64_t>(5) * sim->picard_iters;
     return WD_OK;
 }
 
@@ -927,8 +996,8 @@ int wd_debug_sorted(wd_sim* sim, int32_t* keys, int32_t* ids) {
     int rc = ondemand_search(sim);
     if (rc) return rc;
     const size_t bytes = sizeof(int32_t) * static_cast<size_t>(sim->n);
-    WD_CUDA(cudaMemcpyAsync(keys, sim->sb.keys[sim->search_out], bytes, cudaMemcpyDeviceToHost, sim->stream));
-    WD_CUDA(cudaMemcpyAsync(ids, sim->sb.vals[sim->search_out], bytes, cudaMemcpyDeviceToHost, sim->stream));
+    WD_CUDA(cudaMemcpyAsync(keys, sim->sb.keys[sim->sb.out], bytes, cudaMemcpyDeviceToHost, sim->stream));
+    WD_CUDA(cudaMemcpyAsync(ids, sim->sb.vals[sim->sb.out], bytes, cudaMemcpyDeviceToHost, sim->stream));
     return sync_stream(sim);
 }
 

@@ -251,6 +251,13 @@ class ParticleDynamics:
         check(lib.wd_get_stream(self._h, ctypes.byref(s)))
         return int(s.value or 0)
 
+    def radix_search_count(self) -> tuple[int, int]:
+        """(searches that ran the full radix sort, kernels each such search adds)."""
+        c = ctypes.c_int64()
+        k = ctypes.c_int32()
+        check(lib.wd_radix_search_count(self._h, ctypes.byref(c), ctypes.byref(k)))
+        return int(c.value), int(k.value)
+
     def kernels_per_step(self) -> int:
         v = ctypes.c_int64()
         check(lib.wd_kernels_per_step(self._h, ctypes.byref(v)))

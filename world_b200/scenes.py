@@ -146,7 +146,13 @@ def dense_box(n: int = 1 << 24, *, phi: float = 0.55, seed: int = 2024, mu: floa
     vol = box[0] * box[1] * box[2]
     d = (6.0 * phi * vol / (math.pi * n)) ** (1.0 / 3.0)
     a = (2.0 * (math.pi / 6.0) * d ** 3 / phi) ** (1.0 / 3.0)   # BCC: 2 sites per a^3
-    nx, ny, nz = (int(math.floor((L - d) / a)) for L in box)
+    # shrink the cell until the lattice inside the walls holds n sites (the overall
+    # volume fraction stays phi: the lattice just fills the box a little less)
+    while True:
+        nx, ny, nz = (int(math.floor((L - d) / a)) for L in box)
+        if 2 * nx * ny * nz >= n:
+            break
+        a *= 0.998
     base = np.stack(np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij"),
                     axis=-1).reshape(-1, 3)[:, ::-1].astype(np.float64)   # (x, y, z), z-major
     corner = base * a
