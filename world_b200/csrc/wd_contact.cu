@@ -53,12 +53,11 @@ k_force(DevParams P, ForceArgs A, Skip skip) {
         for (int dx = -1; dx <= 1; ++dx) {
             const int nx = cx + dx;
             if (nx < 0 || nx >= P.grid[0]) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int ny = cy + dy;
-                if (ny < 0 || ny >= P.grid[1]) continue;
-                int lo, hi;
-                column_range(P, A.table, nx, ny, cz, lo, hi);
-                for (int j = lo; j < hi; ++j) {
+            int lo[3], hi[3];
+            row_ranges(P, A.table, nx, cy, cz, lo, hi);
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                for (int j = lo[t]; j < hi[t]; ++j) {
                     if (j == s) continue;
                     const float4 pj = __ldg(&A.pos[j]);
                     float3 d;

@@ -254,6 +254,40 @@ __device__ __forceinline__ float contact_energy(float delta, float clamp_d, floa
     return 0.5f * F * clamp_d + F * (delta - clamp_d);
 }
 
+// Slot ranges of the three columns (nx, cy-1 .. cy+1) around cell z = cz: nine run
+// table loads issued together, one latency instead of three. Columns outside the
+// grid come back empty (lo >= hi).
+__device__ __forceinline__ void row_ranges(const DevParams& P, const int2* __restrict__ table,
+                                           int nx, int cy, int cz, int lo[3], int hi[3]) {
+    const uint32_t gy = static_cast<uint32_t>(P.grid[1]), gz = static_cast<uint32_t>(P.grid[2]);
+    int2 e[3][3];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const int ny = cy + t - 1;
+        const bool col_ok = ny >= 0 && ny < P.grid[1];
+        const uint32_t base = (static_cast<uint32_t>(nx) * gy + static_cast<uint32_t>(ny)) * gz;
+#pragma unroll
+        for (int z = 0; z < 3; ++z) {
+            const int zz = cz + z - 1;
+            e[t][z] = (col_ok && zz >= 0 && zz < P.grid[2])
+                          ? __ldg(&table[base + static_cast<uint32_t>(zz)])
+                          : make_int2(-1, -1);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        lo[t] = 0x7fffffff;
+        hi[t] = 0;
+#pragma unroll
+        for (int z = 0; z < 3; ++z) {
+            if (e[t][z].x >= 0) {
+                lo[t] = min(lo[t], e[t][z].x);
+                hi[t] = max(hi[t], e[t][z].y);
+            }
+        }
+    }
+}
+
 // Range of sorted slots covering cells (x, y, z-1 .. z+1): the three runs are
 // consecutive in (key, id) order, so one [lo, hi) spans them in stencil order.
 __device__ __forceinline__ void column_range(const DevParams& P, const int2* __restrict__ table,
