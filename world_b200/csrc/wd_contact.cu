@@ -24,8 +24,11 @@ __device__ __forceinline__ bool skipped(const Skip& s) {
     return s.prev_res != nullptr && s.tol > 0.f && __uint_as_float(*s.prev_res) < s.tol;
 }
 
+// 5 resident blocks of 256 per SM (<= 51 registers): the candidate loop is
+// latency-bound, so occupancy matters more than the few values the rarely taken
+// contact path may keep in local memory.
 template <bool HIST, bool PICARD>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 5)
 k_force(DevParams P, ForceArgs A, Skip skip) {
     if (PICARD && skipped(skip)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -58,11 +61,10 @@ k_force(DevParams P, ForceArgs A, Skip skip) {
 #pragma unroll
             for (int t = 0; t < 3; ++t) {
                 for (int j = lo[t]; j < hi[t]; ++j) {
-                    if (j == s) continue;
                     const float4 pj = __ldg(&A.pos[j]);
                     float3 d;
                     const float ns = pair_norm_sq(pi, pj, d);
-                    if (ns > cut) continue;
+                    if (ns > cut || j == s) continue;
                     const float norm = sqrtf(ns);
                     const float dist = pair_dist(norm, ri, pj.w);
                     if (!(dist < 0.f)) continue;
