@@ -72,11 +72,11 @@ def env_int(name: str, default: int) -> int:
         return default
 
 
-def workload_config(scene, args) -> dict:
+def workload_config(scene, args, grains=None, scenes=None) -> dict:
     c = scene.cfg
-    return {
+    out = {
         "workload": args.workload,
-        "grains": scene.n,
+        "grains": grains if grains is not None else scene.n,
         "integrator": c.time_integrator,
         "mu": c.physics.friction,
         "tangential_history": bool(c.history),
@@ -87,6 +87,12 @@ def workload_config(scene, args) -> dict:
         "dt": c.dt,
         "l2": "flushed (512 MiB write) before every timed step, flush not timed",
     }
+    if scenes is not None:
+        out["scenes"] = scenes
+        out["diameters"] = "uniform [0.9d, 1.1d]"
+        out["collision_grid"] = "per scene (world_b200/scenes.py)"
+        out["mu"] = "per scene" if args.workload == "design_256" else c.physics.friction
+    return out
 
 
 # ------------------------------------------------------------------ clocks -------
@@ -224,9 +230,10 @@ def run_ours(args) -> int:
     import torch
     import torch.distributed as dist
 
-    from world_b200 import ParticleDynamics
+    from world_b200 import ParticleDynamics, SceneBatch
     from world_b200._lib import check, lib, ptr
-    from world_b200.scenes import scene_for
+    from world_b200.batch import shard_scenes
+    from world_b200.scenes import BATCHED_WORKLOADS, ensemble_for, scene_for
 
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
@@ -245,8 +252,18 @@ def run_ours(args) -> int:
         if world > 1:
             dist.barrier()
 
-    scene = scene_for(args.workload, n=args.grains, seed=12345 + rank)
-    sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
+    scenes_total = None
+    if args.workload in BATCHED_WORKLOADS:
+        # scenes shared out over the ranks, balanced by grain count; each rank steps
+        # its share as one batch
+        members = ensemble_for(args.workload)
+        mine = shard_scenes([m.n for m in members], world)[rank]
+        sim = SceneBatch.from_scenes([members[i] for i in mine])
+        scene = members[mine[0]]
+        scenes_total = len(members)
+    else:
+        scene = scene_for(args.workload, n=args.grains, seed=12345 + rank)
+        sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
     sim.set_kernel_timing(args.direct)
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
@@ -280,7 +297,12 @@ def run_ours(args) -> int:
     launches = sim.kernels_per_step() * args.steps + radix_searches * radix_each
     local_ms = sum(a.elapsed_time(b) for a, b in ev)
     total_ms = max_over_ranks(local_ms)
-    value = n * world * args.steps / (total_ms / 1e3)
+    all_grains = n
+    if world > 1:
+        t = torch.tensor([float(n)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        all_grains = int(t.item())
+    value = all_grains * args.steps / (total_ms / 1e3)
 
     # per-phase timing of the same workload for the roofline (direct launches)
     sim.set_kernel_timing(True)
@@ -305,7 +327,7 @@ def run_ours(args) -> int:
     peak, peak_kind = measured_hbm_peak()
 
     # e2e through the C ABI with pinned host buffers
-    h_state = torch.from_numpy(np.ascontiguousarray(scene.state.reshape(-1))).pin_memory()
+    h_state = torch.from_numpy(sim.get_state()).pin_memory()
     h_pos = torch.empty(3 * n, dtype=torch.float32).pin_memory()
     sim.synchronize()
     barrier()
@@ -319,7 +341,7 @@ def run_ours(args) -> int:
     e1.record(stream)
     e1.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = n * world * args.e2e_steps / (e2e_ms / 1e3)
+    e2e_value = all_grains * args.e2e_steps / (e2e_ms / 1e3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -335,7 +357,7 @@ def run_ours(args) -> int:
             "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
-            "config": workload_config(scene, args),
+            "config": workload_config(scene, args, grains=all_grains, scenes=scenes_total),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(args.workload),
                          "kernel": "k_force (contact forces + integrator)",

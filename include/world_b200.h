@@ -94,6 +94,50 @@ int wd_create_from_arrays(const wd_config* cfg, int64_t n, const float* state,
 
 int wd_destroy(wd_sim* sim);
 
+/* ---- batched scenes (extension) --------------------------------------------------
+ * No reference counterpart as one call: it replaces the dataset and ensemble
+ * drivers' loop of one ParticleDynamics per design row (src/dataset.cpp:163-232,
+ * src/chaos.cpp:176-206). num_scenes independent scenes share one handle and
+ * one step: scene k's grains take the grain ids [first_k, first_k + counts[k]) in
+ * every state, positions, rhs and history array; its density field is the
+ * 4 * nodes_k floats that start at float 4 * node_first_k of the handle's grid
+ * (wd_density_grid_nodes gives the sum of nodes_k), laid out channel-major like a
+ * single scene's grid. History partners are global grain ids. Each scene's
+ * results equal its own single-scene run bit for bit. The scenes must share the
+ * time integrator, Picard iteration count, history mode and dt; a batch runs
+ * Picard with a fixed iteration count (picard_tolerance 0). radii / masses may be
+ * NULL (or hold NULL entries) for the configs' defaults; materials likewise. A NULL
+ * states (or a NULL entry) builds that scene from its config's initialization
+ * section, as wd_create does; counts is read only for the scenes given a state. */
+int wd_create_batch(const wd_config* const* cfgs, int32_t num_scenes, const int64_t* counts,
+                    const float* const* states, const int32_t* const* materials,
+                    const float* const* radii, const float* const* masses, wd_sim** out);
+/* Number of scenes (1 for a handle from wd_create / wd_create_from_arrays). */
+int wd_scene_count(const wd_sim* sim, int32_t* scenes);
+/* Grain id range and density-node range of one scene. */
+int wd_scene_range(const wd_sim* sim, int32_t scene, int64_t* first, int64_t* count,
+                   int64_t* node_first, int64_t* nodes);
+/* Per scene: energy (FP64, one value per scene) and momentum (3 per scene). */
+int wd_compute_scene_energies(wd_sim* sim, double* energies);
+int wd_compute_scene_momenta(wd_sim* sim, double* momenta);
+/* Per scene: grid_overflow_count() and is_stable() (src/particle_dynamics.cu:311-347),
+ * the checks the dataset driver makes of each rollout at every checkpoint
+ * (src/dataset.cpp:203-206). A single-scene handle answers for its one scene. */
+int wd_scene_overflow_counts(wd_sim* sim, int64_t* counts);
+int wd_scene_stability(wd_sim* sim, int32_t* stable);
+/* Stop (frozen != 0) or restart one scene of a batch: the step leaves a frozen
+ * scene's grains where they are and drops their tangential history. The dataset
+ * driver stops a diverged rollout this way (src/dataset.cpp:198-208 stops stepping
+ * it). */
+int wd_freeze_scene(wd_sim* sim, int32_t scene, int32_t frozen);
+/* Ensemble divergence of every scene from reference_scene (src/chaos.cpp:47-78,
+ * 190-222), computed on the device from the current state and a fresh density
+ * deposit: metrics3[3k] = sqrt(mean_i |x_i^(k) - x_i^(ref)|^2) over grains with the
+ * same index, metrics3[3k+1] = ||rho^(k) - rho^(ref)|| / ||rho^(ref)|| (mass
+ * channel), metrics3[3k+2] = |com^(k) - com^(ref)| in node units. Every scene needs
+ * the same grain count and density grid. */
+int wd_chaos_metrics(wd_sim* sim, int32_t reference_scene, double* metrics3);
+
 /* ---- stepping: take_step() (src/particle_dynamics.cu:264-281) -------------------- */
 
 /* nsteps x take_step(), launched asynchronously on the handle's stream. */

@@ -79,3 +79,27 @@ def test_create_without_a_device_returns_a_cuda_status():
     assert _lib.last_error()
     assert not sim.value
     lib.wd_config_destroy(cfg)
+
+
+def test_batch_entry_points_take_the_python_argument_forms():
+    """The ctypes signatures accept what world_b200.batch passes (numpy buffers via
+    ptr(), byref scalars); a NULL handle comes back as WD_ERR_INVALID."""
+    import numpy as np
+    from world_b200._lib import ptr
+    d = np.zeros(8, np.float64)
+    i64 = np.zeros(8, np.int64)
+    i32 = np.zeros(8, np.int32)
+    v = [ctypes.c_int64() for _ in range(4)]
+    s = ctypes.c_int32()
+    calls = [
+        lib.wd_compute_scene_energies(None, ptr(d)),
+        lib.wd_compute_scene_momenta(None, ptr(d)),
+        lib.wd_scene_overflow_counts(None, ptr(i64)),
+        lib.wd_scene_stability(None, ptr(i32)),
+        lib.wd_chaos_metrics(None, 0, ptr(d)),
+        lib.wd_freeze_scene(None, 0, 1),
+        lib.wd_scene_count(None, ctypes.byref(s)),
+        lib.wd_scene_range(None, 0, *[ctypes.byref(x) for x in v]),
+        lib.wd_create_batch(None, 0, None, None, None, None, None, ctypes.byref(ctypes.c_void_p())),
+    ]
+    assert all(c == -1 for c in calls), calls

@@ -2,11 +2,13 @@
 
 The compute path is libworld_b200.so (CUDA kernels + C ABI, include/world_b200.h);
 this package is its Python face: SimConfig / load_config with the reference's YAML
-schema, ParticleDynamics with the reference's step interface, seeded scene
-generators, and state / dataset file formats.
+schema, ParticleDynamics with the reference's step interface, SceneBatch (many
+scenes in one step), seeded scene generators, and state / dataset file formats.
 """
 from ._lib import WD_HIST_CAP, WorldError, lib
 from .config import SimConfig, load_config
 from .particle_dynamics import ParticleDynamics
+from .batch import SceneBatch, SceneRange
 
-__all__ = ["ParticleDynamics", "SimConfig", "load_config", "WorldError", "WD_HIST_CAP", "lib"]
+__all__ = ["ParticleDynamics", "SceneBatch", "SceneRange", "SimConfig", "load_config",
+           "WorldError", "WD_HIST_CAP", "lib"]

@@ -36,7 +36,7 @@ def _load() -> ctypes.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             f"libworld_b200.so not found at {LIB_PATH}; build it with "
-            "`python -m world_b200.build` (nvcc, sm_100a)")
+            "`python world_b200/build.py` (nvcc, sm_100a)")
     return ctypes.CDLL(LIB_PATH)
 
 
@@ -61,6 +61,15 @@ SIGNATURES = {
     "wd_initial_state": ([_p, _p, _p, c_int64, _i64], c_int),
     "wd_create": ([_p, POINTER(c_void_p)], c_int),
     "wd_create_from_arrays": ([_p, c_int64, _p, _p, _p, _p, POINTER(c_void_p)], c_int),
+    "wd_create_batch": ([_p, c_int32, _p, _p, _p, _p, _p, POINTER(c_void_p)], c_int),
+    "wd_scene_count": ([_p, POINTER(c_int32)], c_int),
+    "wd_scene_range": ([_p, c_int32, _i64, _i64, _i64, _i64], c_int),
+    "wd_compute_scene_energies": ([_p, _p], c_int),
+    "wd_compute_scene_momenta": ([_p, _p], c_int),
+    "wd_scene_overflow_counts": ([_p, _p], c_int),
+    "wd_scene_stability": ([_p, _p], c_int),
+    "wd_freeze_scene": ([_p, c_int32, c_int32], c_int),
+    "wd_chaos_metrics": ([_p, c_int32, _p], c_int),
     "wd_destroy": ([_p], c_int),
     "wd_step": ([_p, c_int64], c_int),
     "wd_set_dt": ([_p, c_float], c_int),

@@ -26,7 +26,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-fmad=false",
                      "-Xcompiler", "-fPIC,-O2,-fno-fast-math", "-Xptxas", "-O3",
                      f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
-SOURCES = ["wd_search.cu", "wd_contact.cu", "wd_fields.cu", "wd_sim.cu", "wd_config.cpp"]
+BIN = os.path.join(HERE, "bin")
+DRIVERS = ["dataset", "chaos"]
+SOURCES = ["wd_search.cu", "wd_contact.cu", "wd_fields.cu", "wd_ensemble.cu", "wd_sim.cu",
+           "wd_config.cpp"]
 
 
 def nvcc() -> str:
@@ -67,5 +70,30 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     return LIB
 
 
+def build_drivers(verbose: bool = False) -> list[str]:
+    """The dataset and chaos drivers (world_b200/drivers/*.cpp), linked against the
+    library with an rpath to it, into world_b200/bin/."""
+    lib = build(verbose=verbose)
+    os.makedirs(BIN, exist_ok=True)
+    outs = []
+    for name in DRIVERS:
+        src = os.path.join(HERE, "drivers", name + ".cpp")
+        out = os.path.join(BIN, name)
+        deps = [src, lib] + [os.path.join(ROOT, "include", "world_b200", h)
+                             for h in os.listdir(os.path.join(ROOT, "include", "world_b200"))]
+        if not (os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps)):
+            cmd = [shutil.which("g++") or "g++", "-std=c++17", "-O2", "-Wall",
+                   f"-I{os.path.join(ROOT, 'include')}", src, "-o", out,
+                   f"-L{HERE}", "-lworld_b200", "-Wl,-rpath,$ORIGIN/.."]
+            res = subprocess.run(cmd, capture_output=True, text=True)
+            if res.returncode != 0:
+                raise RuntimeError(f"driver build failed: {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+            if verbose:
+                print(f"built {out}")
+        outs.append(out)
+    return outs
+
+
 if __name__ == "__main__":
     build(verbose=True, extra=sys.argv[1:])
+    build_drivers(verbose=True)

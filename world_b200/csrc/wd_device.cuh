@@ -41,8 +41,27 @@ struct DevParams {
     float picard_tol;
     float rmax;                // largest grain radius (conservative candidate cutoff)
     int history;
-    int n;
+    int n;                     // grains (of the scene, in a scene's own entry)
+    uint32_t cell_base;        // first cell key of the scene (0 for a single scene)
+    int dgrid[3];              // CIC nodes per axis
+    int node_base;             // first CIC node of the scene in the batch's field
+    int frozen;                // batch only: the step leaves this scene's grains as they are
 };
+
+// Scenes of a batch: per-scene parameters and the scene of each slot of the arrays a
+// kernel reads. A single scene passes params == nullptr and uses the kernel's own
+// DevParams; batched kernels (template flag BATCH) look each grain's scene up.
+struct SceneTab {
+    const DevParams* params;
+    const int* scene;
+};
+
+template <bool BATCH>
+__device__ __forceinline__ const DevParams& scene_params(const DevParams& P, const SceneTab& T,
+                                                         int slot) {
+    if (BATCH) return T.params[T.scene[slot]];
+    return P;
+}
 
 // reference src/find_neighbors_kernel.cu:11-22. __float2int_rz is cvt.rzi.s32.f32,
 // the conversion static_cast<int>(float) compiles to.
@@ -260,6 +279,7 @@ __device__ __forceinline__ float contact_energy(float delta, float clamp_d, floa
 __device__ __forceinline__ void row_ranges(const DevParams& P, const int2* __restrict__ table,
                                            int nx, int cy, int cz, int lo[3], int hi[3]) {
     const uint32_t gy = static_cast<uint32_t>(P.grid[1]), gz = static_cast<uint32_t>(P.grid[2]);
+    table += P.cell_base;
     int2 e[3][3];
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
@@ -293,7 +313,7 @@ __device__ __forceinline__ void row_ranges(const DevParams& P, const int2* __res
 __device__ __forceinline__ void column_range(const DevParams& P, const int2* __restrict__ table,
                                              int nx, int ny, int cz, int& lo, int& hi) {
     const int zlo = max(cz - 1, 0), zhi = min(cz + 1, P.grid[2] - 1);
-    const uint32_t base = flat_cell(P, nx, ny, 0);
+    const uint32_t base = P.cell_base + flat_cell(P, nx, ny, 0);
     lo = 0x7fffffff;
     hi = 0;
     for (int z = zlo; z <= zhi; ++z) {

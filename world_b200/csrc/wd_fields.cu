@@ -152,6 +152,114 @@ k_deposit_finish(int n, int64_t nodes, const uint32_t* __restrict__ bounds,
     out[t] = static_cast<float>(static_cast<double>(static_cast<long long>(acc[t])) * inv);
 }
 
+// Batched scenes: one field per scene, laid out scene after scene
+// ([scene][4][nodes of that scene]); each grain deposits with its own scene's grid and
+// the channel scale of its scene (bounds and grain count per scene), so a scene's
+// field is bit-identical to the one it gets alone.
+__global__ void __launch_bounds__(kBlock)
+k_deposit_bounds_batch(int n, const float4* __restrict__ vel, SceneTab T,
+                       uint32_t* __restrict__ bounds) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const float4 v = vel[s];
+    const float m = v.w;
+    if (m == 0.f) return;
+    uint32_t* b = bounds + 4 * T.scene[s];
+    atomicMax(&b[0], __float_as_uint(fabsf(m)));
+    atomicMax(&b[1], __float_as_uint(fabsf(m * v.x)));
+    atomicMax(&b[2], __float_as_uint(fabsf(m * v.y)));
+    atomicMax(&b[3], __float_as_uint(fabsf(m * v.z)));
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_deposit_batch(int n, const float4* __restrict__ pos, const float4* __restrict__ vel, SceneTab T,
+                const uint32_t* __restrict__ bounds, unsigned long long* __restrict__ acc) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = s < n;
+    int sc = 0;
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f), v = x;
+    if (active) {
+        sc = T.scene[s];
+        x = pos[s];
+        v = vel[s];
+        active = v.w != 0.f;
+    }
+    const DevParams& Q = T.params[sc];
+    const int64_t nodes = static_cast<int64_t>(Q.dgrid[0]) * Q.dgrid[1] * Q.dgrid[2];
+    unsigned long long* a = acc + 4 * static_cast<int64_t>(Q.node_base);
+    double scale[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) scale[c] = channel_scale(Q.n, bounds[4 * sc + c]);
+    int ix[2] = {0, 0}, iy[2] = {0, 0}, iz[2] = {0, 0};
+    float wx[2] = {0.f, 0.f}, wy[2] = {0.f, 0.f}, wz[2] = {0.f, 0.f};
+    const float m = v.w;
+    const float mom[3] = {m * v.x, m * v.y, m * v.z};
+    if (active) {
+        axis_weights(x.x, Q.lo[0], Q.hi[0], Q.dgrid[0], ix[0], ix[1], wx[0], wx[1]);
+        axis_weights(x.y, Q.lo[1], Q.hi[1], Q.dgrid[1], iy[0], iy[1], wy[0], wy[1]);
+        axis_weights(x.z, Q.lo[2], Q.hi[2], Q.dgrid[2], iz[0], iz[1], wz[0], wz[1]);
+    }
+#pragma unroll
+    for (int cx = 0; cx < 2; ++cx)
+#pragma unroll
+        for (int cy = 0; cy < 2; ++cy)
+#pragma unroll
+            for (int cz = 0; cz < 2; ++cz) {
+                const float w = wx[cx] * wy[cy] * wz[cz];
+                const bool live = active && w != 0.f;
+                const long long node =
+                    live ? (static_cast<long long>(ix[cx]) * Q.dgrid[1] + iy[cy]) * Q.dgrid[2] + iz[cz]
+                         : -1ll;
+                // lanes combine only within one scene: key the match on (scene, node)
+                const long long key = live ? (static_cast<long long>(sc) << 40) | node : -1ll;
+                long long q[4] = {0, 0, 0, 0};
+                if (live) {
+                    q[0] = __double2ll_rn(static_cast<double>(m * w) * scale[0]);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                        q[k + 1] = __double2ll_rn(static_cast<double>(mom[k] * w) * scale[k + 1]);
+                }
+                const unsigned peers = __match_any_sync(0xffffffffu, key);
+                const int leader = __ffs(peers) - 1;
+                const int lane = threadIdx.x & 31;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    long long sum = 0;
+                    unsigned rest = peers;
+                    while (rest) {
+                        const int src = __ffs(rest) - 1;
+                        rest &= rest - 1u;
+                        sum += __shfl_sync(peers, q[c], src);
+                    }
+                    q[c] = sum;
+                }
+                if (live && lane == leader) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (q[c] != 0)
+                            atomicAdd(&a[c * nodes + node], static_cast<unsigned long long>(q[c]));
+                }
+            }
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_deposit_finish_batch(const DevParams* __restrict__ params, int scenes, int64_t total,
+                       const uint32_t* __restrict__ bounds,
+                       const unsigned long long* __restrict__ acc, float* __restrict__ out) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int lo = 0, hi = scenes;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (4 * static_cast<int64_t>(params[mid].node_base) <= t) lo = mid; else hi = mid;
+    }
+    const DevParams& Q = params[lo];
+    const int64_t nodes = static_cast<int64_t>(Q.dgrid[0]) * Q.dgrid[1] * Q.dgrid[2];
+    const int c = static_cast<int>((t - 4 * static_cast<int64_t>(Q.node_base)) / nodes);
+    const double inv = 1.0 / channel_scale(Q.n, bounds[4 * lo + c]);
+    out[t] = static_cast<float>(static_cast<double>(static_cast<long long>(acc[t])) * inv);
+}
+
 }  // namespace
 
 void launch_deposit(int n, const float4* pos, const float4* vel, const float* lo,
@@ -172,6 +280,19 @@ void launch_deposit(int n, const float4* pos, const float4* vel, const float* lo
     }
     k_deposit_finish<<<static_cast<int>((4 * nodes + kBlock - 1) / kBlock), kBlock, 0, st>>>(
         n, nodes, bounds, acc, out);
+}
+
+void launch_deposit_batch(int n, const float4* pos, const float4* vel, SceneTab T, int scenes,
+                          int64_t total_nodes, uint32_t* bounds, unsigned long long* acc,
+                          float* out, cudaStream_t st) {
+    cudaMemsetAsync(bounds, 0, 4 * sizeof(uint32_t) * static_cast<size_t>(scenes), st);
+    cudaMemsetAsync(acc, 0, 4 * total_nodes * sizeof(unsigned long long), st);
+    if (n > 0) {
+        k_deposit_bounds_batch<<<blocks_for(n), kBlock, 0, st>>>(n, vel, T, bounds);
+        k_deposit_batch<<<blocks_for(n), kBlock, 0, st>>>(n, pos, vel, T, bounds, acc);
+    }
+    k_deposit_finish_batch<<<static_cast<int>((4 * total_nodes + kBlock - 1) / kBlock), kBlock, 0,
+                             st>>>(T.params, scenes, 4 * total_nodes, bounds, acc, out);
 }
 
 }  // namespace wd

@@ -63,17 +63,17 @@ struct Skip {
 //            picks the path (ctrl[1]) and sets `cond` when use_cond;
 //   radix -- stable LSD radix sort of all keys (runs when ctrl[1]);
 //   merge -- merges the sorted movers into the still-sorted rest (idle when ctrl[1]).
-void launch_search_head(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
-                        Skip skip, uint32_t* zero_res, int zero_res_count, bool use_cond,
-                        cudaGraphConditionalHandle cond, unsigned long long* counters,
-                        cudaStream_t st);
+void launch_search_head(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
+                        SearchBuffers& sb, Skip skip, uint32_t* zero_res, int zero_res_count,
+                        bool use_cond, cudaGraphConditionalHandle cond,
+                        unsigned long long* counters, cudaStream_t st);
 void launch_search_radix(const DevParams& P, const int* ids, SearchBuffers& sb, Skip skip,
                          cudaStream_t st);
 void launch_search_merge(const DevParams& P, const int* ids, SearchBuffers& sb, Skip skip,
                          cudaStream_t st);
 // All three parts in stream order (outside graph capture).
-void launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
-                   Skip skip, uint32_t* zero_res, int zero_res_count,
+void launch_search(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
+                   SearchBuffers& sb, Skip skip, uint32_t* zero_res, int zero_res_count,
                    unsigned long long* counters, cudaStream_t st);
 
 // One-time kernel attributes (the mover kernel's shared memory); call before capture.
@@ -89,8 +89,10 @@ int radix_output(int passes);
 void launch_gather(const DevParams& P, SearchBuffers& sb, const float4* posA,
                    const float4* velA, float4* posB, float4* velB, int* idsB,
                    const float4* nposA, const float4* nvelA, float4* nposB, float4* nvelB,
-                   bool snap_from_state, const int* cnt_src, int* cnt_dst, bool step_search,
-                   unsigned long long* counters, Skip skip, cudaStream_t st);
+                   bool snap_from_state, const int* cnt_src, int* cnt_dst, const int* scene_src,
+                   int* scene_dst, bool step_search, unsigned long long* counters,
+                   unsigned long long* scene_overflow, const DevParams* scene_params, Skip skip,
+                   cudaStream_t st);
 
 struct ForceArgs {
     const float4* pos; const float4* vel; const int* ids;  // sorted step input
@@ -106,22 +108,36 @@ struct ForceArgs {
     uint32_t* res_slot;                                    // Picard residual (bits)
     int* picard_used;
     int iter;
+    const DevParams* scene_params;                         // batched scenes (or NULL)
+    const int* scene;                                      // scene of each input slot
+    int* scene_out;                                        // scene of each output slot
+};
+
+// Scene segments of the sorted order, for per-scene reductions: seg[S+1] grain
+// offsets (scene s holds sorted positions [seg[s], seg[s+1])), chunk_base[S+1] prefix
+// of ceil(n_s / kBlock).
+struct Segments {
+    const int* seg;
+    const int* chunk_base;
+    int scenes;
+    int total_chunks;
 };
 
 void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip,
                   cudaStream_t st);
 
-// Total energy at the sorted state (after a search): per-block FP64 partials, then
-// a fixed-order final sum into out. hcnt is in state-slot order; src maps each
-// sorted position to its state slot.
-void launch_energy(const DevParams& P, const float4* pos, const float4* vel, const int* ids,
-                   const int2* table, const float4* hist, const int* hcnt, const int* src,
-                   double* partials, double* out, cudaStream_t st);
+// Total energy per scene at the sorted state (after a search): per-grain FP64 sums,
+// then fixed-order per-segment reductions into out[scene]. hcnt is in state-slot
+// order; src maps each sorted position to its state slot.
+void launch_energy(const DevParams& P, SceneTab T, const float4* pos, const float4* vel,
+                   const int* ids, const int2* table, const float4* hist, const int* hcnt,
+                   const int* src, const Segments& g, double* per_grain, double* partials,
+                   double* out, cudaStream_t st);
 
 // Candidate probes (CSR by grain id).
-void launch_candidate_count(const DevParams& P, const float4* pos, const int* ids,
+void launch_candidate_count(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
                             const int2* table, int* count_by_id, cudaStream_t st);
-void launch_candidate_fill(const DevParams& P, const float4* pos, const int* ids,
+void launch_candidate_fill(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
                            const int2* table, const int64_t* offsets_by_id, int* cand,
                            uint8_t* contact, cudaStream_t st);
 
@@ -134,22 +150,38 @@ void launch_rhs_to_aos(int n, const float4* vel_used, const float4* acc, const i
                        float* out6, cudaStream_t st);
 void launch_state_from_aos(int n, const float* in6, float4* pos, float4* vel, const int* ids,
                            cudaStream_t st);
-void launch_cell_keys_by_id(const DevParams& P, const float4* pos, const int* ids,
+void launch_cell_keys_by_id(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
                             int32_t* keys, cudaStream_t st);
 
 // CIC deposit: deterministic fixed-point accumulation (see wd_fields.cu).
 void launch_deposit(int n, const float4* pos, const float4* vel, const float* lo,
                     const float* hi, const int* dgrid, uint32_t* bounds,
                     unsigned long long* acc, float* out, cudaStream_t st);
+// One field per scene, scene after scene; bounds holds 4 words per scene.
+void launch_deposit_batch(int n, const float4* pos, const float4* vel, SceneTab T, int scenes,
+                          int64_t total_nodes, uint32_t* bounds, unsigned long long* acc,
+                          float* out, cudaStream_t st);
 
-// Reductions.
-void launch_momentum(int n, const float4* vel, double* partials, double* out3,
-                     cudaStream_t st);
+// Reductions (per scene: out3[3 * scene + axis]).
+void launch_segment_sums(const double* values, int n, int comps, const Segments& g,
+                         double* partials, double* out, cudaStream_t st);
+void launch_momentum(int n, const float4* vel, const Segments& g, double* per_grain,
+                     double* partials, double* out3, cudaStream_t st);
 void launch_max_accel(int n, const float4* acc, unsigned long long* counters,
                       cudaStream_t st);
-void launch_stability(const DevParams& P, const float4* pos, unsigned long long* counters,
-                      cudaStream_t st);
+// is_stable: sets counters[kCntUnstable]; a batch also flags scene_unstable[scene].
+void launch_stability(const DevParams& P, SceneTab T, const float4* pos,
+                      unsigned long long* counters, int* scene_unstable, cudaStream_t st);
 
 int reduction_blocks(int n);
+
+// Ensemble metrics (wd_ensemble.cu): per scene, the sum over grains of the squared
+// separation from the reference scene's grain with the same index (grain_sums), and
+// the six node sums sum (rho - rho_ref)^2, sum rho_ref^2, sum rho, sum rho*ix,
+// sum rho*iy, sum rho*iz of the mass channel (node_sums[6 * scene + c]).
+void launch_chaos(int n, const float* pos3, const Segments& grains, double* grain_vals,
+                  double* grain_partials, double* grain_sums, int total_nodes, const float* grid,
+                  const Segments& nodes, int ref, int ny, int nz, double* node_vals,
+                  double* node_partials, double* node_sums, cudaStream_t st);
 
 }  // namespace wd

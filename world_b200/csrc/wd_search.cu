@@ -47,8 +47,9 @@ __device__ __forceinline__ int movers_before(const uint32_t* __restrict__ bits,
 
 // Search pass 1: key of every state slot, mover bits and per-block mover counts;
 // clear the runs of the previous search; zero the radix digit totals.
+template <bool BATCH>
 __global__ void __launch_bounds__(kBlock)
-k_keys(DevParams P, const float4* __restrict__ pos, uint32_t* __restrict__ newkey,
+k_keys(DevParams P, SceneTab T, const float4* __restrict__ pos, uint32_t* __restrict__ newkey,
        uint32_t* __restrict__ moved, int* __restrict__ blk_cnt, int num_blocks,
        const uint32_t* __restrict__ slot_keys, const uint32_t* __restrict__ table_keys,
        int2* __restrict__ table, uint32_t* __restrict__ digit_totals, int totals_count,
@@ -60,10 +61,11 @@ k_keys(DevParams P, const float4* __restrict__ pos, uint32_t* __restrict__ newke
     if (zero_res != nullptr && s < zero_res_count) zero_res[s] = 0u;
     bool mv = false;
     if (s < P.n) {
+        const DevParams& Q = scene_params<BATCH>(P, T, s);
         const float4 p = pos[s];
         int cx, cy, cz;
-        cell_coords(P, p.x, p.y, p.z, cx, cy, cz);
-        const uint32_t key = flat_cell(P, cx, cy, cz);
+        cell_coords(Q, p.x, p.y, p.z, cx, cy, cz);
+        const uint32_t key = Q.cell_base + flat_cell(Q, cx, cy, cz);
         newkey[s] = key;
         mv = key != slot_keys[s];
         const uint32_t kp = table_keys[s];
@@ -391,8 +393,11 @@ k_gather(int n, int ppc, const uint32_t* __restrict__ skey, const uint32_t* __re
          int* __restrict__ idsB, const float4* __restrict__ nposA,
          const float4* __restrict__ nvelA, float4* __restrict__ nposB,
          float4* __restrict__ nvelB, const int* __restrict__ cnt_src, int* __restrict__ cnt_dst,
+         const int* __restrict__ scene_src, int* __restrict__ scene_dst,
          int2* __restrict__ table, uint32_t* __restrict__ table_keys,
-         uint32_t* __restrict__ slot_keys, unsigned long long* __restrict__ counters, Skip skip) {
+         uint32_t* __restrict__ slot_keys, unsigned long long* __restrict__ counters,
+         unsigned long long* __restrict__ scene_overflow,
+         const DevParams* __restrict__ scene_params, Skip skip) {
     if (skipped(skip)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
@@ -412,23 +417,31 @@ k_gather(int n, int ppc, const uint32_t* __restrict__ skey, const uint32_t* __re
         }
     }
     if (cnt_dst) cnt_dst[s] = cnt_src[p];
+    if (scene_dst) scene_dst[s] = scene_src[p];
     const uint32_t k = skey[s];
     table_keys[s] = k;
     if (slot_keys) slot_keys[s] = k;
     int* e = reinterpret_cast<int*>(&table[k]);
     if (s == 0 || skey[s - 1] != k) {
         e[0] = s;
-        if (s + ppc < n && skey[s + ppc] == k) atomicAdd(&counters[kCntGridOverflow], 1ull);
+        // a run holds one scene's grains: its own particles_per_cell applies
+        const int cap = scene_params ? scene_params[scene_src[p]].ppc : ppc;
+        if (s + cap < n && skey[s + cap] == k) {
+            atomicAdd(&counters[kCntGridOverflow], 1ull);
+            if (scene_overflow) atomicAdd(&scene_overflow[scene_src[p]], 1ull);
+        }
     }
     if (s == n - 1 || skey[s + 1] != k) e[1] = s + 1;
 }
 
 // Candidate probes: the same traversal as the contact kernel.
+template <bool BATCH>
 __global__ void __launch_bounds__(kBlock)
-k_cand_count(DevParams P, const float4* __restrict__ pos, const int* __restrict__ ids,
+k_cand_count(DevParams P0, SceneTab T, const float4* __restrict__ pos, const int* __restrict__ ids,
              const int2* __restrict__ table, int* __restrict__ count_by_id) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n) return;
+    if (s >= P0.n) return;
+    const DevParams& P = scene_params<BATCH>(P0, T, s);
     const float4 pi = pos[s];
     int cx, cy, cz;
     cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
@@ -447,12 +460,14 @@ k_cand_count(DevParams P, const float4* __restrict__ pos, const int* __restrict_
     count_by_id[ids[s]] = c;
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(kBlock)
-k_cand_fill(DevParams P, const float4* __restrict__ pos, const int* __restrict__ ids,
+k_cand_fill(DevParams P0, SceneTab T, const float4* __restrict__ pos, const int* __restrict__ ids,
             const int2* __restrict__ table, const int64_t* __restrict__ offsets,
             int* __restrict__ cand, uint8_t* __restrict__ contact) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n) return;
+    if (s >= P0.n) return;
+    const DevParams& P = scene_params<BATCH>(P0, T, s);
     const float4 pi = pos[s];
     int cx, cy, cz;
     cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
@@ -517,10 +532,13 @@ __global__ void k_state_from_aos(int n, const float* __restrict__ in, float4* __
     vel[s] = make_float4(q[3], q[4], q[5], vel[s].w);
 }
 
-__global__ void k_cell_keys_by_id(DevParams P, const float4* __restrict__ pos,
+// Cell key of every grain within its own scene's grid, by grain id.
+template <bool BATCH>
+__global__ void k_cell_keys_by_id(DevParams P0, SceneTab T, const float4* __restrict__ pos,
                                   const int* __restrict__ ids, int32_t* __restrict__ keys) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= P.n) return;
+    if (s >= P0.n) return;
+    const DevParams& P = scene_params<BATCH>(P0, T, s);
     const float4 p = pos[s];
     int cx, cy, cz;
     cell_coords(P, p.x, p.y, p.z, cx, cy, cz);
@@ -529,16 +547,22 @@ __global__ void k_cell_keys_by_id(DevParams P, const float4* __restrict__ pos,
 
 }  // namespace
 
-void launch_search_head(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
-                        Skip skip, uint32_t* zero_res, int zero_res_count, bool use_cond,
-                        cudaGraphConditionalHandle cond, unsigned long long* counters,
-                        cudaStream_t st) {
+void launch_search_head(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
+                        SearchBuffers& sb, Skip skip, uint32_t* zero_res, int zero_res_count,
+                        bool use_cond, cudaGraphConditionalHandle cond,
+                        unsigned long long* counters, cudaStream_t st) {
     const int n = P.n;
     const int totals = kRadix * sb.passes;
     const int kb = blocks_for(n > totals ? n : totals);
-    k_keys<<<kb, kBlock, 0, st>>>(P, pos, sb.newkey, sb.moved, sb.blk_cnt, sb.num_blocks,
-                                  sb.slot_keys, sb.table_keys, sb.table, sb.digit_totals, totals,
-                                  zero_res, zero_res_count, skip);
+    if (T.params) {
+        k_keys<true><<<kb, kBlock, 0, st>>>(P, T, pos, sb.newkey, sb.moved, sb.blk_cnt,
+                                            sb.num_blocks, sb.slot_keys, sb.table_keys, sb.table,
+                                            sb.digit_totals, totals, zero_res, zero_res_count, skip);
+    } else {
+        k_keys<false><<<kb, kBlock, 0, st>>>(P, T, pos, sb.newkey, sb.moved, sb.blk_cnt,
+                                             sb.num_blocks, sb.slot_keys, sb.table_keys, sb.table,
+                                             sb.digit_totals, totals, zero_res, zero_res_count, skip);
+    }
     k_movers<<<1, kMoverThreads, kMoverCap * 12, st>>>(n, sb.blk_cnt, sb.blk_off, sb.num_blocks,
                                                        sb.moved, sb.newkey, ids, sb.mv_key,
                                                        sb.mv_slot, sb.ctrl, use_cond ? 1 : 0,
@@ -582,10 +606,10 @@ void launch_search_merge(const DevParams& P, const int* ids, SearchBuffers& sb, 
                                               sb.vals[sb.out], sb.src, sb.ctrl, skip);
 }
 
-void launch_search(const DevParams& P, const float4* pos, const int* ids, SearchBuffers& sb,
-                   Skip skip, uint32_t* zero_res, int zero_res_count,
+void launch_search(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
+                   SearchBuffers& sb, Skip skip, uint32_t* zero_res, int zero_res_count,
                    unsigned long long* counters, cudaStream_t st) {
-    launch_search_head(P, pos, ids, sb, skip, zero_res, zero_res_count, false, 0, counters, st);
+    launch_search_head(P, T, pos, ids, sb, skip, zero_res, zero_res_count, false, 0, counters, st);
     launch_search_radix(P, ids, sb, skip, st);
     launch_search_merge(P, ids, sb, skip, st);
 }
@@ -600,8 +624,10 @@ int radix_output(int passes) { return (passes - 1) & 1; }
 void launch_gather(const DevParams& P, SearchBuffers& sb, const float4* posA,
                    const float4* velA, float4* posB, float4* velB, int* idsB,
                    const float4* nposA, const float4* nvelA, float4* nposB, float4* nvelB,
-                   bool snap_from_state, const int* cnt_src, int* cnt_dst, bool step_search,
-                   unsigned long long* counters, Skip skip, cudaStream_t st) {
+                   bool snap_from_state, const int* cnt_src, int* cnt_dst, const int* scene_src,
+                   int* scene_dst, bool step_search, unsigned long long* counters,
+                   unsigned long long* scene_overflow, const DevParams* scene_params, Skip skip,
+                   cudaStream_t st) {
     const int nb = blocks_for(P.n);
     const uint32_t* skey = sb.keys[sb.out];
     const uint32_t* sid = sb.vals[sb.out];
@@ -609,31 +635,36 @@ void launch_gather(const DevParams& P, SearchBuffers& sb, const float4* posA,
     if (nposB == nullptr) {
         k_gather<false, false><<<nb, kBlock, 0, st>>>(
             P.n, P.ppc, skey, sid, sb.src, sb.slot_of_id, sb.ctrl, posA, velA, posB, velB, idsB,
-            nullptr, nullptr, nullptr, nullptr, cnt_src, cnt_dst, sb.table, sb.table_keys,
-            slot_keys, counters, skip);
+            nullptr, nullptr, nullptr, nullptr, cnt_src, cnt_dst, scene_src, scene_dst, sb.table,
+            sb.table_keys, slot_keys, counters, scene_overflow, scene_params, skip);
     } else if (snap_from_state) {
         k_gather<true, true><<<nb, kBlock, 0, st>>>(
             P.n, P.ppc, skey, sid, sb.src, sb.slot_of_id, sb.ctrl, posA, velA, posB, velB, idsB,
-            nullptr, nullptr, nposB, nvelB, cnt_src, cnt_dst, sb.table, sb.table_keys, slot_keys,
-            counters, skip);
+            nullptr, nullptr, nposB, nvelB, cnt_src, cnt_dst, scene_src, scene_dst, sb.table,
+            sb.table_keys, slot_keys, counters, scene_overflow, scene_params, skip);
     } else {
         k_gather<true, false><<<nb, kBlock, 0, st>>>(
             P.n, P.ppc, skey, sid, sb.src, sb.slot_of_id, sb.ctrl, posA, velA, posB, velB, idsB,
-            nposA, nvelA, nposB, nvelB, cnt_src, cnt_dst, sb.table, sb.table_keys, slot_keys,
-            counters, skip);
+            nposA, nvelA, nposB, nvelB, cnt_src, cnt_dst, scene_src, scene_dst, sb.table,
+            sb.table_keys, slot_keys, counters, scene_overflow, scene_params, skip);
     }
 }
 
-void launch_candidate_count(const DevParams& P, const float4* pos, const int* ids,
+void launch_candidate_count(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
                             const int2* table, int* count_by_id, cudaStream_t st) {
-    k_cand_count<<<blocks_for(P.n), kBlock, 0, st>>>(P, pos, ids, table, count_by_id);
+    if (T.params) k_cand_count<true><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, ids, table, count_by_id);
+    else k_cand_count<false><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, ids, table, count_by_id);
 }
 
-void launch_candidate_fill(const DevParams& P, const float4* pos, const int* ids,
+void launch_candidate_fill(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
                            const int2* table, const int64_t* offsets_by_id, int* cand,
                            uint8_t* contact, cudaStream_t st) {
-    k_cand_fill<<<blocks_for(P.n), kBlock, 0, st>>>(P, pos, ids, table, offsets_by_id, cand,
-                                                    contact);
+    if (T.params)
+        k_cand_fill<true><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, ids, table, offsets_by_id,
+                                                              cand, contact);
+    else
+        k_cand_fill<false><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, ids, table, offsets_by_id,
+                                                               cand, contact);
 }
 
 void launch_state_to_aos(int n, const float4* pos, const float4* vel, const int* ids,
@@ -656,9 +687,10 @@ void launch_state_from_aos(int n, const float* in6, float4* pos, float4* vel, co
     k_state_from_aos<<<blocks_for(n), kBlock, 0, st>>>(n, in6, pos, vel, ids);
 }
 
-void launch_cell_keys_by_id(const DevParams& P, const float4* pos, const int* ids,
+void launch_cell_keys_by_id(const DevParams& P, SceneTab T, const float4* pos, const int* ids,
                             int32_t* keys, cudaStream_t st) {
-    k_cell_keys_by_id<<<blocks_for(P.n), kBlock, 0, st>>>(P, pos, ids, keys);
+    if (T.params) k_cell_keys_by_id<true><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, ids, keys);
+    else k_cell_keys_by_id<false><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, ids, keys);
 }
 
 }  // namespace wd

@@ -94,6 +94,34 @@ struct wd_sim {
     wd::SearchBuffers sb{};
     uint64_t num_cells = 0;
 
+    // scenes: one for a plain simulation, S for a batch. Per-scene parameters live on
+    // the device only for S > 1 (kernels then look each grain's scene up).
+    int scenes = 1;
+    std::vector<wd::Config> scene_cfg;
+    std::vector<DevParams> scene_P;
+    std::vector<int64_t> scene_off;       // S+1 grain offsets (grain ids of scene s)
+    std::vector<int64_t> scene_nodes_off; // S+1 CIC node offsets
+    DevParams* d_scene_P = nullptr;
+    int* sceneA = nullptr;
+    int* sceneB = nullptr;
+    int* sceneC = nullptr;
+    int* d_seg = nullptr;                 // S+1 segment starts (int)
+    int* d_chunk_base = nullptr;          // S+1 reduction chunk offsets
+    int total_chunks = 0;
+    double* grain_vals = nullptr;         // 3n per-grain values for reductions
+    double* scene_sums = nullptr;         // 3S per-scene sums
+    unsigned long long* scene_overflow = nullptr;  // S lifetime overflow counts (batch)
+    int* scene_unstable = nullptr;        // S is_stable flags (batch)
+    // chaos metrics: node segments of the batch's density field
+    int* d_node_seg = nullptr;
+    int* d_node_chunk = nullptr;
+    int node_chunks = 0;
+    double* node_vals = nullptr;          // 6 values per node
+    double* chaos_partials = nullptr;
+    double* chaos_sums = nullptr;         // 6 per scene
+    double* grain_sums = nullptr;         // 1 per scene
+    float* chaos_grid = nullptr;          // 4 * nodes floats
+
     unsigned long long* counters = nullptr;
     uint32_t* picard_res = nullptr;
     int* picard_used = nullptr;
@@ -145,7 +173,11 @@ void free_sim(wd_sim* s) {
                     s->sb.src, s->sb.tile_counts, s->sb.digit_totals,
                     s->sb.table, s->counters, s->picard_res, s->picard_used, s->partials,
                     s->red_out, s->dep_bounds, s->dep_acc, s->dep_out, s->staging,
-                    s->cand_offsets, s->cand_count};
+                    s->cand_offsets, s->cand_count, s->d_scene_P, s->sceneA, s->sceneB,
+                    s->sceneC, s->d_seg, s->d_chunk_base, s->grain_vals, s->scene_sums,
+                    s->scene_overflow, s->scene_unstable, s->d_node_seg, s->d_node_chunk,
+                    s->node_vals, s->chaos_partials, s->chaos_sums, s->grain_sums,
+                    s->chaos_grid};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
@@ -181,7 +213,20 @@ DevParams make_params(const wd::Config& c, int n, float dt) {
     P.picard_tol = c.picard_tolerance;
     P.history = c.history ? 1 : 0;
     P.n = n;
+    for (int a = 0; a < 3; ++a) P.dgrid[a] = c.dgrid[a];
+    P.cell_base = 0;
+    P.node_base = 0;
+    P.frozen = 0;
     return P;
+}
+
+// Scene tables of the A / B / C arrays (empty for a single scene).
+wd::SceneTab tab(const wd_sim* s, const int* scene) {
+    return s->scenes > 1 ? wd::SceneTab{s->d_scene_P, scene} : wd::SceneTab{nullptr, nullptr};
+}
+
+wd::Segments segments(const wd_sim* s) {
+    return wd::Segments{s->d_seg, s->d_chunk_base, s->scenes, s->total_chunks};
 }
 
 // One neighbor search. Inside graph capture the radix path goes into an IF
@@ -192,7 +237,8 @@ cudaError_t enqueue_search(wd_sim* s, wd::Skip skip, uint32_t* zero_res, int zer
                            bool capture, cudaStream_t st) {
     const DevParams& P = s->P;
     if (!capture) {
-        wd::launch_search(P, s->posA, s->idsA, s->sb, skip, zero_res, zero_res_count, s->counters, st);
+        wd::launch_search(P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, skip, zero_res,
+                          zero_res_count, s->counters, st);
         return cudaGetLastError();
     }
     cudaStreamCaptureStatus status;
@@ -204,8 +250,8 @@ cudaError_t enqueue_search(wd_sim* s, wd::Skip skip, uint32_t* zero_res, int zer
     cudaGraphConditionalHandle cond;
     e = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault);
     if (e != cudaSuccess) return e;
-    wd::launch_search_head(P, s->posA, s->idsA, s->sb, skip, zero_res, zero_res_count, true, cond,
-                           s->counters, st);
+    wd::launch_search_head(P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, skip, zero_res,
+                           zero_res_count, true, cond, s->counters, st);
     e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
     if (e != cudaSuccess) return e;
     cudaGraphNodeParams cp = {};
@@ -246,13 +292,18 @@ cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
     fa.hist_out = s->hist[parity ^ 1];
     fa.hcnt_out = s->hcnt_slot;
     fa.counters = s->counters;
+    const bool batch = s->scenes > 1;
+    fa.scene_params = batch ? s->d_scene_P : nullptr;
+    fa.scene = s->sceneB;
+    fa.scene_out = s->sceneA;
     const wd::Skip none{nullptr, 0.f};
     if (!s->picard) {
         cudaError_t e = enqueue_search(s, none, nullptr, 0, capture, st);
         if (e != cudaSuccess) return e;
         wd::launch_gather(P, s->sb, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr, nullptr,
                           nullptr, nullptr, false, hist ? s->hcnt_slot : nullptr,
-                          hist ? s->hcnt_g : nullptr, true, s->counters, none, st);
+                          hist ? s->hcnt_g : nullptr, batch ? s->sceneA : nullptr,
+                          batch ? s->sceneB : nullptr, true, s->counters, s->scene_overflow, s->d_scene_P, none, st);
         if (mid) cudaEventRecord(mid, st);
         fa.hcnt_in = s->hcnt_g;
         wd::launch_force(P, fa, false, none, st);
@@ -268,7 +319,8 @@ cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
         wd::launch_gather(P, s->sb, s->posA, s->velA, s->posB, s->velB, s->idsB,
                           k == 0 ? nullptr : s->npos[nb ^ 1], k == 0 ? nullptr : s->nvel[nb ^ 1],
                           s->npos[nb], s->nvel[nb], k == 0, hist ? cnt_src : nullptr,
-                          hist ? s->hcnt_snap[nb] : nullptr, true, s->counters, skip, st);
+                          hist ? s->hcnt_snap[nb] : nullptr, batch ? s->sceneA : nullptr,
+                          batch ? s->sceneB : nullptr, true, s->counters, s->scene_overflow, s->d_scene_P, skip, st);
         fa.hcnt_in = s->hcnt_snap[nb];
         fa.npos = s->npos[nb];
         fa.nvel = s->nvel[nb];
@@ -353,16 +405,19 @@ int timed_step(wd_sim* s, int parity) {
 
 // Search on the current state into the C buffers (energy, probes).
 int ondemand_search(wd_sim* s) {
+    const bool batch = s->scenes > 1;
     if (!s->posC) {
         WD_CUDA(dalloc(&s->posC, s->n));
         WD_CUDA(dalloc(&s->velC, s->n));
         WD_CUDA(dalloc(&s->idsC, s->n));
+        if (batch) WD_CUDA(dalloc(&s->sceneC, s->n));
     }
     const wd::Skip none{nullptr, 0.f};
-    wd::launch_search(s->P, s->posA, s->idsA, s->sb, none, nullptr, 0, s->counters, s->stream);
+    wd::launch_search(s->P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, none, nullptr, 0,
+                      s->counters, s->stream);
     wd::launch_gather(s->P, s->sb, s->posA, s->velA, s->posC, s->velC, s->idsC, nullptr, nullptr,
-                      nullptr, nullptr, false, nullptr, nullptr, false, s->counters, none,
-                      s->stream);
+                      nullptr, nullptr, false, nullptr, nullptr, batch ? s->sceneA : nullptr,
+                      batch ? s->sceneC : nullptr, false, s->counters, s->scene_overflow, s->d_scene_P, none, s->stream);
     WD_CUDA(cudaGetLastError());
     return WD_OK;
 }
@@ -434,10 +489,33 @@ int alloc_sim(wd_sim* s) {
     WD_CUDA(cudaMemset(s->picard_res, 0, sizeof(uint32_t) * (s->picard_iters > 0 ? s->picard_iters : 1)));
     WD_CUDA(dalloc(&s->picard_used, 1));
     WD_CUDA(cudaMemset(s->picard_used, 0, sizeof(int)));
-    WD_CUDA(dalloc(&s->partials, static_cast<size_t>(3) * wd::reduction_blocks(n)));
     WD_CUDA(dalloc(&s->red_out, 4));
     WD_CUDA(dalloc(&s->staging, static_cast<size_t>(6) * n));
-    s->dep_nodes = static_cast<int64_t>(s->cfg.dgrid[0]) * s->cfg.dgrid[1] * s->cfg.dgrid[2];
+    s->dep_nodes = s->scene_nodes_off.back();
+    // per-scene reduction layout (segments of the sorted order, 256-grain chunks)
+    const int S = s->scenes;
+    std::vector<int> seg(S + 1), chunk(S + 1);
+    chunk[0] = 0;
+    for (int k = 0; k <= S; ++k) seg[k] = static_cast<int>(s->scene_off[k]);
+    for (int k = 0; k < S; ++k)
+        chunk[k + 1] = chunk[k] + static_cast<int>((s->scene_off[k + 1] - s->scene_off[k] + wd::kBlock - 1) / wd::kBlock);
+    s->total_chunks = chunk[S];
+    WD_CUDA(dalloc(&s->d_seg, S + 1));
+    WD_CUDA(dalloc(&s->d_chunk_base, S + 1));
+    WD_CUDA(cudaMemcpy(s->d_seg, seg.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice));
+    WD_CUDA(cudaMemcpy(s->d_chunk_base, chunk.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice));
+    WD_CUDA(dalloc(&s->partials, static_cast<size_t>(3) * s->total_chunks));
+    WD_CUDA(dalloc(&s->scene_sums, static_cast<size_t>(3) * S));
+    WD_CUDA(dalloc(&s->grain_vals, static_cast<size_t>(3) * n));
+    if (S > 1) {
+        WD_CUDA(dalloc(&s->d_scene_P, S));
+        WD_CUDA(cudaMemcpy(s->d_scene_P, s->scene_P.data(), sizeof(DevParams) * S, cudaMemcpyHostToDevice));
+        WD_CUDA(dalloc(&s->sceneA, n));
+        WD_CUDA(dalloc(&s->sceneB, n));
+        WD_CUDA(dalloc(&s->scene_overflow, S));
+        WD_CUDA(cudaMemset(s->scene_overflow, 0, sizeof(unsigned long long) * S));
+        WD_CUDA(dalloc(&s->scene_unstable, S));
+    }
     return WD_OK;
 }
 
@@ -459,45 +537,23 @@ int upload_initial(wd_sim* s, const float* state) {
     WD_CUDA(cudaMemcpy(s->velB, s->velA, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
     WD_CUDA(cudaMemcpy(s->idsB, s->idsA, sizeof(int) * n, cudaMemcpyDeviceToDevice));
     WD_CUDA(cudaMemset(s->acc, 0, sizeof(float4) * n));
+    if (s->scenes > 1) {
+        std::vector<int> sc(n);
+        for (int k = 0; k < s->scenes; ++k)
+            for (int64_t i = s->scene_off[k]; i < s->scene_off[k + 1]; ++i) sc[i] = k;
+        WD_CUDA(cudaMemcpy(s->sceneA, sc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+        WD_CUDA(cudaMemcpy(s->sceneB, sc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    }
     return WD_OK;
 }
 
-int create_impl(const wd::Config& cfg, int64_t n64, const float* state,
-                const int32_t* material, const float* radius, const float* mass,
-                wd_sim** out) {
-    if (!out) return fail(WD_ERR_INVALID, "wd_create: out is NULL");
-    *out = nullptr;
-    if (n64 <= 0 || n64 > (int64_t{1} << 30))
-        return fail(WD_ERR_INVALID, "wd_create: grain count must be in [1, 2^30]");
-    if (!state) return fail(WD_ERR_INVALID, "wd_create: state is NULL");
-    for (int a = 0; a < 3; ++a) {
-        if (cfg.grid[a] <= 0) return fail(WD_ERR_INVALID, "wd_create: collision grid sizes must be > 0");
-        if (cfg.dgrid[a] <= 0) return fail(WD_ERR_INVALID, "wd_create: density grid sizes must be > 0");
-    }
-    const uint64_t cells = static_cast<uint64_t>(cfg.grid[0]) * cfg.grid[1] * cfg.grid[2];
-    if (cells >= (uint64_t{1} << 32))
-        return fail(WD_ERR_INVALID, "wd_create: collision grid exceeds 2^32 cells");
-    if (!(cfg.particle_radius > 0.f) && !radius)
-        return fail(WD_ERR_INVALID, "wd_create: physics.particle_radius must be > 0");
-    if (cfg.picard_iterations < 1 && cfg.time_integrator != "semi_implicit_euler")
-        return fail(WD_ERR_INVALID, "wd_create: picard_iterations must be >= 1");
-
-    wd_sim* s = new wd_sim();
-    s->cfg = cfg;
-    s->n = static_cast<int>(n64);
-    s->dt = cfg.dt;
-    s->picard = cfg.time_integrator != "semi_implicit_euler";
-    s->picard_iters = s->picard ? cfg.picard_iterations : 1;
-    s->num_cells = cells;
-    s->P = make_params(cfg, s->n, s->dt);
-    s->radius.resize(s->n);
-    s->mass.resize(s->n);
-    s->material.resize(s->n);
-    for (int i = 0; i < s->n; ++i) {
+// Per-grain radius and mass of one scene (the reference's mass table, or density).
+int scene_grains(const wd::Config& cfg, int64_t n, const int32_t* material, const float* radius,
+                 const float* mass, std::vector<float>& r_out, std::vector<float>& m_out,
+                 std::vector<int32_t>& mat_out) {
+    for (int64_t i = 0; i < n; ++i) {
         const int32_t mat = material ? material[i] : cfg.particle_material;
-        s->material[i] = mat;
         const float r = radius ? radius[i] : cfg.particle_radius;
-        s->radius[i] = r;
         float m;
         if (mass) {
             m = mass[i];
@@ -505,20 +561,111 @@ int create_impl(const wd::Config& cfg, int64_t n64, const float* state,
             const double rd = r;
             m = static_cast<float>(static_cast<double>(cfg.density) * 4.0 / 3.0 * 3.14159265358979323846 * rd * rd * rd);
         } else {
-            if (mat < 0 || static_cast<size_t>(mat) >= cfg.masses.size()) {
-                delete s;
+            if (mat < 0 || static_cast<size_t>(mat) >= cfg.masses.size())
                 return fail(WD_ERR_INVALID, "wd_create: material id " + std::to_string(mat) +
                                                 " has no entry in materials.masses");
-            }
             m = cfg.masses[mat];
         }
-        s->mass[i] = m;
+        r_out.push_back(r);
+        m_out.push_back(m);
+        mat_out.push_back(mat);
     }
-    float rmax = 0.f;
-    for (int i = 0; i < s->n; ++i) rmax = fmaxf(rmax, s->radius[i]);
-    s->P.rmax = rmax;
+    return WD_OK;
+}
+
+int check_scene_config(const wd::Config& cfg, bool have_radius) {
+    for (int a = 0; a < 3; ++a) {
+        if (cfg.grid[a] <= 0) return fail(WD_ERR_INVALID, "wd_create: collision grid sizes must be > 0");
+        if (cfg.dgrid[a] <= 0) return fail(WD_ERR_INVALID, "wd_create: density grid sizes must be > 0");
+    }
+    if (!(cfg.particle_radius > 0.f) && !have_radius)
+        return fail(WD_ERR_INVALID, "wd_create: physics.particle_radius must be > 0");
+    if (cfg.picard_iterations < 1 && cfg.time_integrator != "semi_implicit_euler")
+        return fail(WD_ERR_INVALID, "wd_create: picard_iterations must be >= 1");
+    return WD_OK;
+}
+
+// S scenes in one handle. Scene k's grains get the global ids [off_k, off_k + n_k);
+// its collision cells and CIC nodes are placed after those of the scenes before it.
+// All scenes share the integrator, Picard settings, history mode and dt; a batch
+// (S > 1) runs Picard with a fixed iteration count only.
+int create_scenes(const wd::Config* const* cfgs, int S, const int64_t* counts,
+                  const float* const* states, const int32_t* const* materials,
+                  const float* const* radii, const float* const* masses, wd_sim** out) {
+    if (!out) return fail(WD_ERR_INVALID, "wd_create: out is NULL");
+    *out = nullptr;
+    if (S < 1 || !cfgs || !counts || !states) return fail(WD_ERR_INVALID, "wd_create: no scenes");
+    int64_t total = 0;
+    uint64_t cells = 0;
+    int64_t nodes = 0;
+    const wd::Config& c0 = *cfgs[0];
+    for (int k = 0; k < S; ++k) {
+        if (!cfgs[k] || !states[k]) return fail(WD_ERR_INVALID, "wd_create: NULL scene config or state");
+        const wd::Config& c = *cfgs[k];
+        int rc = check_scene_config(c, radii && radii[k]);
+        if (rc) return rc;
+        if (counts[k] <= 0) return fail(WD_ERR_INVALID, "wd_create: every scene needs grains");
+        const bool picard = c0.time_integrator != "semi_implicit_euler";
+        if (k > 0 && (c.time_integrator != c0.time_integrator || c.history != c0.history ||
+                      c.dt != c0.dt || (picard && c.picard_iterations != c0.picard_iterations)))
+            return fail(WD_ERR_INVALID, "wd_create: scenes of a batch must share the integrator, "
+                                        "Picard iterations, history mode and dt");
+        total += counts[k];
+        cells += static_cast<uint64_t>(c.grid[0]) * c.grid[1] * c.grid[2];
+        nodes += static_cast<int64_t>(c.dgrid[0]) * c.dgrid[1] * c.dgrid[2];
+    }
+    if (S > 1 && c0.time_integrator != "semi_implicit_euler" && c0.picard_tolerance > 0.f)
+        return fail(WD_ERR_INVALID, "wd_create: a batch of scenes runs Picard with a fixed "
+                                    "iteration count (time_integration.picard_tolerance: 0)");
+    if (total > (int64_t{1} << 30)) return fail(WD_ERR_INVALID, "wd_create: grain count must be in [1, 2^30]");
+    if (cells >= (uint64_t{1} << 32))
+        return fail(WD_ERR_INVALID, "wd_create: collision grids exceed 2^32 cells in total");
+    if (nodes >= (int64_t{1} << 31)) return fail(WD_ERR_INVALID, "wd_create: density grids too large");
+
+    wd_sim* s = new wd_sim();
+    s->cfg = c0;
+    s->scenes = S;
+    s->n = static_cast<int>(total);
+    s->dt = c0.dt;
+    s->picard = c0.time_integrator != "semi_implicit_euler";
+    s->picard_iters = s->picard ? c0.picard_iterations : 1;
+    s->num_cells = cells;
+    s->scene_off.assign(1, 0);
+    s->scene_nodes_off.assign(1, 0);
+    uint64_t cell_base = 0;
+    for (int k = 0; k < S; ++k) {
+        const wd::Config& c = *cfgs[k];
+        s->scene_cfg.push_back(c);
+        const size_t first = s->radius.size();
+        int rc = scene_grains(c, counts[k], materials ? materials[k] : nullptr,
+                              radii ? radii[k] : nullptr, masses ? masses[k] : nullptr, s->radius,
+                              s->mass, s->material);
+        if (rc) {
+            delete s;
+            return rc;
+        }
+        DevParams Q = make_params(c, static_cast<int>(counts[k]), s->dt);
+        float rmax = 0.f;
+        for (size_t i = first; i < s->radius.size(); ++i) rmax = fmaxf(rmax, s->radius[i]);
+        Q.rmax = rmax;
+        Q.cell_base = static_cast<uint32_t>(cell_base);
+        Q.node_base = static_cast<int>(s->scene_nodes_off.back());
+        s->scene_P.push_back(Q);
+        cell_base += static_cast<uint64_t>(c.grid[0]) * c.grid[1] * c.grid[2];
+        s->scene_off.push_back(s->scene_off.back() + counts[k]);
+        s->scene_nodes_off.push_back(s->scene_nodes_off.back() +
+                                     static_cast<int64_t>(c.dgrid[0]) * c.dgrid[1] * c.dgrid[2]);
+    }
+    // whole-handle parameters: scene 0's physics for a single scene; for a batch only
+    // n, dt, history and the Picard settings are read from it
+    s->P = s->scene_P[0];
+    s->P.n = s->n;
+    std::vector<float> all_state(static_cast<size_t>(6) * s->n);
+    for (int k = 0; k < S; ++k)
+        std::memcpy(all_state.data() + 6 * s->scene_off[k], states[k],
+                    sizeof(float) * 6 * static_cast<size_t>(counts[k]));
     int rc = alloc_sim(s);
-    if (rc == WD_OK) rc = upload_initial(s, state);
+    if (rc == WD_OK) rc = upload_initial(s, all_state.data());
     if (rc != WD_OK) {
         const std::string msg = wd::last_error_cstr();
         free_sim(s);
@@ -526,6 +673,21 @@ int create_impl(const wd::Config& cfg, int64_t n64, const float* state,
     }
     *out = s;
     return WD_OK;
+}
+
+int create_impl(const wd::Config& cfg, int64_t n64, const float* state,
+                const int32_t* material, const float* radius, const float* mass,
+                wd_sim** out) {
+    if (n64 <= 0 || n64 > (int64_t{1} << 30))
+        return fail(WD_ERR_INVALID, "wd_create: grain count must be in [1, 2^30]");
+    if (!state) return fail(WD_ERR_INVALID, "wd_create: state is NULL");
+    const wd::Config* cfgs[1] = {&cfg};
+    const int64_t counts[1] = {n64};
+    const float* states[1] = {state};
+    const int32_t* mats[1] = {material};
+    const float* radii[1] = {radius};
+    const float* masses[1] = {mass};
+    return create_scenes(cfgs, 1, counts, states, mats, radii, masses, out);
 }
 
 }  // namespace
@@ -618,6 +780,57 @@ int wd_create_from_arrays(const wd_config* cfg, int64_t n, const float* state,
     return create_impl(cfg->cfg, n, state, material, radius, mass, out);
 }
 
+int wd_create_batch(const wd_config* const* cfgs, int32_t num_scenes, const int64_t* counts,
+                    const float* const* states, const int32_t* const* materials,
+                    const float* const* radii, const float* const* masses, wd_sim** out) {
+    if (!cfgs || num_scenes < 1) return fail(WD_ERR_INVALID, "wd_create_batch: no scenes");
+    const int S = num_scenes;
+    std::vector<const wd::Config*> c(S);
+    std::vector<wd::Grains> built(S);
+    std::vector<int64_t> cnt(S);
+    std::vector<const float*> st(S);
+    std::vector<const int32_t*> mat(S);
+    for (int k = 0; k < S; ++k) {
+        if (!cfgs[k]) return fail(WD_ERR_INVALID, "wd_create_batch: NULL config");
+        c[k] = &cfgs[k]->cfg;
+        mat[k] = materials ? materials[k] : nullptr;
+        if (states && states[k]) {
+            if (!counts) return fail(WD_ERR_INVALID, "wd_create_batch: states given without counts");
+            st[k] = states[k];
+            cnt[k] = counts[k];
+            continue;
+        }
+        // no state: the scene's own initialization section, as wd_create
+        std::string err;
+        const int rc = wd::build_initial_grains(*c[k], &built[k], &err);
+        if (rc < 0) return fail(rc, err);
+        if (built[k].material.empty())
+            return fail(WD_ERR_INVALID, "wd_create_batch: scene " + std::to_string(k) +
+                                            " initialization produced no grains");
+        st[k] = built[k].state.data();
+        cnt[k] = static_cast<int64_t>(built[k].material.size());
+        if (!mat[k]) mat[k] = built[k].material.data();
+    }
+    return create_scenes(c.data(), S, cnt.data(), st.data(), mat.data(), radii, masses, out);
+}
+
+int wd_scene_count(const wd_sim* sim, int32_t* scenes) {
+    if (!sim || !scenes) return fail(WD_ERR_INVALID, "wd_scene_count: NULL argument");
+    *scenes = sim->scenes;
+    return WD_OK;
+}
+
+int wd_scene_range(const wd_sim* sim, int32_t scene, int64_t* first, int64_t* count,
+                   int64_t* node_first, int64_t* nodes) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_scene_range: NULL handle");
+    if (scene < 0 || scene >= sim->scenes) return fail(WD_ERR_INVALID, "wd_scene_range: scene out of range");
+    if (first) *first = sim->scene_off[scene];
+    if (count) *count = sim->scene_off[scene + 1] - sim->scene_off[scene];
+    if (node_first) *node_first = sim->scene_nodes_off[scene];
+    if (nodes) *nodes = sim->scene_nodes_off[scene + 1] - sim->scene_nodes_off[scene];
+    return WD_OK;
+}
+
 int wd_destroy(wd_sim* sim) {
     if (!sim) return WD_OK;
     if (sim->stream) cudaStreamSynchronize(sim->stream);
@@ -650,6 +863,15 @@ int wd_set_dt(wd_sim* sim, float dt) {
     if (dt != sim->dt) {
         sim->dt = dt;
         sim->P.dt = dt;
+        for (DevParams& Q : sim->scene_P) Q.dt = dt;
+        if (sim->d_scene_P) {
+            // ordered after the steps already queued, before the next one
+            WD_CUDA(cudaMemcpyAsync(sim->d_scene_P, sim->scene_P.data(),
+                                    sizeof(DevParams) * sim->scene_P.size(),
+                                    cudaMemcpyHostToDevice, sim->stream));
+            int rc = sync_stream(sim);
+            if (rc) return rc;
+        }
         sim->graph_dirty = true;
     }
     return WD_OK;
@@ -849,7 +1071,7 @@ int wd_density_grid_nodes(const wd_sim* sim, int64_t* nodes) {
 int wd_compute_density_grid_device(wd_sim* sim, float* d_grid) {
     if (!sim || !d_grid) return fail(WD_ERR_INVALID, "wd_compute_density_grid_device: NULL argument");
     if (!sim->dep_acc) {
-        WD_CUDA(dalloc(&sim->dep_bounds, 4));
+        WD_CUDA(dalloc(&sim->dep_bounds, static_cast<size_t>(4) * sim->scenes));
         WD_CUDA(dalloc(&sim->dep_acc, static_cast<size_t>(4) * sim->dep_nodes));
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -858,8 +1080,12 @@ int wd_compute_density_grid_device(wd_sim* sim, float* d_grid) {
         e1 = take_event(sim);
         WD_CUDA(cudaEventRecord(e0, sim->stream));
     }
-    wd::launch_deposit(sim->n, sim->posA, sim->velA, sim->cfg.dom_lo, sim->cfg.dom_hi,
-                       sim->cfg.dgrid, sim->dep_bounds, sim->dep_acc, d_grid, sim->stream);
+    if (sim->scenes > 1)
+        wd::launch_deposit_batch(sim->n, sim->posA, sim->velA, tab(sim, sim->sceneA), sim->scenes,
+                                 sim->dep_nodes, sim->dep_bounds, sim->dep_acc, d_grid, sim->stream);
+    else
+        wd::launch_deposit(sim->n, sim->posA, sim->velA, sim->cfg.dom_lo, sim->cfg.dom_hi,
+                           sim->cfg.dgrid, sim->dep_bounds, sim->dep_acc, d_grid, sim->stream);
     WD_CUDA(cudaGetLastError());
     if (e0) {
         WD_CUDA(cudaEventRecord(e1, sim->stream));
@@ -883,31 +1109,58 @@ int wd_compute_density_grid(wd_sim* sim, float* grid) {
     return sync_stream(sim);
 }
 
-int wd_compute_total_energy(wd_sim* sim, double* energy) {
-    if (!sim || !energy) return fail(WD_ERR_INVALID, "wd_compute_total_energy: NULL argument");
+int wd_compute_scene_energies(wd_sim* sim, double* energies) {
+    if (!sim || !energies) return fail(WD_ERR_INVALID, "wd_compute_scene_energies: NULL argument");
     int rc = ondemand_search(sim);
     if (rc) return rc;
-    wd::launch_energy(sim->P, sim->posC, sim->velC, sim->idsC, sim->sb.table,
-                      sim->hist[sim->hist_cur], sim->hcnt_slot, sim->sb.src, sim->partials,
-                      sim->red_out, sim->stream);
+    wd::launch_energy(sim->P, tab(sim, sim->sceneC), sim->posC, sim->velC, sim->idsC,
+                      sim->sb.table, sim->hist[sim->hist_cur], sim->hcnt_slot, sim->sb.src,
+                      segments(sim), sim->grain_vals, sim->partials, sim->scene_sums, sim->stream);
     WD_CUDA(cudaGetLastError());
-    WD_CUDA(cudaMemcpyAsync(energy, sim->red_out, sizeof(double), cudaMemcpyDeviceToHost, sim->stream));
+    WD_CUDA(cudaMemcpyAsync(energies, sim->scene_sums, sizeof(double) * sim->scenes,
+                            cudaMemcpyDeviceToHost, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_compute_total_energy(wd_sim* sim, double* energy) {
+    if (!sim || !energy) return fail(WD_ERR_INVALID, "wd_compute_total_energy: NULL argument");
+    std::vector<double> e(sim->scenes);
+    int rc = wd_compute_scene_energies(sim, e.data());
+    if (rc) return rc;
+    double t = 0.0;
+    for (double v : e) t += v;
+    *energy = t;
+    return WD_OK;
+}
+
+int wd_compute_scene_momenta(wd_sim* sim, double* momenta) {
+    if (!sim || !momenta) return fail(WD_ERR_INVALID, "wd_compute_scene_momenta: NULL argument");
+    wd::launch_momentum(sim->n, sim->velA, segments(sim), sim->grain_vals, sim->partials,
+                        sim->scene_sums, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    WD_CUDA(cudaMemcpyAsync(momenta, sim->scene_sums, 3 * sizeof(double) * sim->scenes,
+                            cudaMemcpyDeviceToHost, sim->stream));
     return sync_stream(sim);
 }
 
 int wd_compute_momentum(wd_sim* sim, double* momentum3) {
     if (!sim || !momentum3) return fail(WD_ERR_INVALID, "wd_compute_momentum: NULL argument");
-    wd::launch_momentum(sim->n, sim->velA, sim->partials, sim->red_out, sim->stream);
-    WD_CUDA(cudaGetLastError());
-    WD_CUDA(cudaMemcpyAsync(momentum3, sim->red_out, 3 * sizeof(double), cudaMemcpyDeviceToHost,
-                            sim->stream));
-    return sync_stream(sim);
+    std::vector<double> m(static_cast<size_t>(3) * sim->scenes);
+    int rc = wd_compute_scene_momenta(sim, m.data());
+    if (rc) return rc;
+    for (int a = 0; a < 3; ++a) {
+        double t = 0.0;
+        for (int k = 0; k < sim->scenes; ++k) t += m[3 * k + a];
+        momentum3[a] = t;
+    }
+    return WD_OK;
 }
 
 int wd_is_stable(wd_sim* sim, int32_t* stable) {
     if (!sim || !stable) return fail(WD_ERR_INVALID, "wd_is_stable: NULL argument");
     WD_CUDA(cudaMemsetAsync(sim->counters + wd::kCntUnstable, 0, sizeof(unsigned long long), sim->stream));
-    wd::launch_stability(sim->P, sim->posA, sim->counters, sim->stream);
+    wd::launch_stability(sim->P, tab(sim, sim->sceneA), sim->posA, sim->counters, nullptr,
+                         sim->stream);
     WD_CUDA(cudaGetLastError());
     unsigned long long flag = 0;
     WD_CUDA(cudaMemcpyAsync(&flag, sim->counters + wd::kCntUnstable, sizeof(flag),
@@ -984,7 +1237,7 @@ int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
 int wd_debug_cell_keys(wd_sim* sim, int32_t* keys) {
     if (!sim || !keys) return fail(WD_ERR_INVALID, "wd_debug_cell_keys: NULL argument");
     int32_t* d = reinterpret_cast<int32_t*>(sim->staging);
-    wd::launch_cell_keys_by_id(sim->P, sim->posA, sim->idsA, d, sim->stream);
+    wd::launch_cell_keys_by_id(sim->P, tab(sim, sim->sceneA), sim->posA, sim->idsA, d, sim->stream);
     WD_CUDA(cudaGetLastError());
     WD_CUDA(cudaMemcpyAsync(keys, d, sizeof(int32_t) * static_cast<size_t>(sim->n),
                             cudaMemcpyDeviceToHost, sim->stream));
@@ -1011,7 +1264,8 @@ int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* c
         WD_CUDA(dalloc(&sim->cand_count, n));
         WD_CUDA(dalloc(&sim->cand_offsets, static_cast<size_t>(n) + 1));
     }
-    wd::launch_candidate_count(sim->P, sim->posC, sim->idsC, sim->sb.table, sim->cand_count, sim->stream);
+    wd::launch_candidate_count(sim->P, tab(sim, sim->sceneC), sim->posC, sim->idsC, sim->sb.table,
+                               sim->cand_count, sim->stream);
     WD_CUDA(cudaGetLastError());
     std::vector<int> counts(n);
     WD_CUDA(cudaMemcpyAsync(counts.data(), sim->cand_count, sizeof(int) * n, cudaMemcpyDeviceToHost, sim->stream));
@@ -1027,8 +1281,8 @@ int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* c
     WD_CUDA(dalloc(&d_contact, static_cast<size_t>(*total)));
     WD_CUDA(cudaMemcpyAsync(sim->cand_offsets, offsets, sizeof(int64_t) * (n + 1),
                             cudaMemcpyHostToDevice, sim->stream));
-    wd::launch_candidate_fill(sim->P, sim->posC, sim->idsC, sim->sb.table, sim->cand_offsets,
-                              d_cand, d_contact, sim->stream);
+    wd::launch_candidate_fill(sim->P, tab(sim, sim->sceneC), sim->posC, sim->idsC, sim->sb.table,
+                              sim->cand_offsets, d_cand, d_contact, sim->stream);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(cand, d_cand, sizeof(int32_t) * static_cast<size_t>(*total),
@@ -1040,6 +1294,115 @@ int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* c
     cudaFree(d_cand);
     cudaFree(d_contact);
     WD_CUDA(e);
+    return WD_OK;
+}
+
+// ---- batched scenes: per-scene diagnostics and ensemble metrics -----------------
+
+int wd_scene_overflow_counts(wd_sim* sim, int64_t* counts) {
+    if (!sim || !counts) return fail(WD_ERR_INVALID, "wd_scene_overflow_counts: NULL argument");
+    if (sim->scenes == 1) return read_counter(sim, wd::kCntGridOverflow, counts);
+    std::vector<unsigned long long> v(sim->scenes);
+    WD_CUDA(cudaMemcpyAsync(v.data(), sim->scene_overflow, sizeof(unsigned long long) * v.size(),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    const int rc = sync_stream(sim);
+    if (rc) return rc;
+    for (int k = 0; k < sim->scenes; ++k) counts[k] = static_cast<int64_t>(v[k]);
+    return WD_OK;
+}
+
+int wd_scene_stability(wd_sim* sim, int32_t* stable) {
+    if (!sim || !stable) return fail(WD_ERR_INVALID, "wd_scene_stability: NULL argument");
+    if (sim->scenes == 1) return wd_is_stable(sim, stable);
+    WD_CUDA(cudaMemsetAsync(sim->counters + wd::kCntUnstable, 0, sizeof(unsigned long long), sim->stream));
+    WD_CUDA(cudaMemsetAsync(sim->scene_unstable, 0, sizeof(int) * sim->scenes, sim->stream));
+    wd::launch_stability(sim->P, tab(sim, sim->sceneA), sim->posA, sim->counters,
+                         sim->scene_unstable, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    std::vector<int> v(sim->scenes);
+    WD_CUDA(cudaMemcpyAsync(v.data(), sim->scene_unstable, sizeof(int) * v.size(),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    const int rc = sync_stream(sim);
+    if (rc) return rc;
+    for (int k = 0; k < sim->scenes; ++k) stable[k] = v[k] ? 0 : 1;
+    return WD_OK;
+}
+
+int wd_freeze_scene(wd_sim* sim, int32_t scene, int32_t frozen) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_freeze_scene: NULL handle");
+    if (sim->scenes == 1) return fail(WD_ERR_INVALID, "wd_freeze_scene: not a batch of scenes");
+    if (scene < 0 || scene >= sim->scenes) return fail(WD_ERR_INVALID, "wd_freeze_scene: scene out of range");
+    sim->scene_P[scene].frozen = frozen ? 1 : 0;
+    // ordered after the steps already queued, before the next one
+    WD_CUDA(cudaMemcpyAsync(sim->d_scene_P + scene, &sim->scene_P[scene], sizeof(DevParams),
+                            cudaMemcpyHostToDevice, sim->stream));
+    return sync_stream(sim);
+}
+
+int wd_chaos_metrics(wd_sim* sim, int32_t reference_scene, double* metrics3) {
+    if (!sim || !metrics3) return fail(WD_ERR_INVALID, "wd_chaos_metrics: NULL argument");
+    const int S = sim->scenes;
+    if (reference_scene < 0 || reference_scene >= S)
+        return fail(WD_ERR_INVALID, "wd_chaos_metrics: reference scene out of range");
+    const int64_t n0 = sim->scene_off[1] - sim->scene_off[0];
+    for (int k = 0; k < S; ++k) {
+        const wd::Config& c = sim->scene_cfg[k];
+        const wd::Config& c0 = sim->scene_cfg[0];
+        if (sim->scene_off[k + 1] - sim->scene_off[k] != n0 ||
+            c.dgrid[0] != c0.dgrid[0] || c.dgrid[1] != c0.dgrid[1] || c.dgrid[2] != c0.dgrid[2])
+            return fail(WD_ERR_INVALID, "wd_chaos_metrics: every scene needs the same grain "
+                                        "count and density grid");
+    }
+    const int total_nodes = static_cast<int>(sim->dep_nodes);
+    if (!sim->d_node_seg) {
+        std::vector<int> seg(S + 1), chunk(S + 1);
+        chunk[0] = 0;
+        for (int k = 0; k <= S; ++k) seg[k] = static_cast<int>(sim->scene_nodes_off[k]);
+        for (int k = 0; k < S; ++k)
+            chunk[k + 1] = chunk[k] + static_cast<int>((seg[k + 1] - seg[k] + wd::kBlock - 1) / wd::kBlock);
+        sim->node_chunks = chunk[S];
+        WD_CUDA(dalloc(&sim->d_node_seg, S + 1));
+        WD_CUDA(dalloc(&sim->d_node_chunk, S + 1));
+        WD_CUDA(cudaMemcpy(sim->d_node_seg, seg.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice));
+        WD_CUDA(cudaMemcpy(sim->d_node_chunk, chunk.data(), sizeof(int) * (S + 1), cudaMemcpyHostToDevice));
+        WD_CUDA(dalloc(&sim->node_vals, static_cast<size_t>(6) * total_nodes));
+        WD_CUDA(dalloc(&sim->chaos_partials, static_cast<size_t>(6) * sim->node_chunks));
+        WD_CUDA(dalloc(&sim->chaos_sums, static_cast<size_t>(6) * S));
+        WD_CUDA(dalloc(&sim->grain_sums, S));
+        WD_CUDA(dalloc(&sim->chaos_grid, static_cast<size_t>(4) * total_nodes));
+    }
+    int rc = wd_compute_density_grid_device(sim, sim->chaos_grid);
+    if (rc) return rc;
+    float* pos3 = reinterpret_cast<float*>(sim->staging);
+    rc = wd_get_positions_device(sim, pos3);
+    if (rc) return rc;
+    const wd::Segments nodes{sim->d_node_seg, sim->d_node_chunk, S, sim->node_chunks};
+    wd::launch_chaos(sim->n, pos3, segments(sim), sim->grain_vals, sim->partials, sim->grain_sums,
+                     total_nodes, sim->chaos_grid, nodes, reference_scene, sim->cfg.dgrid[1],
+                     sim->cfg.dgrid[2], sim->node_vals, sim->chaos_partials, sim->chaos_sums,
+                     sim->stream);
+    WD_CUDA(cudaGetLastError());
+    std::vector<double> g(S), f(static_cast<size_t>(6) * S);
+    WD_CUDA(cudaMemcpyAsync(g.data(), sim->grain_sums, sizeof(double) * S, cudaMemcpyDeviceToHost,
+                            sim->stream));
+    WD_CUDA(cudaMemcpyAsync(f.data(), sim->chaos_sums, sizeof(double) * 6 * S,
+                            cudaMemcpyDeviceToHost, sim->stream));
+    rc = sync_stream(sim);
+    if (rc) return rc;
+    const double* fr = &f[6 * static_cast<size_t>(reference_scene)];
+    double com_ref[3];
+    for (int a = 0; a < 3; ++a) com_ref[a] = fr[2] > 0.0 ? fr[3 + a] / fr[2] : 0.0;
+    for (int k = 0; k < S; ++k) {
+        const double* fk = &f[6 * static_cast<size_t>(k)];
+        metrics3[3 * k] = std::sqrt(g[k] / static_cast<double>(n0));
+        metrics3[3 * k + 1] = fk[1] > 0.0 ? std::sqrt(fk[0] / fk[1]) : 0.0;
+        double dd = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            const double com = fk[2] > 0.0 ? fk[3 + a] / fk[2] : 0.0;
+            dd += (com - com_ref[a]) * (com - com_ref[a]);
+        }
+        metrics3[3 * k + 2] = std::sqrt(dd);
+    }
     return WD_OK;
 }
 

@@ -52,6 +52,9 @@ class ParticleDynamics:
                     raise ValueError(f"{name} has {arr.size} entries for {n} grains")
             check(lib.wd_create_from_arrays(self.config.handle, n, ptr(st), ptr(mat), ptr(rad),
                                             ptr(ms), ctypes.byref(h)))
+        self._attach(h)
+
+    def _attach(self, h: ctypes.c_void_p) -> None:
         self._h = h
         n64 = ctypes.c_int64()
         check(lib.wd_get_n(h, ctypes.byref(n64)))

@@ -109,12 +109,14 @@ def column_collapse(n: int = N_REF, *, diameters: str = "uniform", seed: int = 1
                     mu: float = 0.5, restitution: float = 0.5, k_n: float = 1e5,
                     density: float = 2500.0, dt: float = 1e-5, history: bool = True,
                     integrator: str = "semi_implicit_euler", picard_iterations: int = 8,
-                    picard_tol: float = 1e-6, cic: int = 64, d: float = D_REF) -> Scene:
+                    picard_tol: float = 1e-6, cic: int = 64, d: float = D_REF,
+                    aspect: float = 4.0) -> Scene:
     rng = np.random.default_rng(seed)
     scale = (n / N_REF) ** (1.0 / 3.0)
-    R = 0.1 * scale
-    H = 4.0 * R
-    box = (1.0 * scale, 1.0 * scale, 0.5 * scale)
+    # column volume pi R^2 H with H = aspect * R, equal to the aspect-4 column's
+    R = 0.1 * scale * (4.0 / aspect) ** (1.0 / 3.0)
+    H = aspect * R
+    box = (1.0 * scale, 1.0 * scale, max(0.5 * scale, 1.25 * H))
     diam = _diameters(rng, n, d, diameters)
     d_max = float(diam.max())
     # smallest spacing (>= d_max) whose first n sites fit in the cylinder
@@ -135,7 +137,44 @@ def column_collapse(n: int = N_REF, *, diameters: str = "uniform", seed: int = 1
                   dt=dt, history=history, integrator=integrator,
                   picard_iterations=picard_iterations, picard_tol=picard_tol, cic=cic)
     return Scene(cfg, state, (0.5 * diam).astype(np.float32),
-                 f"column_collapse n={n} d={diameters} mu={mu} {integrator}")
+                 f"column_collapse n={n} d={diameters} mu={mu} H/R={aspect:g} {integrator}")
+
+
+def perturbed_members(base: Scene, members: int, sigma: float = 50e-6,
+                      seed: int = 7) -> list[Scene]:
+    """Ensemble members of one scene: every grain moved by isotropic N(0, sigma^2)
+    per axis, member m drawing from its own seed (seed, m). The reference perturbs
+    by uniform +-p r per axis at initialization (src/particle_dynamics.cu:190-202);
+    this Gaussian form is the ensemble's own generator."""
+    out = []
+    for m in range(members):
+        rng = np.random.default_rng([seed, m])
+        st = base.state.copy()
+        st[:, :3] = (st[:, :3].astype(np.float64) +
+                     rng.normal(0.0, sigma, size=(base.n, 3))).astype(np.float32)
+        out.append(Scene(base.cfg.copy(), st, base.radius.copy(), f"{base.name} member={m}"))
+    return out
+
+
+def ensemble_set_a(members: int = 64, n: int = N_REF, sigma: float = 50e-6,
+                   seed: int = 7) -> list[Scene]:
+    """64 perturbed copies of the 32,768-grain column (2,097,152 grains in all)."""
+    return perturbed_members(column_collapse(n, diameters="uniform", cic=64), members,
+                             sigma, seed)
+
+
+def ensemble_set_b(scenes: int = 256, seed: int = 99, n_min: int = 4096,
+                   n_max: int = 131072) -> list[Scene]:
+    """Heterogeneous design: per scene n log-uniform in [n_min, n_max], aspect ratio
+    H/R uniform in [1, 6] and friction uniform in [0, 0.8] (about 9.4 M grains for
+    the default 256 scenes)."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(math.log(n_min), math.log(n_max), scenes)).astype(np.int64)
+    aspects = rng.uniform(1.0, 6.0, scenes)
+    mus = rng.uniform(0.0, 0.8, scenes)
+    return [column_collapse(int(ns[k]), diameters="uniform", mu=float(mus[k]),
+                            aspect=float(aspects[k]), cic=32, seed=int(seed * 1000 + k))
+            for k in range(scenes)]
 
 
 def dense_box(n: int = 1 << 24, *, phi: float = 0.55, seed: int = 2024, mu: float = 0.5,
@@ -190,3 +229,16 @@ def scene_for(workload: str, n: int | None = None, seed: int | None = None) -> S
     if workload == "dense_16m":
         return dense_box(n or (1 << 24), **kw)
     raise ValueError(f"unknown workload '{workload}'")
+
+
+BATCHED_WORKLOADS = ("ensemble_64x32k", "design_256")
+
+
+def ensemble_for(workload: str) -> list[Scene]:
+    """Named batched workloads: ensemble_64x32k (64 perturbed 32,768-grain columns)
+    and design_256 (256 heterogeneous columns)."""
+    if workload == "ensemble_64x32k":
+        return ensemble_set_a()
+    if workload == "design_256":
+        return ensemble_set_b()
+    raise ValueError(f"unknown batched workload '{workload}'")
