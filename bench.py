@@ -24,6 +24,11 @@ cpu_baseline -- the oracle port (C, OpenMP on all host cores) on a bounded sampl
 Multi-GPU: one process per GPU (torchrun), each rank advancing its own ensemble
 member of the same workload (seed 12345 + rank); no collective on the data path,
 scaling "weak"; only the timing max-reduction uses NCCL.
+
+Batched workloads (--workload ensemble_64x32k: 64 perturbed 32,768-grain columns;
+design_256: 256 columns with n log-uniform in [4096, 131072], H/R in [1, 6], mu in
+[0, 0.8]): all scenes step as one SceneBatch; with N ranks the scenes are shared out
+by grain count (world_b200.batch.shard_scenes), total work fixed ("strong").
 """
 from __future__ import annotations
 
@@ -49,7 +54,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse_args():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="collapse_1m_sie_mu05")
@@ -116,6 +121,14 @@ class ClockSampler:
                  "-lms", "20"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # the timed region starts only once the sampler is producing samples
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            self.fh.flush()
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -203,7 +216,7 @@ def run_reference(args) -> int:
         return 0
     from world_b200.scenes import scene_for
     scene = scene_for(args.workload, n=args.grains, seed=12345)
-    budget = min(180.0, max(10.0, 0.5 * args.steps))
+    budget = min(60.0, max(10.0, 0.5 * args.steps))
     rate, steps, elapsed, threads = cpu_oracle_rate(scene, budget, args.steps,
                                                     warmup=min(args.warmup, 1))
     sample = (f"{steps} of {args.steps} requested steps of the full {scene.n}-grain workload "
@@ -343,6 +356,17 @@ def run_ours(args) -> int:
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e_value = all_grains * args.e2e_steps / (e2e_ms / 1e3)
 
+    scene_results = None
+    if scenes_total:
+        # per-scene energies of every rank's shard, gathered (the batched workloads'
+        # only exchange: a final gather of per-scene results)
+        from world_b200.batch import gather_scene_values
+        energies = sim.scene_energies()
+        if world > 1:
+            energies = gather_scene_values(energies, mine, scenes_total)[:, 0]
+        scene_results = {"scenes": int(len(energies)), "energy_sum_J": float(np.sum(energies)),
+                         "energy_min_J": float(np.min(energies))}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, steps, elapsed, threads = cpu_oracle_rate(scene, args.cpu_seconds, 10_000)
@@ -355,7 +379,8 @@ def run_ours(args) -> int:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "scaling": "strong" if scenes_total else "weak", "vs_baseline": None,
+            "dtype": "fp32",
             "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
             "config": workload_config(scene, args, grains=all_grains, scenes=scenes_total),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -372,6 +397,7 @@ def run_ours(args) -> int:
             "gpu_launches": launches,
             "radix_searches_timed": radix_searches,
             "history_entries_per_grain": entries / n,
+            "scene_results": scene_results,
         }
         print(json.dumps(line), flush=True)
     sim.close()

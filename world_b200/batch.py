@@ -163,3 +163,21 @@ class SceneBatch(ParticleDynamics):
         out = np.empty(3 * len(self.ranges), np.float64)
         check(lib.wd_chaos_metrics(self._h, int(reference_scene), ptr(out)))
         return out.reshape(-1, 3)
+
+
+def gather_scene_values(local: np.ndarray, mine: Sequence[int], total: int, group=None) -> np.ndarray:
+    """Per-scene results of every rank on every rank: ``local`` holds one row per
+    scene in ``mine`` (this rank's shard, in order); the answer holds one row per
+    scene of the whole ensemble. One all-reduce of a (total, width) FP64 array in
+    which each row has a single non-zero contributor, so the sums are exact. Needs
+    an initialised torch.distributed process group (gloo on CPU, NCCL on GPUs)."""
+    import torch
+    import torch.distributed as dist
+
+    loc = np.asarray(local, np.float64).reshape(len(mine), -1)
+    full = np.zeros((total, loc.shape[1]), np.float64)
+    full[list(mine)] = loc
+    device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.from_numpy(full).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy()
