@@ -178,6 +178,23 @@ int wd_get_stream(const wd_sim* sim, void** stream);
 /* Block until all work queued on the handle's stream is done. */
 int wd_synchronize(wd_sim* sim);
 
+/* ---- files and frames ------------------------------------------------------------ */
+
+/* The reference's state file (int32 n + 6n float32 by grain id), readable by its
+ * initialize_from_file (src/particle_dynamics.cu:212-235). */
+int wd_write_state_file(wd_sim* sim, const char* path);
+/* Checkpoint (extension: the reference saves no more than the state file): the state
+ * file at path plus "<path>.sidecar" (magic "WDCKPT01", version 1: time, dt, radius,
+ * mass, material and the tangential springs by grain id). A handle created from it
+ * with the same config continues bit for bit as the saved one would have. Single-scene
+ * handles only. */
+int wd_write_checkpoint(wd_sim* sim, const char* path);
+int wd_create_from_checkpoint(const wd_config* cfg, const char* path, wd_sim** out);
+/* The broadcast frame of src/broadcast.cpp:95-108: frame[0..3n) positions by grain id,
+ * frame[3n] = simulated time, frame[3n+1..3n+5] = meta5 (real-time ratio,
+ * find-neighbors, compute-rhs, take-step and unpack times in ms; NULL: zeros). */
+int wd_pack_frame(wd_sim* sim, const float* meta5, float* frame);
+
 /* ---- tangential history (extension: no reference counterpart) ------------------- */
 
 /* Per grain id: count[n], partner[n*WD_HIST_CAP] (grain id, or -1-2a / -2-2a for the

@@ -163,3 +163,41 @@ def test_create_errors_are_statuses(tmp_path):
         ParticleDynamics(cfg)
     with pytest.raises(ValueError):
         ParticleDynamics(SimConfig(), state=np.zeros((4, 6), np.float32), radius=np.ones(3, np.float32))
+
+
+def test_checkpoint_resume_is_bit_identical(tmp_path):
+    from test_gpu_parity import packed_poly
+    from world_b200.state_io import read_checkpoint, read_state_file
+    cfg, st, rad = packed_poly(n=1500, seed=31, mu=0.5)
+    a = ParticleDynamics(cfg, state=st, radius=rad)
+    a.advance(60)
+    a.dt = 8e-6                      # the checkpoint carries dt too
+    a.advance(5)
+    path = str(tmp_path / "ck.bin")
+    a.write_checkpoint(path)
+    ck = read_checkpoint(path)
+    np.testing.assert_array_equal(ck["state"].reshape(-1), a.get_state())
+    assert ck["time"] == np.float32(a.time) and ck["dt"] == np.float32(8e-6)
+    cnt, part, xi = a.get_history()
+    np.testing.assert_array_equal(ck["count"], cnt)
+    assert cnt.sum() > 0
+    a.advance(40)
+    b = ParticleDynamics.from_checkpoint(cfg, path)
+    assert b.time == ck["time"]
+    b.advance(40)
+    np.testing.assert_array_equal(b.get_state(), a.get_state())
+    assert b.time == a.time
+    c1, p1, x1 = a.get_history()
+    c2, p2, x2 = b.get_history()
+    np.testing.assert_array_equal(c1, c2)
+    live = (np.arange(p1.size) % 24) < np.repeat(c1, 24)
+    np.testing.assert_array_equal(p1[live], p2[live])
+    np.testing.assert_array_equal(x1.reshape(-1, 3)[live], x2.reshape(-1, 3)[live])
+    # the state file alone is the reference's format
+    a.write_state_file(str(tmp_path / "s.bin"))
+    np.testing.assert_array_equal(read_state_file(str(tmp_path / "s.bin")).reshape(-1), a.get_state())
+    frame = a.pack_frame([1.0, 2.0, 3.0, 4.0, 5.0])
+    np.testing.assert_array_equal(frame[:3 * a.n], a.get_positions())
+    assert frame[3 * a.n] == np.float32(a.time)
+    np.testing.assert_array_equal(frame[3 * a.n + 1:], [1, 2, 3, 4, 5])
+    a.close(); b.close()

@@ -95,3 +95,45 @@ def test_grain_properties_table_and_density():
     cfg.physics.density = 2500.0
     r, m = grain_properties(cfg, mat, np.float32([0.0025, 0.003, 0.0025]))
     assert np.allclose(m, 2500 * 4 / 3 * np.pi * np.float64(r) ** 3, rtol=1e-6)
+
+
+def test_checkpoint_reader_and_missing_sidecar(tmp_path):
+    import ctypes
+    from world_b200 import SimConfig, WorldError
+    from world_b200._lib import check, lib
+    from world_b200.state_io import read_checkpoint, write_state_file
+    n = 5
+    rng = np.random.default_rng(1)
+    st = rng.random((n, 6)).astype(np.float32)
+    path = tmp_path / "c.bin"
+    write_state_file(path, st)
+    h = ctypes.c_void_p()
+    cfg = SimConfig()
+    # a state file without its sidecar is not a checkpoint (checked before any device call)
+    with pytest.raises(WorldError, match="sidecar"):
+        check(lib.wd_create_from_checkpoint(cfg.handle, str(path).encode(), ctypes.byref(h)))
+    with pytest.raises(WorldError, match="cannot read"):
+        check(lib.wd_create_from_checkpoint(cfg.handle, str(tmp_path / "none.bin").encode(),
+                                            ctypes.byref(h)))
+    r, m = rng.random(n).astype(np.float32), rng.random(n).astype(np.float32)
+    mat = np.arange(n, dtype=np.int32)
+    cnt = np.array([0, 2, 1, 0, 3], np.int32)
+    part = rng.integers(-6, n, n * 24).astype(np.int32)
+    xi = rng.random(n * 24 * 3).astype(np.float32)
+    with open(str(path) + ".sidecar", "wb") as f:
+        f.write(b"WDCKPT01")
+        f.write(np.array([1, 1], "<u4").tobytes())
+        f.write(np.array([n], "<i8").tobytes())
+        f.write(np.array([0.25, 1e-5], "<f4").tobytes())
+        for a in (r, m, mat, cnt, part, xi):
+            f.write(a.tobytes())
+    ck = read_checkpoint(path)
+    np.testing.assert_array_equal(ck["state"], st)
+    assert ck["time"] == np.float32(0.25) and ck["dt"] == np.float32(1e-5)
+    for k, a in (("radius", r), ("mass", m), ("material", mat), ("count", cnt),
+                 ("partner", part), ("xi", xi)):
+        np.testing.assert_array_equal(ck[k], a)
+    with open(str(path) + ".sidecar", "ab") as f:
+        f.write(b"\0")
+    with pytest.raises(ValueError, match="trailing"):
+        read_checkpoint(path)

@@ -70,6 +70,10 @@ SIGNATURES = {
     "wd_scene_stability": ([_p, _p], c_int),
     "wd_freeze_scene": ([_p, c_int32, c_int32], c_int),
     "wd_chaos_metrics": ([_p, c_int32, _p], c_int),
+    "wd_write_state_file": ([_p, c_char_p], c_int),
+    "wd_write_checkpoint": ([_p, c_char_p], c_int),
+    "wd_create_from_checkpoint": ([_p, c_char_p, POINTER(c_void_p)], c_int),
+    "wd_pack_frame": ([_p, _p, _p], c_int),
     "wd_destroy": ([_p], c_int),
     "wd_step": ([_p, c_int64], c_int),
     "wd_set_dt": ([_p, c_float], c_int),

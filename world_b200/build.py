@@ -29,7 +29,7 @@ CUDA_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-fmad=false",
 BIN = os.path.join(HERE, "bin")
 DRIVERS = ["dataset", "chaos"]
 SOURCES = ["wd_search.cu", "wd_contact.cu", "wd_fields.cu", "wd_ensemble.cu", "wd_sim.cu",
-           "wd_config.cpp"]
+           "wd_config.cpp", "wd_io.cpp"]
 
 
 def nvcc() -> str:

@@ -81,6 +81,20 @@ class ParticleDynamics:
         self.time_unpack_state = 0.0
         self.unpack_state()
 
+    @classmethod
+    def from_checkpoint(cls, config: SimConfig, path: str) -> "ParticleDynamics":
+        """Resume from write_checkpoint(path): state, time, dt, radii, masses, materials
+        and tangential springs; the run continues bit for bit."""
+        obj = cls.__new__(cls)
+        obj.config = config
+        h = ctypes.c_void_p()
+        check(lib.wd_create_from_checkpoint(config.handle, str(path).encode(), ctypes.byref(h)))
+        obj._attach(h)
+        dt = ctypes.c_float()
+        check(lib.wd_get_dt(h, ctypes.byref(dt)))
+        obj._dt = float(dt.value)
+        return obj
+
     # -- lifetime --------------------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -174,6 +188,26 @@ class ParticleDynamics:
         import torch
         torch.cuda.current_stream().synchronize()
         check(lib.wd_set_state_device(self._h, ptr(t.contiguous())))
+
+    # -- files and frames ------------------------------------------------------------
+    def write_state_file(self, path: str) -> None:
+        """The reference's state file (int32 n + 6n float32), for initialize_from_file."""
+        check(lib.wd_write_state_file(self._h, str(path).encode()))
+
+    def write_checkpoint(self, path: str) -> None:
+        """State file at path plus path + ".sidecar" (time, dt, radii, masses,
+        materials, tangential springs) for a bit-identical resume."""
+        check(lib.wd_write_checkpoint(self._h, str(path).encode()))
+
+    def pack_frame(self, meta5=None) -> np.ndarray:
+        """The broadcast frame: 3n positions, time, then the five meta floats
+        (real-time ratio and the four phase times in ms)."""
+        out = np.empty(3 * self.n + 6, np.float32)
+        m = None if meta5 is None else np.ascontiguousarray(meta5, np.float32)
+        if m is not None and m.size != 5:
+            raise ValueError("meta5 needs 5 floats")
+        check(lib.wd_pack_frame(self._h, ptr(m), ptr(out)))
+        return out
 
     # -- tangential history ----------------------------------------------------------
     def get_history(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:

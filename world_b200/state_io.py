@@ -3,6 +3,11 @@
 State file (reader: src/particle_dynamics.cu:212-235; writer:
 surrogate/decode_particles.py:355-361): little-endian int32 n, then n*6 float32 laid
 out [x, y, z, vx, vy, vz] per grain. Grains get `initialization.particle_material`.
+
+Checkpoint sidecar ("<state file>.sidecar", written by wd_write_checkpoint):
+"WDCKPT01", uint32 version 1, uint32 flags (bit 0: springs), int64 n, float32 time,
+float32 dt, float32 radius[n], float32 mass[n], int32 material[n], and with springs
+int32 count[n], int32 partner[n*24], float32 xi[n*24*3]; little-endian, by grain id.
 """
 from __future__ import annotations
 
@@ -63,3 +68,37 @@ def read_state_file(path: str | os.PathLike) -> np.ndarray:
     if body.size < 6 * n:
         raise ValueError(f"{path}: short of {6 * n} floats")
     return body[:6 * n].reshape(n, 6).copy()
+
+
+CKPT_MAGIC = b"WDCKPT01"
+HIST_CAP = 24
+
+
+def read_checkpoint(path: str | os.PathLike) -> dict:
+    """The state file at path and its sidecar as arrays (a reader for tooling)."""
+    state = read_state_file(path)
+    n = state.shape[0]
+    with open(str(path) + ".sidecar", "rb") as f:
+        raw = f.read()
+    if raw[:8] != CKPT_MAGIC:
+        raise ValueError(f"{path}.sidecar: bad magic {raw[:8]!r}")
+    version, flags = (int(v) for v in np.frombuffer(raw[8:16], "<u4"))
+    if version != 1:
+        raise ValueError(f"{path}.sidecar: version {version}")
+    sn = int(np.frombuffer(raw[16:24], "<i8")[0])
+    if sn != n:
+        raise ValueError(f"{path}.sidecar: {sn} grains, state file has {n}")
+    time, dt = (float(v) for v in np.frombuffer(raw[24:32], "<f4"))
+    o = 32
+    out = {"state": state, "time": np.float32(time), "dt": np.float32(dt)}
+    for name, dtype, count in (("radius", "<f4", n), ("mass", "<f4", n), ("material", "<i4", n)):
+        out[name] = np.frombuffer(raw[o:o + 4 * count], dtype).copy()
+        o += 4 * count
+    if flags & 1:
+        for name, dtype, count in (("count", "<i4", n), ("partner", "<i4", n * HIST_CAP),
+                                   ("xi", "<f4", n * HIST_CAP * 3)):
+            out[name] = np.frombuffer(raw[o:o + 4 * count], dtype).copy()
+            o += 4 * count
+    if o != len(raw):
+        raise ValueError(f"{path}.sidecar: {len(raw) - o} trailing bytes")
+    return out
