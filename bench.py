@@ -25,6 +25,9 @@ Multi-GPU: one process per GPU (torchrun), each rank advancing its own ensemble
 member of the same workload (seed 12345 + rank); no collective on the data path,
 scaling "weak"; only the timing max-reduction uses NCCL.
 
+--workload adjoint_32k: the reverse pass (world_b200.adjoint) over a 200-step window of
+the 32,768-grain column, its throughput and its cost relative to the forward window.
+
 Batched workloads (--workload ensemble_64x32k: 64 perturbed 32,768-grain columns;
 design_256: 256 columns with n log-uniform in [4096, 131072], H/R in [1, 6], mu in
 [0, 0.8]): all scenes step as one SceneBatch; with N ranks the scenes are shared out
@@ -407,10 +410,91 @@ def run_ours(args) -> int:
     return 0
 
 
+def run_adjoint(args) -> int:
+    """Gradient of a density loss over a 200-step window of the 32,768-grain column
+    after 12,000 steps (0.12 s: the lower layers have reached the floor and the column
+    is collapsing; before about 2,700 steps the lattice falls without a contact): loss = mean((rho_64^3(T) - rho_target)^2), target
+    from the same window with mu = 0.4, e = 0.6; gradients in v0 and (mu, e, k_n).
+    Reports the window's reverse pass in grain-steps/s and its cost relative to the
+    plain forward window on the same GPU. One GPU."""
+    import numpy as np
+    import torch
+
+    from world_b200 import ParticleDynamics
+    from world_b200.adjoint import deposit, window
+    from world_b200.scenes import column_collapse
+
+    if env_int("RANK", 0) != 0:
+        return 0
+    torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+    scene = column_collapse(32768, diameters="uniform", cic=64)
+    cfg = scene.cfg
+    cfg.kernel_timing = False
+    ph = cfg.physics
+    mu, e, k = float(ph.friction), float(ph.restitution), float(ph.normal_stiffness)
+    sim = ParticleDynamics(cfg, state=scene.state, radius=scene.radius)
+    pre_roll = 12000
+    sim.advance(pre_roll)
+    start = torch.from_numpy(sim.get_state()).cuda().reshape(-1, 6)
+    x0, v0 = start[:, :3].contiguous(), start[:, 3:].contiguous()
+    steps, every = 200, 20
+    stream = torch.cuda.ExternalStream(sim.stream_ptr())
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return out, a.elapsed_time(b)
+
+    # target field: the same window with mu = 0.4, e = 0.6
+    sim.set_contact_params(0.4, 0.6, k)
+    sim.set_state_tensor(start.reshape(-1))
+    sim.advance(steps)
+    sim.compute_density_grid()
+    target = torch.from_numpy(sim.host_density_grid[:sim.density_grid_nodes()].copy()).cuda()
+    target = target.reshape(cfg.density_grid_size_x, cfg.density_grid_size_y, cfg.density_grid_size_z)
+    sim.set_contact_params(mu, e, k)
+    for _ in range(max(1, args.warmup // 3)):
+        sim.set_state_tensor(start.reshape(-1))
+        sim.advance(steps)
+    sim.set_state_tensor(start.reshape(-1))
+    _, fwd_ms = timed(lambda: sim.advance(steps))
+
+    tv0 = v0.clone().requires_grad_(True)
+    theta = torch.tensor([mu, e, k], dtype=torch.float64, requires_grad=True)
+    (x, v), rec_ms = timed(lambda: window(sim, x0, tv0, theta, steps, every))
+    grid = deposit(sim, x, v)
+    loss = ((grid[0].double() - target.double()) ** 2).mean()
+    _, bwd_ms = timed(lambda: loss.backward())
+    n = sim.n
+    line = {
+        "metric": "adjoint grain-steps/s, 200-step window at 32,768 grains FP32",
+        "value": n * steps / (bwd_ms / 1e3), "unit": "grain-steps/s", "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "fp32",
+        "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
+        "config": {"workload": "adjoint_32k", "grains": n, "pre_roll_steps": pre_roll,
+                   "window_steps": steps, "checkpoint_every": every, "cic_grid": 64,
+                   "loss": "mean((rho_T - rho_target)^2), target mu=0.4 e=0.6"},
+        "forward_window_ms": fwd_ms, "record_ms": rec_ms, "backward_ms": bwd_ms,
+        "record_over_forward": rec_ms / fwd_ms, "backward_over_forward": bwd_ms / fwd_ms,
+        "loss": float(loss.detach()),
+        "grad_theta": theta.grad.tolist(),
+        "grad_v0_norm": float(tv0.grad.norm()),
+    }
+    print(json.dumps(line), flush=True)
+    sim.close()
+    return 0
+
+
 def main() -> int:
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "adjoint_32k":
+        return run_adjoint(args)
     return run_ours(args)
 
 

@@ -195,6 +195,32 @@ int wd_create_from_checkpoint(const wd_config* cfg, const char* path, wd_sim** o
  * find-neighbors, compute-rhs, take-step and unpack times in ms; NULL: zeros). */
 int wd_pack_frame(wd_sim* sim, const float* meta5, float* frame);
 
+/* ---- reverse pass (extension: the reference has no derivatives) ------------------
+ * Gradients of a loss on the state at the end of a window of semi-implicit Euler
+ * steps with respect to the state at its start and to the contact parameters
+ * (mu, restitution, k_n), by a hand-written adjoint of the fused contact + integrator
+ * step: the contact set and the clamp / stick-slip / viscous-cap branches of each
+ * step are those the forward took. The window is recorded with checkpoints every
+ * checkpoint_every steps; the reverse pass replays one segment at a time from its
+ * checkpoint. Single-scene handles; semi-implicit Euler only. */
+
+/* mu, restitution and k_n (physics.normal_stiffness; k_t follows as 2/7 k_n unless
+ * physics.tangential_stiffness is set) of a live handle. */
+int wd_set_contact_params(wd_sim* sim, float mu, float restitution, float k_n);
+/* steps x take_step() from the current state, keeping the checkpoints.
+ * WD_ERR_CAPACITY if a grain ran out of spring slots in the window. */
+int wd_adjoint_record(wd_sim* sim, int64_t steps, int32_t checkpoint_every);
+/* Device pointers, AoS3 by grain id: d_gx, d_gv = dL/dx, dL/dv at the window's end
+ * (NULL: zero); d_gx0, d_gv0 receive dL/dx, dL/dv at its start (NULL: skipped);
+ * theta3 (host) receives dL/dmu, dL/de, dL/dk_n. The handle is left at the window's
+ * end, as after wd_adjoint_record. */
+int wd_adjoint_backward(wd_sim* sim, const float* d_gx, const float* d_gv, float* d_gx0,
+                        float* d_gv0, double* theta3);
+/* Adjoint of compute_density_grid at the current state: d_ggrid (device, 4*nodes,
+ * channel-major) = dL/dgrid; d_gx, d_gv (device, AoS3 by grain id) receive dL/dx and
+ * dL/dv. The CIC weights are differentiated inside their cells. */
+int wd_deposit_vjp(wd_sim* sim, const float* d_ggrid, float* d_gx, float* d_gv);
+
 /* ---- tangential history (extension: no reference counterpart) ------------------- */
 
 /* Per grain id: count[n], partner[n*WD_HIST_CAP] (grain id, or -1-2a / -2-2a for the

@@ -101,5 +101,12 @@ def test_batch_entry_points_take_the_python_argument_forms():
         lib.wd_scene_count(None, ctypes.byref(s)),
         lib.wd_scene_range(None, 0, *[ctypes.byref(x) for x in v]),
         lib.wd_create_batch(None, 0, None, None, None, None, None, ctypes.byref(ctypes.c_void_p())),
+        lib.wd_set_contact_params(None, 0.5, 0.5, 1e5),
+        lib.wd_adjoint_record(None, 10, 5),
+        lib.wd_adjoint_backward(None, ptr(d), ptr(d), ptr(d), ptr(d), ptr(d)),
+        lib.wd_deposit_vjp(None, ptr(d), ptr(d), ptr(d)),
+        lib.wd_write_state_file(None, b"x"),
+        lib.wd_write_checkpoint(None, b"x"),
+        lib.wd_pack_frame(None, None, ptr(d)),
     ]
     assert all(c == -1 for c in calls), calls

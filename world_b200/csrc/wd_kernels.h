@@ -175,6 +175,30 @@ void launch_stability(const DevParams& P, SceneTab T, const float4* pos,
 
 int reduction_blocks(int n);
 
+// Reverse pass (wd_adjoint.cu). Adjoint arrays are float4 (x, y, z, unused) by grain
+// id; spring rows are kHistCap entries per grain id.
+struct AdjArgs {
+    const float4* pos; const float4* vel; const int* ids;  // sorted state of step t
+    const int2* table;
+    const float4* hist_in; const int* hcnt_in;     // springs at t (counts by sorted slot)
+    const float4* hist_next; const int* hcnt_next; // springs at t+1 (counts by id)
+    const float4* lx; const float4* lvt; const float4* lf; const float4* lxi;
+    float4* lx_out; float4* lv_out; float4* lxi_out;
+    double* theta;                                  // [3][n], accumulated
+    int kt_from_kn;
+};
+void launch_adj_prep(int n, float dt, const float4* vel, const int* ids, const float4* lx,
+                     const float4* lv, float4* lvt, float4* lf, cudaStream_t st);
+void launch_adj_step(const DevParams& P, const AdjArgs& a, cudaStream_t st);
+void launch_counts_by_id(int n, const int* ids, const int* cnt_slot, int* cnt_id,
+                         cudaStream_t st);
+// AoS3 floats by grain id <-> float4 by grain id (a == nullptr: zeros).
+void launch_aos3_to_f4(int n, const float* a, float4* o, cudaStream_t st);
+void launch_f4_to_aos3(int n, const float4* a, float* o, cudaStream_t st);
+void launch_deposit_vjp(int n, const float4* pos, const float4* vel, const int* ids,
+                        const float* lo, const float* hi, const int* size, const float* g,
+                        float4* gx, float4* gv, cudaStream_t st);
+
 // Ensemble metrics (wd_ensemble.cu): per scene, the sum over grains of the squared
 // separation from the reference scene's grain with the same index (grain_sums), and
 // the six node sums sum (rho - rho_ref)^2, sum rho_ref^2, sum rho, sum rho*ix,

@@ -8,6 +8,7 @@
 //     contact+integrate), instead of eleven launches each followed by
 //     cudaDeviceSynchronize (src/kernel.cu:31-38);
 //   * errors come back as status codes; nothing calls exit() or abort().
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -122,6 +123,29 @@ struct wd_sim {
     double* grain_sums = nullptr;         // 1 per scene
     float* chaos_grid = nullptr;          // 4 * nodes floats
 
+    // reverse pass: snapshots of the step state (checkpoints of a recorded window and
+    // the states of the segment being replayed) and the adjoint buffers
+    struct Snap {
+        float4* pos = nullptr;
+        float4* vel = nullptr;
+        int* ids = nullptr;
+        uint32_t* keys = nullptr;
+        int* hcnt = nullptr;
+        float4* hist = nullptr;
+        float time = 0.f;
+    };
+    std::vector<Snap> adj_ckpt, adj_seg;
+    Snap adj_end;
+    int64_t adj_steps = 0;
+    int adj_every = 0;
+    float4* adj_lx[2] = {nullptr, nullptr};
+    float4* adj_lv[2] = {nullptr, nullptr};
+    float4* adj_lxi[2] = {nullptr, nullptr};
+    float4* adj_lvt = nullptr;
+    float4* adj_lf = nullptr;
+    int* adj_cnt_next = nullptr;
+    double* adj_theta = nullptr;
+
     unsigned long long* counters = nullptr;
     uint32_t* picard_res = nullptr;
     int* picard_used = nullptr;
@@ -160,6 +184,71 @@ void destroy_graphs(wd_sim* s) {
     s->graph_dirty = true;
 }
 
+// ---- snapshots of the step state, for the reverse pass ---------------------------
+
+void free_snap(wd_sim::Snap& q) {
+    void* ptrs[] = {q.pos, q.vel, q.ids, q.keys, q.hcnt, q.hist};
+    for (void* p : ptrs) cudaFree(p);
+    q = wd_sim::Snap{};
+}
+
+void free_tape(wd_sim* s) {
+    for (auto& q : s->adj_ckpt) free_snap(q);
+    for (auto& q : s->adj_seg) free_snap(q);
+    free_snap(s->adj_end);
+    s->adj_ckpt.clear();
+    s->adj_seg.clear();
+    s->adj_steps = 0;
+    s->adj_every = 0;
+}
+
+cudaError_t alloc_snap(wd_sim* s, wd_sim::Snap& q) {
+    const size_t n = static_cast<size_t>(s->n);
+    cudaError_t e = dalloc(&q.pos, n);
+    if (e == cudaSuccess) e = dalloc(&q.vel, n);
+    if (e == cudaSuccess) e = dalloc(&q.ids, n);
+    if (e == cudaSuccess) e = dalloc(&q.keys, n);
+    if (e == cudaSuccess && s->P.history) e = dalloc(&q.hcnt, n);
+    if (e == cudaSuccess && s->P.history) e = dalloc(&q.hist, n * wd::kHistCap);
+    return e;
+}
+
+// The state a step reads: sorted state, the keys of its slots (the incremental search
+// compares against them), the stored springs and their counts, and the time.
+cudaError_t take_snap(wd_sim* s, wd_sim::Snap& q) {
+    const size_t n = static_cast<size_t>(s->n);
+    cudaStream_t st = s->stream;
+    cudaError_t e = cudaMemcpyAsync(q.pos, s->posA, n * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q.vel, s->velA, n * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q.ids, s->idsA, n * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q.keys, s->sb.slot_keys, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && s->P.history) {
+        e = cudaMemcpyAsync(q.hcnt, s->hcnt_slot, n * sizeof(int), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(q.hist, s->hist[s->hist_cur], n * wd::kHistCap * sizeof(float4),
+                                cudaMemcpyDeviceToDevice, st);
+    }
+    q.time = s->time;
+    return e;
+}
+
+cudaError_t put_snap(wd_sim* s, const wd_sim::Snap& q) {
+    const size_t n = static_cast<size_t>(s->n);
+    cudaStream_t st = s->stream;
+    cudaError_t e = cudaMemcpyAsync(s->posA, q.pos, n * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->velA, q.vel, n * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->idsA, q.ids, n * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->sb.slot_keys, q.keys, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && s->P.history) {
+        e = cudaMemcpyAsync(s->hcnt_slot, q.hcnt, n * sizeof(int), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(s->hist[s->hist_cur], q.hist, n * wd::kHistCap * sizeof(float4),
+                                cudaMemcpyDeviceToDevice, st);
+    }
+    s->time = q.time;
+    return e;
+}
+
 void free_sim(wd_sim* s) {
     if (!s) return;
     destroy_graphs(s);
@@ -182,6 +271,10 @@ void free_sim(wd_sim* s) {
         if (b) cudaFree(b);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : s->ev_pending) cudaEventDestroy(e);
+    free_tape(s);
+    void* adj[] = {s->adj_lx[0], s->adj_lx[1], s->adj_lv[0], s->adj_lv[1], s->adj_lxi[0],
+                   s->adj_lxi[1], s->adj_lvt, s->adj_lf, s->adj_cnt_next, s->adj_theta};
+    for (void* p : adj) cudaFree(p);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     if (s->aux_stream) cudaStreamDestroy(s->aux_stream);
     delete s;
@@ -1295,6 +1388,187 @@ int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* c
     cudaFree(d_contact);
     WD_CUDA(e);
     return WD_OK;
+}
+
+// ---- reverse pass -------------------------------------------------------------------
+
+int wd_set_contact_params(wd_sim* sim, float mu, float restitution, float k_n) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_set_contact_params: NULL handle");
+    if (sim->scenes != 1) return fail(WD_ERR_INVALID, "wd_set_contact_params: not for a batch of scenes");
+    if (!(k_n > 0.f) || !(mu >= 0.f) || !(restitution >= 0.f))
+        return fail(WD_ERR_INVALID, "wd_set_contact_params: need mu >= 0, restitution >= 0, k_n > 0");
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    sim->cfg.friction = mu;
+    sim->cfg.restitution = restitution;
+    sim->cfg.normal_stiffness = k_n;
+    const float rmax = sim->P.rmax;
+    sim->P = make_params(sim->cfg, sim->n, sim->dt);
+    sim->P.rmax = rmax;
+    sim->scene_P[0] = sim->P;
+    sim->scene_cfg[0] = sim->cfg;
+    sim->graph_dirty = true;
+    return WD_OK;
+}
+
+int wd_adjoint_record(wd_sim* sim, int64_t steps, int32_t checkpoint_every) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_adjoint_record: NULL handle");
+    if (sim->picard) return fail(WD_ERR_INVALID, "wd_adjoint_record: the reverse pass covers semi-implicit Euler only");
+    if (sim->scenes != 1) return fail(WD_ERR_INVALID, "wd_adjoint_record: not for a batch of scenes");
+    if (steps < 1 || checkpoint_every < 1) return fail(WD_ERR_INVALID, "wd_adjoint_record: steps and checkpoint_every must be >= 1");
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    free_tape(sim);
+    const int64_t nck = (steps + checkpoint_every - 1) / checkpoint_every;
+    sim->adj_ckpt.resize(static_cast<size_t>(nck));
+    for (auto& q : sim->adj_ckpt) WD_CUDA(alloc_snap(sim, q));
+    WD_CUDA(alloc_snap(sim, sim->adj_end));
+    int64_t hist_over0 = 0;
+    rc = read_counter(sim, wd::kCntHistOverflow, &hist_over0);
+    if (rc) return rc;
+    for (int64_t k = 0; k < steps; ++k) {
+        if (k % checkpoint_every == 0) WD_CUDA(take_snap(sim, sim->adj_ckpt[static_cast<size_t>(k / checkpoint_every)]));
+        rc = wd_step(sim, 1);
+        if (rc) return rc;
+    }
+    WD_CUDA(take_snap(sim, sim->adj_end));
+    int64_t hist_over1 = 0;
+    rc = read_counter(sim, wd::kCntHistOverflow, &hist_over1);
+    if (rc) return rc;
+    sim->adj_steps = steps;
+    sim->adj_every = checkpoint_every;
+    if (hist_over1 != hist_over0)
+        return fail(WD_ERR_CAPACITY, "wd_adjoint_record: a grain ran out of spring slots in the "
+                                     "window; the reverse pass needs every spring stored");
+    return WD_OK;
+}
+
+int wd_adjoint_backward(wd_sim* sim, const float* d_gx, const float* d_gv, float* d_gx0,
+                        float* d_gv0, double* theta3) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_adjoint_backward: NULL handle");
+    if (sim->adj_steps < 1) return fail(WD_ERR_INVALID, "wd_adjoint_backward: no window recorded (wd_adjoint_record)");
+    const int n = sim->n;
+    cudaStream_t st = sim->stream;
+    const bool hist = sim->P.history != 0;
+    if (!sim->adj_lvt) {
+        for (int b = 0; b < 2; ++b) {
+            WD_CUDA(dalloc(&sim->adj_lx[b], n));
+            WD_CUDA(dalloc(&sim->adj_lv[b], n));
+            if (hist) WD_CUDA(dalloc(&sim->adj_lxi[b], static_cast<size_t>(n) * wd::kHistCap));
+        }
+        WD_CUDA(dalloc(&sim->adj_lvt, n));
+        WD_CUDA(dalloc(&sim->adj_lf, n));
+        WD_CUDA(dalloc(&sim->adj_cnt_next, n));
+        WD_CUDA(dalloc(&sim->adj_theta, static_cast<size_t>(3) * n));
+    }
+    const int every = sim->adj_every;
+    if (sim->adj_seg.size() < static_cast<size_t>(every) + 1) {
+        const size_t old = sim->adj_seg.size();
+        sim->adj_seg.resize(static_cast<size_t>(every) + 1);
+        for (size_t k = old; k < sim->adj_seg.size(); ++k) WD_CUDA(alloc_snap(sim, sim->adj_seg[k]));
+    }
+    unsigned long long saved[wd::kNumCounters];
+    WD_CUDA(cudaMemcpyAsync(saved, sim->counters, sizeof(saved), cudaMemcpyDeviceToHost, st));
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+
+    int cur = 0;
+    wd::launch_aos3_to_f4(n, d_gx, sim->adj_lx[0], st);
+    wd::launch_aos3_to_f4(n, d_gv, sim->adj_lv[0], st);
+    if (hist)
+        WD_CUDA(cudaMemsetAsync(sim->adj_lxi[0], 0, sizeof(float4) * n * wd::kHistCap, st));
+    WD_CUDA(cudaMemsetAsync(sim->adj_theta, 0, sizeof(double) * 3 * n, st));
+    const DevParams& P = sim->P;
+    const wd::Skip none{nullptr, 0.f};
+    const int64_t nseg = static_cast<int64_t>(sim->adj_ckpt.size());
+    for (int64_t seg = nseg - 1; seg >= 0; --seg) {
+        const int64_t s0 = seg * every;
+        const int len = static_cast<int>(std::min<int64_t>(sim->adj_steps, s0 + every) - s0);
+        // replay the segment from its checkpoint, keeping every step's state
+        WD_CUDA(put_snap(sim, sim->adj_ckpt[static_cast<size_t>(seg)]));
+        for (int k = 0; k < len; ++k) {
+            rc = wd_step(sim, 1);
+            if (rc) return rc;
+            WD_CUDA(take_snap(sim, sim->adj_seg[static_cast<size_t>(k) + 1]));
+        }
+        for (int t = len - 1; t >= 0; --t) {
+            const wd_sim::Snap& now = t == 0 ? sim->adj_ckpt[static_cast<size_t>(seg)]
+                                             : sim->adj_seg[static_cast<size_t>(t)];
+            const wd_sim::Snap& next = sim->adj_seg[static_cast<size_t>(t) + 1];
+            WD_CUDA(put_snap(sim, now));
+            // the step's neighbor search and gather, as the forward ran them
+            wd::launch_search(P, tab(sim, sim->sceneA), sim->posA, sim->idsA, sim->sb, none,
+                              nullptr, 0, sim->counters, st);
+            wd::launch_gather(P, sim->sb, sim->posA, sim->velA, sim->posB, sim->velB, sim->idsB,
+                              nullptr, nullptr, nullptr, nullptr, false,
+                              hist ? sim->hcnt_slot : nullptr, hist ? sim->hcnt_g : nullptr,
+                              nullptr, nullptr, false, sim->counters, nullptr, nullptr, none, st);
+            if (hist) {
+                wd::launch_counts_by_id(n, next.ids, next.hcnt, sim->adj_cnt_next, st);
+                WD_CUDA(cudaMemsetAsync(sim->adj_lxi[cur ^ 1], 0, sizeof(float4) * n * wd::kHistCap, st));
+            }
+            wd::launch_adj_prep(n, P.dt, sim->velB, sim->idsB, sim->adj_lx[cur], sim->adj_lv[cur],
+                                sim->adj_lvt, sim->adj_lf, st);
+            wd::AdjArgs a{};
+            a.pos = sim->posB; a.vel = sim->velB; a.ids = sim->idsB; a.table = sim->sb.table;
+            a.hist_in = hist ? now.hist : nullptr;
+            a.hcnt_in = hist ? sim->hcnt_g : nullptr;
+            a.hist_next = hist ? next.hist : nullptr;
+            a.hcnt_next = hist ? sim->adj_cnt_next : nullptr;
+            a.lx = sim->adj_lx[cur]; a.lvt = sim->adj_lvt; a.lf = sim->adj_lf;
+            a.lxi = hist ? sim->adj_lxi[cur] : nullptr;
+            a.lx_out = sim->adj_lx[cur ^ 1]; a.lv_out = sim->adj_lv[cur ^ 1];
+            a.lxi_out = hist ? sim->adj_lxi[cur ^ 1] : nullptr;
+            a.theta = sim->adj_theta;
+            a.kt_from_kn = sim->cfg.tangential_stiffness > 0.f ? 0 : 1;
+            wd::launch_adj_step(P, a, st);
+            WD_CUDA(cudaGetLastError());
+            cur ^= 1;
+        }
+    }
+    if (d_gx0) wd::launch_f4_to_aos3(n, sim->adj_lx[cur], d_gx0, st);
+    if (d_gv0) wd::launch_f4_to_aos3(n, sim->adj_lv[cur], d_gv0, st);
+    wd::launch_segment_sums(sim->adj_theta, n, 3, segments(sim), sim->partials, sim->scene_sums, st);
+    WD_CUDA(cudaGetLastError());
+    double th[3];
+    WD_CUDA(cudaMemcpyAsync(th, sim->scene_sums, sizeof(th), cudaMemcpyDeviceToHost, st));
+    // back to the window's end, counters as they were
+    WD_CUDA(put_snap(sim, sim->adj_end));
+    WD_CUDA(cudaMemcpyAsync(sim->counters, saved, sizeof(saved), cudaMemcpyHostToDevice, st));
+    rc = sync_stream(sim);
+    if (rc) return rc;
+    if (theta3) {
+        const float e = sim->cfg.restitution;
+        theta3[0] = th[0];
+        theta3[1] = (e > 0.f && e < 1.f) ? th[1] / static_cast<double>(e) : 0.0;
+        theta3[2] = th[2];
+    }
+    return WD_OK;
+}
+
+int wd_deposit_vjp(wd_sim* sim, const float* d_ggrid, float* d_gx, float* d_gv) {
+    if (!sim || !d_ggrid) return fail(WD_ERR_INVALID, "wd_deposit_vjp: NULL argument");
+    if (sim->scenes != 1) return fail(WD_ERR_INVALID, "wd_deposit_vjp: not for a batch of scenes");
+    const int n = sim->n;
+    if (!sim->adj_lvt) {
+        for (int b = 0; b < 2; ++b) {
+            WD_CUDA(dalloc(&sim->adj_lx[b], n));
+            WD_CUDA(dalloc(&sim->adj_lv[b], n));
+        }
+        WD_CUDA(dalloc(&sim->adj_lvt, n));
+        WD_CUDA(dalloc(&sim->adj_lf, n));
+        WD_CUDA(dalloc(&sim->adj_cnt_next, n));
+        WD_CUDA(dalloc(&sim->adj_theta, static_cast<size_t>(3) * n));
+        if (sim->P.history)
+            for (int b = 0; b < 2; ++b)
+                WD_CUDA(dalloc(&sim->adj_lxi[b], static_cast<size_t>(n) * wd::kHistCap));
+    }
+    wd::launch_deposit_vjp(n, sim->posA, sim->velA, sim->idsA, sim->cfg.dom_lo, sim->cfg.dom_hi,
+                           sim->cfg.dgrid, d_ggrid, sim->adj_lvt, sim->adj_lf, sim->stream);
+    if (d_gx) wd::launch_f4_to_aos3(n, sim->adj_lvt, d_gx, sim->stream);
+    if (d_gv) wd::launch_f4_to_aos3(n, sim->adj_lf, d_gv, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    return sync_stream(sim);
 }
 
 // ---- batched scenes: per-scene diagnostics and ensemble metrics -----------------

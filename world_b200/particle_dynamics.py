@@ -189,6 +189,39 @@ class ParticleDynamics:
         torch.cuda.current_stream().synchronize()
         check(lib.wd_set_state_device(self._h, ptr(t.contiguous())))
 
+    # -- reverse pass (CUDA tensors, AoS3 by grain id) ---------------------------------
+    def set_contact_params(self, mu: float, restitution: float, k_n: float) -> None:
+        check(lib.wd_set_contact_params(self._h, ctypes.c_float(mu), ctypes.c_float(restitution),
+                                        ctypes.c_float(k_n)))
+
+    def adjoint_record(self, steps: int, checkpoint_every: int = 20) -> None:
+        check(lib.wd_adjoint_record(self._h, int(steps), int(checkpoint_every)))
+
+    def adjoint_backward(self, gx=None, gv=None):
+        """(dL/dx0, dL/dv0 as (n, 3) CUDA tensors, dL/d(mu, e, k_n) as a float64 array)
+        for dL/dx, dL/dv at the end of the recorded window."""
+        import torch
+        dev = torch.device("cuda")
+        gx_ = None if gx is None else gx.detach().to(dev, torch.float32).contiguous()
+        gv_ = None if gv is None else gv.detach().to(dev, torch.float32).contiguous()
+        gx0 = torch.empty((self.n, 3), dtype=torch.float32, device=dev)
+        gv0 = torch.empty((self.n, 3), dtype=torch.float32, device=dev)
+        theta = np.zeros(3, np.float64)
+        torch.cuda.current_stream().synchronize()
+        check(lib.wd_adjoint_backward(self._h, ptr(gx_), ptr(gv_), ptr(gx0), ptr(gv0), ptr(theta)))
+        return gx0, gv0, theta
+
+    def deposit_vjp(self, ggrid):
+        """(dL/dx, dL/dv) as (n, 3) CUDA tensors for dL/dgrid (4 * nodes) at the current state."""
+        import torch
+        dev = torch.device("cuda")
+        g = ggrid.detach().to(dev, torch.float32).contiguous()
+        gx = torch.empty((self.n, 3), dtype=torch.float32, device=dev)
+        gv = torch.empty((self.n, 3), dtype=torch.float32, device=dev)
+        torch.cuda.current_stream().synchronize()
+        check(lib.wd_deposit_vjp(self._h, ptr(g), ptr(gx), ptr(gv)))
+        return gx, gv
+
     # -- files and frames ------------------------------------------------------------
     def write_state_file(self, path: str) -> None:
         """The reference's state file (int32 n + 6n float32), for initialize_from_file."""
