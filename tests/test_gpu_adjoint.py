@@ -4,7 +4,7 @@ contact pattern of its base run frozen.
 
 The adjoint runs in FP32 on the FP32 trajectory; the differences run in FP64 on the FP64
 trajectory (which follows the oracle to 1e-6 m over these windows). Directional
-derivatives must agree to 1%; in practice they agree far closer.
+derivatives must agree to 0.1% (measured on a B200: 1e-7 to 5e-5 relative).
 """
 from __future__ import annotations
 
@@ -19,7 +19,7 @@ from world_b200.adjoint import deposit, window
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-2
+RTOL = 1e-3
 
 
 def _fd(f, h):
