@@ -253,6 +253,9 @@ int wd_compute_max_acceleration(wd_sim* sim, float* max_accel);
  * particles_per_cell grains in a cell (src/find_neighbors_kernel.cu:230-234). No
  * grain is dropped here: the sorted search has no per-cell capacity. */
 int wd_grid_overflow_count(wd_sim* sim, int64_t* count);
+/* Verlet lists (simulation.neighbor_skin > 0): builds so far, kernels one build
+ * launches, and the mean list length of the last build (0 without lists). */
+int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length);
 /* Lifetime count of contacts that found no free history slot (WD_HIST_CAP). */
 int wd_history_overflow_count(wd_sim* sim, int64_t* count);
 /* find_neighbors_wct / compute_rhs_wct / take_step_wct / density_grid_wct

@@ -87,6 +87,7 @@ struct SimConfig {
     // extensions
     bool history = false;
     float picard_tolerance = 0.0f;
+    float neighbor_skin = 0.0f;
 };
 
 namespace detail {
@@ -120,6 +121,7 @@ void visit(SimConfig& c, Io&& io) {
     io("simulation", "density_grid_size_y", c.density_grid_size_y);
     io("simulation", "density_grid_size_z", c.density_grid_size_z);
     io("simulation", "history", c.history);
+    io("simulation", "neighbor_skin", c.neighbor_skin);
     io("domain", "x_min", c.domain.x_min);
     io("domain", "x_max", c.domain.x_max);
     io("domain", "y_min", c.domain.y_min);

@@ -1,0 +1,122 @@
+"""Verlet lists (simulation.neighbor_skin > 0) against the searched step.
+
+With a skin the grid search runs only when some grain has moved 0.45 skin since the
+last list build; contacts are taken from the lists and accumulated in the searched
+step's canonical order. States, springs and energies must equal the searched run's
+(skin 0, itself bit-identical to the oracle) to the last bit, in graph and in direct
+launch mode, for single scenes and batches, including the list-overflow fallback."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle.oracle import OracleSim, params_from_config
+from test_gpu_parity import packed_poly
+from world_b200 import ParticleDynamics, SceneBatch, SimConfig
+from world_b200.scenes import column_collapse
+from world_b200.state_io import grain_properties, initial_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(cfg, state, radius, steps, skin, timing=False):
+    out = []
+    for sk in (0.0, skin):
+        c = cfg.copy()
+        c.neighbor_skin = sk
+        c.kernel_timing = timing
+        sim = ParticleDynamics(c, state=state, radius=radius)
+        sim.advance(steps)
+        out.append(sim)
+    return out
+
+
+def _same(a, b):
+    np.testing.assert_array_equal(a.get_state(), b.get_state())
+    ca, pa, xa = a.get_history()
+    cb, pb, xb = b.get_history()
+    np.testing.assert_array_equal(ca, cb)
+    live = (np.arange(pa.size) % 24) < np.repeat(ca, 24)
+    np.testing.assert_array_equal(pa[live], pb[live])
+    np.testing.assert_array_equal(xa.reshape(-1, 3)[live], xb.reshape(-1, 3)[live])
+    np.testing.assert_array_equal(a.get_rhs(), b.get_rhs())
+    assert a.compute_total_energy() == b.compute_total_energy()
+
+
+@pytest.mark.parametrize("timing", [False, True])
+def test_lists_equal_search_every_step_packed_springs(timing):
+    cfg, st, rad = packed_poly(n=3000, seed=21, mu=0.5)
+    ref, lst = _pair(cfg, st, rad, 200, 0.5e-3, timing)
+    _same(ref, lst)
+    builds, kernels, mean_len = lst.list_stats()
+    assert 1 <= builds < 200 and kernels > 0 and mean_len > 0.5
+    assert ref.list_stats()[0] == 0
+
+
+def test_lists_equal_search_every_step_reference_cube():
+    cfg = SimConfig()
+    cfg.init_jitter = 0.3
+    cfg.kernel_timing = False
+    st, _ = initial_state(cfg)
+    ref, lst = _pair(cfg, st, None, 300, 2e-3)
+    _same(ref, lst)
+
+
+def test_lists_equal_search_in_a_collapsing_column():
+    sc = column_collapse(8192, diameters="lognormal", mu=0.5, cic=32)
+    sc.cfg.kernel_timing = False
+    ref, lst = _pair(sc.cfg, sc.state, sc.radius, 400, 0.1 * 5e-3)
+    _same(ref, lst)
+    assert lst.list_stats()[0] < 400
+
+
+def test_tiny_skin_and_overflowing_lists_stay_exact():
+    cfg, st, rad = packed_poly(n=1500, seed=22, mu=0.3)
+    cfg.kernel_timing = False
+    # a skin far below a step's motion: a build every step
+    ref, lst = _pair(cfg, st, rad, 60, 1e-9)
+    _same(ref, lst)
+    # a skin of several diameters: lists overflow, the searched path takes over
+    ref, lst = _pair(cfg, st, rad, 60, 2e-2)
+    _same(ref, lst)
+
+
+def test_lists_match_the_oracle():
+    cfg, st, rad = packed_poly(n=1200, seed=23, mu=0.5)
+    cfg.neighbor_skin = 0.4e-3
+    cfg.kernel_timing = False
+    _, mass = grain_properties(cfg, np.full(st.shape[0], cfg.particle_material, np.int32), rad)
+    sim = ParticleDynamics(cfg, state=st, radius=rad)
+    ref = OracleSim(params_from_config(cfg), st, rad, mass)
+    sim.advance(80)
+    ref.step(80)
+    np.testing.assert_array_equal(sim.get_state(), ref.state)
+
+
+def test_set_state_mid_run_rebuilds():
+    cfg, st, rad = packed_poly(n=1000, seed=24, mu=0.4)
+    ref, lst = _pair(cfg, st, rad, 30, 0.5e-3)
+    mid = ref.get_state().reshape(-1, 6).copy()
+    mid[:, 2] += 1e-4                     # every grain lifted: old lists are stale
+    ref.set_state(mid)
+    lst.set_state(mid)
+    ref.advance(40)
+    lst.advance(40)
+    _same(ref, lst)
+
+
+def test_batch_with_lists_equals_searched_batch():
+    a = packed_poly(n=1200, seed=25, mu=0.5)
+    b = packed_poly(n=900, seed=26, mu=0.2)
+    sims = []
+    for skin in (0.0, 0.5e-3):
+        cfgs = []
+        for c in (a[0], b[0]):
+            cc = c.copy()
+            cc.neighbor_skin = skin
+            cc.kernel_timing = False
+            cfgs.append(cc)
+        sb = SceneBatch(cfgs, [a[1], b[1]], radii=[a[2], b[2]])
+        sb.advance(150)
+        sims.append(sb)
+    _same(*sims)

@@ -28,7 +28,8 @@ CUDA_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-fmad=false",
                      f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
 BIN = os.path.join(HERE, "bin")
 DRIVERS = ["dataset", "chaos"]
-SOURCES = ["wd_search.cu", "wd_contact.cu", "wd_fields.cu", "wd_ensemble.cu", "wd_adjoint.cu",
+SOURCES = ["wd_search.cu", "wd_contact.cu", "wd_lists.cu", "wd_fields.cu", "wd_ensemble.cu",
+           "wd_adjoint.cu",
            "wd_sim.cu",
            "wd_config.cpp", "wd_io.cpp"]
 

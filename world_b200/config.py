@@ -26,6 +26,7 @@ FIELDS: dict[str, tuple[str, str, type]] = {
     "density_grid_size_y": ("simulation", "density_grid_size_y", int),
     "density_grid_size_z": ("simulation", "density_grid_size_z", int),
     "history": ("simulation", "history", bool),
+    "neighbor_skin": ("simulation", "neighbor_skin", float),
     "domain.x_min": ("domain", "x_min", float),
     "domain.x_max": ("domain", "x_max", float),
     "domain.y_min": ("domain", "y_min", float),

@@ -86,6 +86,7 @@ const std::vector<Entry>& registry() {
         WD_E("simulation", "density_grid_size_y", Kind::I, dgrid[1]),
         WD_E("simulation", "density_grid_size_z", Kind::I, dgrid[2]),
         WD_E("simulation", "history", Kind::B, history),
+        WD_E("simulation", "neighbor_skin", Kind::F, neighbor_skin),
         WD_E("domain", "x_min", Kind::F, dom_lo[0]),
         WD_E("domain", "x_max", Kind::F, dom_hi[0]),
         WD_E("domain", "y_min", Kind::F, dom_lo[1]),

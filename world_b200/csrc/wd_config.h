@@ -4,6 +4,9 @@
 // (src/sim_config.h:28-205, src/sim_config.cpp:54-195). New keys live in the existing
 // sections and default to the reference's behaviour when absent:
 //   simulation.history            false  -> viscous tangential friction (reference)
+//   simulation.neighbor_skin      0      -> neighbor search every step (reference); > 0:
+//                                           Verlet lists with this skin (m), rebuilt when
+//                                           a grain has moved 0.45 skin since the build
 //   physics.normal_stiffness      0      -> k_n = max_force / particle_radius
 //   physics.tangential_stiffness  0      -> k_t = 2/7 k_n when history is on
 //   physics.density               0      -> masses from the material table
@@ -24,6 +27,7 @@ struct Config {
     int threads_per_block = 256;
     int dgrid[3] = {32, 32, 32};
     bool history = false;
+    float neighbor_skin = 0.f;
     // domain
     float dom_lo[3] = {-1.f, -1.f, -1.f};
     float dom_hi[3] = {1.f, 1.f, 1.f};

@@ -14,6 +14,7 @@ namespace wd {
 
 constexpr int kHistCap = 24;          // tangential-history slots per grain
 constexpr uint32_t kNoKey = 0xFFFFFFFFu;
+constexpr int kNbrCap = 48;            // Verlet-list entries per grain
 
 // Lifetime counters kept on the device.
 enum Counter : int {
@@ -22,6 +23,7 @@ enum Counter : int {
     kCntUnstable = 2,       // scratch for is_stable
     kCntMaxAccel = 3,       // scratch for compute_max_acceleration (float bits)
     kCntRadixSearches = 4,  // searches that took the full radix-sort path
+    kCntListBuilds = 5,     // Verlet-list builds
     kNumCounters = 8,
 };
 
@@ -46,6 +48,7 @@ struct DevParams {
     int dgrid[3];              // CIC nodes per axis
     int node_base;             // first CIC node of the scene in the batch's field
     int frozen;                // batch only: the step leaves this scene's grains as they are
+    float skin;                // Verlet-list skin (0: search every step)
 };
 
 // Scenes of a batch: per-scene parameters and the scene of each slot of the arrays a

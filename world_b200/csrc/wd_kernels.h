@@ -126,6 +126,32 @@ struct Segments {
 void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip,
                   cudaStream_t st);
 
+// Verlet lists (simulation.neighbor_skin > 0, semi-implicit Euler). list_ctrl words:
+// [0] max |x - x_build|^2 since the build (float bits), [1] a list overflowed,
+// [2] rebuild requested by the host, [3] this step's decision (1.0f: rebuild).
+enum ListCtrl { kLcDisp = 0, kLcOverflow = 1, kLcForce = 2, kLcDecision = 3, kLcWords = 4 };
+struct ListArgs {
+    const float4* pos; const float4* vel; const int* ids;  // state of the step
+    const int2* table;                                     // fresh only at a build
+    float4* pos_out; float4* vel_out; int* ids_out; float4* acc_out;
+    const float4* hist_in; const int* hcnt_in;
+    float4* hist_out; int* hcnt_out;
+    unsigned long long* counters;
+    const int* nbr; const int* nbr_cnt; const float4* xbuild;
+    uint32_t* list_ctrl;
+    const DevParams* scene_params; const int* scene; int* scene_out;
+};
+void launch_list_decide(uint32_t* list_ctrl, float thr_sq, unsigned long long* counters,
+                        bool use_cond, cudaGraphConditionalHandle cond, cudaStream_t st);
+void launch_list_build(const DevParams& P, SceneTab T, const float4* pos, const int2* table,
+                       int* nbr, int* nbr_cnt, float4* xbuild, uint32_t* list_ctrl, Skip skip,
+                       cudaStream_t st);
+void launch_list_copy(int n, const float4* pos, const float4* vel, const int* ids,
+                      const int* hcnt, const int* scene, float4* pos_out, float4* vel_out,
+                      int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st);
+void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st);
+void launch_list_length(int n, const int* nbr_cnt, unsigned long long* out, cudaStream_t st);
+
 // Total energy per scene at the sorted state (after a search): per-grain FP64 sums,
 // then fixed-order per-segment reductions into out[scene]. hcnt is in state-slot
 // order; src maps each sorted position to its state slot.

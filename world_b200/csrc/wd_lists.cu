@@ -1,0 +1,308 @@
+// wd_lists.cu -- Verlet neighbor lists for the semi-implicit Euler step.
+//
+// The reference searches the grid every step (src/particle_dynamics.cu:264-281). With
+// simulation.neighbor_skin = s > 0 the search runs only when needed: a build sorts the
+// grains as the search does, and lists, for every grain, the grains whose centres are
+// closer than r_i + r_j + s, in the contact kernel's canonical visiting order (stencil
+// cell, then grain id). Until some grain has moved 0.45 s from where the build saw it,
+// every contact of every step is in the lists (|d| >= r_i + r_j + s - 0.9 s), so the
+// step computes the same contact set as the searched step.
+//
+// The results are bit-identical to the searched step because forces are accumulated
+// in the same order: the kernel checks that the contacts it meets arrive in canonical
+// order for the current positions ((stencil offset of the partner's current cell,
+// partner id) non-decreasing); a grain for which a cell crossing broke that order
+// re-sorts its contacts before accumulating them.
+//
+// Between builds the state stays in one order and ping-pongs between two buffers; a
+// build gathers it into the new order, lists the neighbors, and copies it back.
+#include "wd_kernels.h"
+
+namespace wd {
+namespace {
+
+__device__ __forceinline__ bool skipped(const Skip& s) {
+    return s.prev_res != nullptr && s.tol > 0.f && __uint_as_float(*s.prev_res) < s.tol;
+}
+
+// One thread: decide whether this step builds, reset the build-relative state, and
+// switch the build's conditional node (graph mode).
+__global__ void k_list_decide(uint32_t* __restrict__ ctrl, float thr_sq,
+                              unsigned long long* __restrict__ counters, int use_cond,
+                              cudaGraphConditionalHandle cond) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const float disp = __uint_as_float(ctrl[kLcDisp]);
+    const bool build = ctrl[kLcForce] != 0u || ctrl[kLcOverflow] != 0u || !(disp < thr_sq);
+    ctrl[kLcDecision] = build ? __float_as_uint(1.f) : 0u;
+    if (build) {
+        ctrl[kLcDisp] = 0u;
+        ctrl[kLcOverflow] = 0u;
+        ctrl[kLcForce] = 0u;
+        counters[kCntListBuilds] += 1ull;
+    }
+    if (use_cond) cudaGraphSetConditional(cond, build ? 1u : 0u);
+}
+
+// The list of every grain, from the run table of the build's sorted state: the
+// contact kernel's stencil walk with the skin added to the contact distance.
+template <bool BATCH>
+__global__ void __launch_bounds__(kBlock)
+k_list_build(DevParams P0, SceneTab T, const float4* __restrict__ pos,
+             const int2* __restrict__ table, int* __restrict__ nbr, int* __restrict__ nbr_cnt,
+             float4* __restrict__ xbuild, uint32_t* __restrict__ ctrl, Skip skip) {
+    if (skipped(skip)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = P0.n;
+    if (s >= n) return;
+    const DevParams& P = scene_params<BATCH>(P0, T, s);
+    const float4 pi = pos[s];
+    int cx, cy, cz;
+    cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+    int cnt = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int nx = cx + dx;
+        if (nx < 0 || nx >= P.grid[0]) continue;
+        int lo[3], hi[3];
+        row_ranges(P, table, nx, cy, cz, lo, hi);
+        for (int t = 0; t < 3; ++t) {
+            for (int j = lo[t]; j < hi[t]; ++j) {
+                if (j == s) continue;
+                const float4 pj = __ldg(&pos[j]);
+                float3 d;
+                const float ns = pair_norm_sq(pi, pj, d);
+                const float reach = (pi.w + pj.w) + P.skin;
+                if (ns < reach * reach) {
+                    if (cnt < kNbrCap) nbr[static_cast<int64_t>(cnt) * n + s] = j;
+                    ++cnt;
+                }
+            }
+        }
+    }
+    nbr_cnt[s] = cnt;
+    xbuild[s] = pi;
+    if (cnt > kNbrCap) atomicOr(&ctrl[kLcOverflow], 1u);
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_list_copy(int n, const float4* __restrict__ pos, const float4* __restrict__ vel,
+            const int* __restrict__ ids, const int* __restrict__ hcnt,
+            const int* __restrict__ scene, float4* __restrict__ pos_out,
+            float4* __restrict__ vel_out, int* __restrict__ ids_out, int* __restrict__ hcnt_out,
+            int* __restrict__ scene_out, Skip skip) {
+    if (skipped(skip)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    pos_out[s] = pos[s];
+    vel_out[s] = vel[s];
+    ids_out[s] = ids[s];
+    if (hcnt) hcnt_out[s] = hcnt[s];
+    if (scene) scene_out[s] = scene[s];
+}
+
+// Position of a partner in the canonical visiting order: the stencil offset of its
+// current cell (dx, then dy, then dz, ascending), then its id.
+__device__ __forceinline__ unsigned long long visit_key(const DevParams& P, int cx, int cy,
+                                                        int cz, float4 pj, int jd) {
+    int jx, jy, jz;
+    cell_coords(P, pj.x, pj.y, pj.z, jx, jy, jz);
+    const int sidx = ((jx - cx + 1) * 3 + (jy - cy + 1)) * 3 + (jz - cz + 1);
+    return (static_cast<unsigned long long>(static_cast<unsigned>(sidx)) << 32) |
+           static_cast<unsigned>(jd);
+}
+
+template <bool HIST, bool BATCH>
+__global__ void __launch_bounds__(kBlock, 5)
+k_force_list(DevParams P0, ListArgs A) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = P0.n;
+    uint32_t disp_bits = 0u;
+    if (s < n) {
+        const int scene = BATCH ? A.scene[s] : 0;
+        const DevParams& P = BATCH ? A.scene_params[scene] : P0;
+        const float4 pi = A.pos[s];
+        const float4 vi = A.vel[s];
+        const int id = A.ids[s];
+        if (BATCH && P.frozen) {
+            A.pos_out[s] = pi;
+            A.vel_out[s] = vi;
+            A.ids_out[s] = id;
+            A.scene_out[s] = scene;
+            A.acc_out[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (HIST) A.hcnt_out[s] = 0;
+        } else {
+            const float3 pos = make_float3(pi.x, pi.y, pi.z);
+            const float3 vel = make_float3(vi.x, vi.y, vi.z);
+            const float ri = pi.w, mi = vi.w;
+            float3 f = make_float3(0.f, 0.f, 0.f);
+            HistRow h;
+            if (HIST) {
+                h.in = A.hist_in + static_cast<int64_t>(id) * kHistCap;
+                h.in_count = A.hcnt_in[s];
+                h.out = A.hist_out + static_cast<int64_t>(id) * kHistCap;
+                h.out_count = 0;
+            }
+            wall_forces<HIST>(P, pos, vel, ri, mi, f, h, A.counters);
+            const float3 f_walls = f;
+            const int out_walls = HIST ? h.out_count : 0;
+            const float cut = contact_cutoff_sq(ri, P.rmax);
+            int cx, cy, cz;
+            cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+            const int cnt = A.nbr_cnt[s];
+            bool ordered = true;
+            if (cnt <= kNbrCap) {
+                // the list, in its build order, while the contacts arrive in canonical order
+                unsigned long long last = 0ull;
+                for (int e = 0; e < cnt; ++e) {
+                    const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+                    const float4 pj = __ldg(&A.pos[j]);
+                    float3 d;
+                    const float ns = pair_norm_sq(pi, pj, d);
+                    if (ns > cut) continue;
+                    const float norm = sqrtf(ns);
+                    const float dist = pair_dist(norm, ri, pj.w);
+                    if (!(dist < 0.f)) continue;
+                    const int jd = __ldg(&A.ids[j]);
+                    const unsigned long long key = visit_key(P, cx, cy, cz, pj, jd);
+                    if (key < last) {
+                        ordered = false;
+                        break;
+                    }
+                    last = key;
+                    const float4 vj = __ldg(&A.vel[j]);
+                    pair_force<HIST>(P, d, norm, dist, vel, mi, vj, jd, f, h, A.counters);
+                }
+                if (!ordered) {
+                    // a cell crossing re-ordered this grain's contacts: sort, then redo
+                    f = f_walls;
+                    if (HIST) h.out_count = out_walls;
+                    unsigned long long keys[kNbrCap];
+                    int slots[kNbrCap];
+                    int m = 0;
+                    for (int e = 0; e < cnt; ++e) {
+                        const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+                        const float4 pj = __ldg(&A.pos[j]);
+                        float3 d;
+                        const float ns = pair_norm_sq(pi, pj, d);
+                        if (ns > cut) continue;
+                        const float dist = pair_dist(sqrtf(ns), ri, pj.w);
+                        if (!(dist < 0.f)) continue;
+                        const unsigned long long key = visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j]));
+                        int q = m++;  // m <= cnt <= kNbrCap
+                        while (q > 0 && keys[q - 1] > key) {
+                            keys[q] = keys[q - 1];
+                            slots[q] = slots[q - 1];
+                            --q;
+                        }
+                        keys[q] = key;
+                        slots[q] = j;
+                    }
+                    for (int q = 0; q < m; ++q) {
+                        const int j = slots[q];
+                        const float4 pj = __ldg(&A.pos[j]);
+                        float3 d;
+                        const float ns = pair_norm_sq(pi, pj, d);
+                        const float norm = sqrtf(ns);
+                        const float dist = pair_dist(norm, ri, pj.w);
+                        const float4 vj = __ldg(&A.vel[j]);
+                        pair_force<HIST>(P, d, norm, dist, vel, mi, vj,
+                                         static_cast<int>(keys[q] & 0xffffffffull), f, h, A.counters);
+                    }
+                }
+            } else {
+                // list overflow: this step built the lists, so the run table is fresh
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int nx = cx + dx;
+                    if (nx < 0 || nx >= P.grid[0]) continue;
+                    int lo[3], hi[3];
+                    row_ranges(P, A.table, nx, cy, cz, lo, hi);
+                    for (int t = 0; t < 3; ++t) {
+                        for (int j = lo[t]; j < hi[t]; ++j) {
+                            const float4 pj = __ldg(&A.pos[j]);
+                            float3 d;
+                            const float ns = pair_norm_sq(pi, pj, d);
+                            if (ns > cut || j == s) continue;
+                            const float norm = sqrtf(ns);
+                            const float dist = pair_dist(norm, ri, pj.w);
+                            if (!(dist < 0.f)) continue;
+                            const float4 vj = __ldg(&A.vel[j]);
+                            const int partner = HIST ? __ldg(&A.ids[j]) : 0;
+                            pair_force<HIST>(P, d, norm, dist, vel, mi, vj, partner, f, h,
+                                             A.counters);
+                        }
+                    }
+                }
+            }
+            if (HIST) A.hcnt_out[s] = h.out_count;
+            const float3 a = make_float3(f.x / mi, f.y / mi, f.z / mi);
+            const float3 v1 = make_float3(fmaf(P.dt, a.x, vel.x), fmaf(P.dt, a.y, vel.y),
+                                          fmaf(P.dt, a.z, vel.z));
+            const float3 x1 = make_float3(fmaf(P.dt, v1.x, pos.x), fmaf(P.dt, v1.y, pos.y),
+                                          fmaf(P.dt, v1.z, pos.z));
+            A.pos_out[s] = make_float4(x1.x, x1.y, x1.z, ri);
+            A.vel_out[s] = make_float4(v1.x, v1.y, v1.z, mi);
+            A.ids_out[s] = id;
+            if (BATCH) A.scene_out[s] = scene;
+            A.acc_out[s] = make_float4(a.x, a.y, a.z, 0.f);
+            const float4 xb = A.xbuild[s];
+            const float ex = x1.x - xb.x, ey = x1.y - xb.y, ez = x1.z - xb.z;
+            const float d2 = ex * ex + ey * ey + ez * ez;
+            // NaN compares above every float: a diverging grain forces a build
+            disp_bits = d2 >= 0.f ? __float_as_uint(d2) : 0x7f800000u;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) disp_bits = max(disp_bits, __shfl_xor_sync(0xffffffffu, disp_bits, o));
+    if ((threadIdx.x & 31) == 0 && disp_bits != 0u) atomicMax(&A.list_ctrl[kLcDisp], disp_bits);
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_list_length(int n, const int* __restrict__ cnt, unsigned long long* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long v = s < n ? static_cast<unsigned long long>(min(cnt[s], kNbrCap + 1)) : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(out, v);
+}
+
+}  // namespace
+
+void launch_list_decide(uint32_t* list_ctrl, float thr_sq, unsigned long long* counters,
+                        bool use_cond, cudaGraphConditionalHandle cond, cudaStream_t st) {
+    k_list_decide<<<1, 32, 0, st>>>(list_ctrl, thr_sq, counters, use_cond ? 1 : 0, cond);
+}
+
+void launch_list_build(const DevParams& P, SceneTab T, const float4* pos, const int2* table,
+                       int* nbr, int* nbr_cnt, float4* xbuild, uint32_t* list_ctrl, Skip skip,
+                       cudaStream_t st) {
+    if (T.params)
+        k_list_build<true><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, table, nbr, nbr_cnt,
+                                                                xbuild, list_ctrl, skip);
+    else
+        k_list_build<false><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, table, nbr, nbr_cnt,
+                                                                 xbuild, list_ctrl, skip);
+}
+
+void launch_list_copy(int n, const float4* pos, const float4* vel, const int* ids,
+                      const int* hcnt, const int* scene, float4* pos_out, float4* vel_out,
+                      int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st) {
+    k_list_copy<<<blocks_for(n), kBlock, 0, st>>>(n, pos, vel, ids, hcnt, scene, pos_out,
+                                                  vel_out, ids_out, hcnt_out, scene_out, skip);
+}
+
+void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st) {
+    const int nb = blocks_for(P.n);
+    const bool batch = a.scene_params != nullptr;
+    if (P.history) {
+        if (batch) k_force_list<true, true><<<nb, kBlock, 0, st>>>(P, a);
+        else k_force_list<true, false><<<nb, kBlock, 0, st>>>(P, a);
+    } else {
+        if (batch) k_force_list<false, true><<<nb, kBlock, 0, st>>>(P, a);
+        else k_force_list<false, false><<<nb, kBlock, 0, st>>>(P, a);
+    }
+}
+
+void launch_list_length(int n, const int* nbr_cnt, unsigned long long* out, cudaStream_t st) {
+    k_list_length<<<blocks_for(n), kBlock, 0, st>>>(n, nbr_cnt, out);
+}
+
+}  // namespace wd

@@ -123,6 +123,16 @@ struct wd_sim {
     double* grain_sums = nullptr;         // 1 per scene
     float* chaos_grid = nullptr;          // 4 * nodes floats
 
+    // Verlet lists (simulation.neighbor_skin > 0, semi-implicit Euler): the state
+    // ping-pongs between the A and B buffers; lpar counts the swaps mod 2.
+    bool lists = false;
+    int lpar = 0;
+    int* nbr = nullptr;
+    int* nbr_cnt = nullptr;
+    float4* xbuild = nullptr;
+    uint32_t* list_ctrl = nullptr;
+    unsigned long long* list_len = nullptr;
+
     // reverse pass: snapshots of the step state (checkpoints of a recorded window and
     // the states of the segment being replayed) and the adjoint buffers
     struct Snap {
@@ -183,6 +193,8 @@ void destroy_graphs(wd_sim* s) {
     }
     s->graph_dirty = true;
 }
+
+cudaError_t request_list_build(wd_sim* s);
 
 // ---- snapshots of the step state, for the reverse pass ---------------------------
 
@@ -246,6 +258,7 @@ cudaError_t put_snap(wd_sim* s, const wd_sim::Snap& q) {
                                 cudaMemcpyDeviceToDevice, st);
     }
     s->time = q.time;
+    if (e == cudaSuccess) e = request_list_build(s);
     return e;
 }
 
@@ -266,7 +279,7 @@ void free_sim(wd_sim* s) {
                     s->sceneC, s->d_seg, s->d_chunk_base, s->grain_vals, s->scene_sums,
                     s->scene_overflow, s->scene_unstable, s->d_node_seg, s->d_node_chunk,
                     s->node_vals, s->chaos_partials, s->chaos_sums, s->grain_sums,
-                    s->chaos_grid};
+                    s->chaos_grid, s->nbr, s->nbr_cnt, s->xbuild, s->list_ctrl, s->list_len};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
@@ -310,6 +323,7 @@ DevParams make_params(const wd::Config& c, int n, float dt) {
     P.cell_base = 0;
     P.node_base = 0;
     P.frozen = 0;
+    P.skin = c.neighbor_skin;
     return P;
 }
 
@@ -320,6 +334,22 @@ wd::SceneTab tab(const wd_sim* s, const int* scene) {
 
 wd::Segments segments(const wd_sim* s) {
     return wd::Segments{s->d_seg, s->d_chunk_base, s->scenes, s->total_chunks};
+}
+
+// List mode: the buffers holding the state after a step become the A buffers.
+void swap_state(wd_sim* s) {
+    std::swap(s->posA, s->posB);
+    std::swap(s->velA, s->velB);
+    std::swap(s->idsA, s->idsB);
+    if (s->P.history) std::swap(s->hcnt_slot, s->hcnt_g);
+    if (s->scenes > 1) std::swap(s->sceneA, s->sceneB);
+    s->lpar ^= 1;
+}
+
+// The state changed outside a step: the next step rebuilds the lists.
+cudaError_t request_list_build(wd_sim* s) {
+    if (!s->lists) return cudaSuccess;
+    return cudaMemsetAsync(s->list_ctrl + wd::kLcForce, 1, 1, s->stream);
 }
 
 // One neighbor search. Inside graph capture the radix path goes into an IF
@@ -425,14 +455,103 @@ cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
     return cudaGetLastError();
 }
 
+// List build: search and gather the state (A) into the new order (B), list the
+// neighbors of the sorted state, copy it back to A. `gate` skips it all when the
+// step's decision says no build (direct launches); in a graph it is the body of an
+// IF node and runs ungated.
+void enqueue_list_build(wd_sim* s, wd::Skip gate, cudaStream_t st) {
+    const DevParams& P = s->P;
+    const bool hist = P.history != 0, batch = s->scenes > 1;
+    wd::launch_search(P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, gate, nullptr, 0,
+                      s->counters, st);
+    wd::launch_gather(P, s->sb, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr, nullptr,
+                      nullptr, nullptr, false, hist ? s->hcnt_slot : nullptr,
+                      hist ? s->hcnt_g : nullptr, batch ? s->sceneA : nullptr,
+                      batch ? s->sceneB : nullptr, true, s->counters, s->scene_overflow,
+                      s->d_scene_P, gate, st);
+    wd::launch_list_build(P, tab(s, s->sceneB), s->posB, s->sb.table, s->nbr, s->nbr_cnt,
+                          s->xbuild, s->list_ctrl, gate, st);
+    wd::launch_list_copy(s->n, s->posB, s->velB, s->idsB, hist ? s->hcnt_g : nullptr,
+                         batch ? s->sceneB : nullptr, s->posA, s->velA, s->idsA,
+                         hist ? s->hcnt_slot : nullptr, batch ? s->sceneA : nullptr, gate, st);
+}
+
+// One list-mode step: decide, build if needed, contacts + integration from A into B.
+cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool capture,
+                              cudaEvent_t mid = nullptr) {
+    const DevParams& P = s->P;
+    const bool hist = P.history != 0, batch = s->scenes > 1;
+    const float reach = 0.45f * P.skin;
+    const float thr = reach * reach;
+    if (!capture) {
+        wd::launch_list_decide(s->list_ctrl, thr, s->counters, false, 0, st);
+        enqueue_list_build(s, wd::Skip{s->list_ctrl + wd::kLcDecision, 0.5f}, st);
+    } else {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t graph = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+        if (e != cudaSuccess) return e;
+        cudaGraphConditionalHandle cond;
+        e = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) return e;
+        wd::launch_list_decide(s->list_ctrl, thr, s->counters, true, cond, st);
+        e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+        if (e != cudaSuccess) return e;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
+        if (e != cudaSuccess) return e;
+        e = cudaStreamBeginCaptureToGraph(s->aux_stream, cp.conditional.phGraph_out[0], nullptr,
+                                          nullptr, 0, cudaStreamCaptureModeRelaxed);
+        if (e != cudaSuccess) return e;
+        enqueue_list_build(s, wd::Skip{nullptr, 0.f}, s->aux_stream);
+        cudaGraph_t captured = nullptr;
+        e = cudaStreamEndCapture(s->aux_stream, &captured);
+        if (e != cudaSuccess) return e;
+        e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+        if (e != cudaSuccess) return e;
+    }
+    if (mid) cudaEventRecord(mid, st);
+    wd::ListArgs a{};
+    a.pos = s->posA; a.vel = s->velA; a.ids = s->idsA; a.table = s->sb.table;
+    a.pos_out = s->posB; a.vel_out = s->velB; a.ids_out = s->idsB; a.acc_out = s->acc;
+    a.hist_in = hist ? s->hist[parity] : nullptr;
+    a.hcnt_in = hist ? s->hcnt_slot : nullptr;
+    a.hist_out = hist ? s->hist[parity ^ 1] : nullptr;
+    a.hcnt_out = hist ? s->hcnt_g : nullptr;
+    a.counters = s->counters;
+    a.nbr = s->nbr; a.nbr_cnt = s->nbr_cnt; a.xbuild = s->xbuild; a.list_ctrl = s->list_ctrl;
+    a.scene_params = batch ? s->d_scene_P : nullptr;
+    a.scene = s->sceneA;
+    a.scene_out = s->sceneB;
+    wd::launch_force_list(P, a, st);
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_any_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
+                             cudaEvent_t mid = nullptr) {
+    return s->lists ? enqueue_step_list(s, parity, st, capture, mid)
+                    : enqueue_step(s, parity, st, capture, mid);
+}
+
 int build_graphs(wd_sim* s) {
     destroy_graphs(s);
-    const int count = s->P.history ? 2 : 1;
+    const int count = (s->P.history || s->lists) ? 2 : 1;
     for (int parity = 0; parity < count; ++parity) {
         cudaGraph_t g = nullptr;
+        // list mode: capture the graph of parity q with the buffers it will see
+        const bool swapped = s->lists && s->lpar != parity;
+        if (swapped) swap_state(s);
         WD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        const cudaError_t ce = enqueue_step(s, parity, s->stream, true);
+        const cudaError_t ce = enqueue_any_step(s, parity, s->stream, true);
         const cudaError_t ee = cudaStreamEndCapture(s->stream, &g);
+        if (swapped) swap_state(s);
         if (ce != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             WD_CUDA(ce);
@@ -487,7 +606,7 @@ int timed_step(wd_sim* s, int parity) {
     cudaEvent_t e0 = take_event(s), e1 = take_event(s), e2 = take_event(s);
     WD_CUDA(cudaEventRecord(e0, st));
     if (s->picard) WD_CUDA(cudaEventRecord(e1, st));
-    WD_CUDA(enqueue_step(s, parity, st, false, s->picard ? nullptr : e1));
+    WD_CUDA(enqueue_any_step(s, parity, st, false, s->picard ? nullptr : e1));
     WD_CUDA(cudaEventRecord(e2, st));
     WD_CUDA(cudaGetLastError());
     s->ev_pending.push_back(e0);
@@ -609,6 +728,15 @@ int alloc_sim(wd_sim* s) {
         WD_CUDA(cudaMemset(s->scene_overflow, 0, sizeof(unsigned long long) * S));
         WD_CUDA(dalloc(&s->scene_unstable, S));
     }
+    if (s->lists) {
+        WD_CUDA(dalloc(&s->nbr, static_cast<size_t>(n) * wd::kNbrCap));
+        WD_CUDA(dalloc(&s->nbr_cnt, n));
+        WD_CUDA(dalloc(&s->xbuild, n));
+        WD_CUDA(dalloc(&s->list_ctrl, wd::kLcWords));
+        WD_CUDA(dalloc(&s->list_len, 1));
+        const uint32_t init[wd::kLcWords] = {0u, 0u, 1u, 0u};  // the first step builds
+        WD_CUDA(cudaMemcpy(s->list_ctrl, init, sizeof(init), cudaMemcpyHostToDevice));
+    }
     return WD_OK;
 }
 
@@ -700,9 +828,11 @@ int create_scenes(const wd::Config* const* cfgs, int S, const int64_t* counts,
         if (counts[k] <= 0) return fail(WD_ERR_INVALID, "wd_create: every scene needs grains");
         const bool picard = c0.time_integrator != "semi_implicit_euler";
         if (k > 0 && (c.time_integrator != c0.time_integrator || c.history != c0.history ||
-                      c.dt != c0.dt || (picard && c.picard_iterations != c0.picard_iterations)))
+                      c.dt != c0.dt || (picard && c.picard_iterations != c0.picard_iterations) ||
+                      c.neighbor_skin != c0.neighbor_skin))
             return fail(WD_ERR_INVALID, "wd_create: scenes of a batch must share the integrator, "
-                                        "Picard iterations, history mode and dt");
+                                        "Picard iterations, history mode, neighbor skin and dt");
+        if (c.neighbor_skin < 0.f) return fail(WD_ERR_INVALID, "wd_create: simulation.neighbor_skin must be >= 0");
         total += counts[k];
         cells += static_cast<uint64_t>(c.grid[0]) * c.grid[1] * c.grid[2];
         nodes += static_cast<int64_t>(c.dgrid[0]) * c.dgrid[1] * c.dgrid[2];
@@ -722,6 +852,7 @@ int create_scenes(const wd::Config* const* cfgs, int S, const int64_t* counts,
     s->dt = c0.dt;
     s->picard = c0.time_integrator != "semi_implicit_euler";
     s->picard_iters = s->picard ? c0.picard_iterations : 1;
+    s->lists = c0.neighbor_skin > 0.f && !s->picard;
     s->num_cells = cells;
     s->scene_off.assign(1, 0);
     s->scene_nodes_off.assign(1, 0);
@@ -934,7 +1065,7 @@ int wd_destroy(wd_sim* sim) {
 int wd_step(wd_sim* sim, int64_t nsteps) {
     if (!sim || nsteps < 0) return fail(WD_ERR_INVALID, "wd_step: bad argument");
     for (int64_t k = 0; k < nsteps; ++k) {
-        const int parity = sim->P.history ? sim->hist_cur : 0;
+        const int parity = sim->lists ? sim->lpar : (sim->P.history ? sim->hist_cur : 0);
         if (sim->cfg.kernel_timing) {
             const int rc = timed_step(sim, parity);
             if (rc) return rc;
@@ -945,6 +1076,7 @@ int wd_step(wd_sim* sim, int64_t nsteps) {
             }
             WD_CUDA(cudaGraphLaunch(sim->graph[parity], sim->stream));
         }
+        if (sim->lists) swap_state(sim);
         if (sim->P.history) sim->hist_cur ^= 1;
         sim->time += sim->dt;
     }
@@ -1019,6 +1151,7 @@ int wd_set_state_device(wd_sim* sim, const float* d_state) {
     if (!sim || !d_state) return fail(WD_ERR_INVALID, "wd_set_state_device: NULL argument");
     wd::launch_state_from_aos(sim->n, d_state, sim->posA, sim->velA, sim->idsA, sim->stream);
     WD_CUDA(cudaGetLastError());
+    WD_CUDA(request_list_build(sim));
     return WD_OK;
 }
 
@@ -1323,7 +1456,8 @@ int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
     if (!sim || !kernels) return fail(WD_ERR_INVALID, "wd_kernels_per_step: NULL argument");
     // keys, mover kernel, merge, gather, contact per search; a search that takes the
     // radix path adds 1 + 3 per pass (wd_radix_search_count)
-    *kernels = static_cast<int64_t>(5) * sim->picard_iters;
+    // list mode: the decision and the contact kernel; builds add wd_list_stats' count
+    *kernels = sim->lists ? 2 : static_cast<int64_t>(5) * sim->picard_iters;
     return WD_OK;
 }
 
@@ -1387,6 +1521,31 @@ int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* c
     cudaFree(d_cand);
     cudaFree(d_contact);
     WD_CUDA(e);
+    return WD_OK;
+}
+
+int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_list_stats: NULL handle");
+    if (kernels_each)
+        *kernels_each = sim->lists ? 2 + (1 + 3 * sim->sb.passes) + 1 + 3 : 0;
+    if (builds) {
+        int rc = read_counter(sim, wd::kCntListBuilds, builds);
+        if (rc) return rc;
+    }
+    if (mean_length) {
+        *mean_length = 0.0;
+        if (sim->lists) {
+            WD_CUDA(cudaMemsetAsync(sim->list_len, 0, sizeof(unsigned long long), sim->stream));
+            wd::launch_list_length(sim->n, sim->nbr_cnt, sim->list_len, sim->stream);
+            WD_CUDA(cudaGetLastError());
+            unsigned long long total = 0;
+            WD_CUDA(cudaMemcpyAsync(&total, sim->list_len, sizeof(total), cudaMemcpyDeviceToHost,
+                                    sim->stream));
+            int rc = sync_stream(sim);
+            if (rc) return rc;
+            *mean_length = static_cast<double>(total) / static_cast<double>(sim->n);
+        }
+    }
     return WD_OK;
 }
 

@@ -328,6 +328,14 @@ class ParticleDynamics:
         check(lib.wd_radix_search_count(self._h, ctypes.byref(c), ctypes.byref(k)))
         return int(c.value), int(k.value)
 
+    def list_stats(self) -> tuple[int, int, float]:
+        """(Verlet-list builds so far, kernels each build launches, mean list length)."""
+        b = ctypes.c_int64()
+        k = ctypes.c_int32()
+        m = ctypes.c_double()
+        check(lib.wd_list_stats(self._h, ctypes.byref(b), ctypes.byref(k), ctypes.byref(m)))
+        return int(b.value), int(k.value), float(m.value)
+
     def kernels_per_step(self) -> int:
         v = ctypes.c_int64()
         check(lib.wd_kernels_per_step(self._h, ctypes.byref(v)))
