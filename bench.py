@@ -15,6 +15,10 @@ value  -- device time of K steps (CUDA events on the library's stream around eac
 e2e    -- the same metric through the C ABI with host buffers: each step
           wd_set_state() from pinned host memory, wd_step(1), wd_get_positions() to
           pinned host memory, all inside the timed region.
+neighbor search -- Verlet lists with a skin of 0.1 mean diameters by default
+          (--skin; 0 searches the grid every step as the reference does): the grid
+          search and sort run only when a grain has moved 0.45 skin since the last
+          build; the results are bit-identical either way.
 roofline -- the contact kernel (forces + integrator, the dominant kernel): its
           algorithmic bytes per launch over its average event-timed duration,
           against the measured HBM copy bandwidth.
@@ -66,6 +70,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--phase-steps", type=int, default=50)
+    ap.add_argument("--skin", type=float, default=-1.0,
+                    help="Verlet-list skin in m (simulation.neighbor_skin); negative: 0.1 x the "
+                         "mean grain diameter; 0: grid search every step, as the reference")
     ap.add_argument("--direct", action="store_true",
                     help="launch each step's kernels directly instead of as one CUDA graph "
                          "(for per-kernel profilers, which cannot see inside graphs with "
@@ -94,6 +101,7 @@ def workload_config(scene, args, grains=None, scenes=None) -> dict:
         "cic_grid": c.density_grid_size_x,
         "dt": c.dt,
         "l2": "flushed (512 MiB write) before every timed step, flush not timed",
+        "neighbor_skin_m": c.neighbor_skin,
     }
     if scenes is not None:
         out["scenes"] = scenes
@@ -268,17 +276,25 @@ def run_ours(args) -> int:
         if world > 1:
             dist.barrier()
 
+    def with_skin(sc):
+        skin = args.skin if args.skin >= 0 else 0.1 * 2.0 * float(np.mean(sc.radius))
+        sc.cfg.neighbor_skin = skin
+        return sc
+
     scenes_total = None
     if args.workload in BATCHED_WORKLOADS:
         # scenes shared out over the ranks, balanced by grain count; each rank steps
         # its share as one batch
         members = ensemble_for(args.workload)
         mine = shard_scenes([m.n for m in members], world)[rank]
+        skin = with_skin(members[mine[0]]).cfg.neighbor_skin
+        for i in mine:
+            members[i].cfg.neighbor_skin = skin
         sim = SceneBatch.from_scenes([members[i] for i in mine])
         scene = members[mine[0]]
         scenes_total = len(members)
     else:
-        scene = scene_for(args.workload, n=args.grains, seed=12345 + rank)
+        scene = with_skin(scene_for(args.workload, n=args.grains, seed=12345 + rank))
         sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
     sim.set_kernel_timing(args.direct)
     n = sim.n
@@ -296,6 +312,7 @@ def run_ours(args) -> int:
           for _ in range(args.steps)]
     torch.cuda.synchronize()
     radix0, radix_each = sim.radix_search_count()
+    builds0, build_kernels, _ = sim.list_stats()
     barrier()
     # Each step: an L2 flush (512 MiB write) queued on the library's stream, then the
     # step bracketed by events on that stream. Nothing syncs the host inside the loop,
@@ -310,7 +327,13 @@ def run_ours(args) -> int:
     barrier()
     clocks = sampler.stop() if sampler else None
     radix_searches = sim.radix_search_count()[0] - radix0
-    launches = sim.kernels_per_step() * args.steps + radix_searches * radix_each
+    builds, _, mean_list = sim.list_stats()
+    builds -= builds0
+    lists = scene.cfg.neighbor_skin > 0
+    # list mode: a build launches the whole search (its radix kernels gated) and the
+    # list kernels; otherwise a search adds the radix kernels only when it takes them
+    launches = sim.kernels_per_step() * args.steps + (
+        builds * build_kernels if lists else radix_searches * radix_each)
     local_ms = sum(a.elapsed_time(b) for a, b in ev)
     total_ms = max_over_ranks(local_ms)
     all_grains = n
@@ -339,6 +362,9 @@ def run_ours(args) -> int:
     # (16 B per entry each way) plus the per-grain counts (4 B each way)
     hist_bytes = (2 * 16 * entries + 8 * n) if scene.cfg.history else 0
     contact_bytes = 88 * n + hist_bytes
+    if lists:
+        # plus the list count and the build position (20 B) and the list (4 B / entry)
+        contact_bytes += int(20 * n + 4 * mean_list * n)
     achieved = contact_bytes / (contact_ms / 1e3) / 1e9
     peak, peak_kind = measured_hbm_peak()
 
@@ -399,6 +425,8 @@ def run_ours(args) -> int:
             "clocks": clocks,
             "gpu_launches": launches,
             "radix_searches_timed": radix_searches,
+            "neighbor_lists": {"skin_m": scene.cfg.neighbor_skin, "builds_timed": builds,
+                               "mean_list_length": mean_list} if lists else None,
             "history_entries_per_grain": entries / n,
             "scene_results": scene_results,
         }
