@@ -11,6 +11,8 @@ deposit as differentiable functions, with the library's hand-written reverse pas
 
 The reference has no derivatives; the contact set and the clamp / stick-slip / viscous
 branches of every step are those the forward took (world_b200/csrc/wd_adjoint.cu).
+A window starts from (x0, v0) and the handle's current tangential springs (its
+history rows); set them (set_history) before evaluating the same window again.
 """
 from __future__ import annotations
 

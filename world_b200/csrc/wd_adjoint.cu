@@ -32,6 +32,9 @@ struct AdjStep {
     const int* hcnt_in;
     const float4* hist_next;
     const int* hcnt_next;
+    // the step's pair contacts per sorted slot, in the forward's visiting order
+    const int* clist;
+    const int* ccnt;
     // adjoints of step t's outputs, by grain id
     const float4* lx;
     const float4* lvt;     // lv' + dt lx'
@@ -200,57 +203,83 @@ k_adj_step(DevParams P, AdjStep A) {
         }
     }
 
-    // pairs, in the forward's canonical order
-    const float cut = contact_cutoff_sq(ri, P.rmax);
-    int cx, cy, cz;
-    cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
-    for (int dx = -1; dx <= 1; ++dx) {
-        const int nx = cx + dx;
-        if (nx < 0 || nx >= P.grid[0]) continue;
-        int lo[3], hi[3];
-        row_ranges(P, A.table, nx, cy, cz, lo, hi);
-        for (int t = 0; t < 3; ++t) {
-            for (int j = lo[t]; j < hi[t]; ++j) {
-                const float4 pj = A.pos[j];
-                float3 d;
-                const float ns = pair_norm_sq(pi, pj, d);
-                if (ns > cut || j == s) continue;
-                const float norm = sqrtf(ns);
-                const float dist = pair_dist(norm, ri, pj.w);
-                if (!(dist < 0.f)) continue;
-                const float4 vj = A.vel[j];
-                const int jd = A.ids[j];
-                const float3 lf_j = f3(A.lf[jd]);
-                float3 xi = zero, lxi_ij = zero, lxi_ji = zero;
-                int k_in = -1;
-                if (HIST) {
-                    k_in = row_find(in_row, in_count, jd);
-                    if (k_in >= 0) xi = f3(in_row[k_in]);
-                    if (out_count < kHistCap)
-                        lxi_ij = f3(A.lxi[static_cast<int64_t>(id) * kHistCap + out_count]);
-                    ++out_count;
-                    const float4* jrow = A.hist_next + static_cast<int64_t>(jd) * kHistCap;
-                    const int kj = row_find(jrow, A.hcnt_next[jd], id);
-                    if (kj >= 0) lxi_ji = f3(A.lxi[static_cast<int64_t>(jd) * kHistCap + kj]);
-                }
-                const float3 w_rel_f = make_float3(lf_i.x - lf_j.x, lf_i.y - lf_j.y, lf_i.z - lf_j.z);
-                const float3 w_rel_x = make_float3(lxi_ij.x - lxi_ji.x, lxi_ij.y - lxi_ji.y,
-                                                   lxi_ij.z - lxi_ji.z);
-                const float3 vr = make_float3(vel.x - vj.x, vel.y - vj.y, vel.z - vj.z);
-                float axi[3] = {0.f, 0.f, 0.f};
-                pair_blocks<HIST>(P, A, d, vr, xi, ri, pj.w, mi, vj.w, w_rel_f, w_rel_x, lf_i,
-                                  lxi_ij, ax, av, axi, th);
-                if (HIST && k_in >= 0)
-                    A.lxi_out[static_cast<int64_t>(id) * kHistCap + k_in] =
-                        make_float4(axi[0], axi[1], axi[2], 0.f);
-            }
+    // pairs, in the forward's visiting order (recorded by the replay)
+    const int nc = A.ccnt[s];
+    for (int e = 0; e < nc; ++e) {
+        const int j = A.clist[static_cast<int64_t>(e) * P.n + s];
+        const float4 pj = A.pos[j];
+        float3 d;
+        pair_norm_sq(pi, pj, d);
+        const float4 vj = A.vel[j];
+        const int jd = A.ids[j];
+        const float3 lf_j = f3(A.lf[jd]);
+        float3 xi = zero, lxi_ij = zero, lxi_ji = zero;
+        int k_in = -1;
+        if (HIST) {
+            k_in = row_find(in_row, in_count, jd);
+            if (k_in >= 0) xi = f3(in_row[k_in]);
+            if (out_count < kHistCap)
+                lxi_ij = f3(A.lxi[static_cast<int64_t>(id) * kHistCap + out_count]);
+            ++out_count;
+            const float4* jrow = A.hist_next + static_cast<int64_t>(jd) * kHistCap;
+            const int kj = row_find(jrow, A.hcnt_next[jd], id);
+            if (kj >= 0) lxi_ji = f3(A.lxi[static_cast<int64_t>(jd) * kHistCap + kj]);
         }
+        const float3 w_rel_f = make_float3(lf_i.x - lf_j.x, lf_i.y - lf_j.y, lf_i.z - lf_j.z);
+        const float3 w_rel_x = make_float3(lxi_ij.x - lxi_ji.x, lxi_ij.y - lxi_ji.y,
+                                           lxi_ij.z - lxi_ji.z);
+        const float3 vr = make_float3(vel.x - vj.x, vel.y - vj.y, vel.z - vj.z);
+        float axi[3] = {0.f, 0.f, 0.f};
+        pair_blocks<HIST>(P, A, d, vr, xi, ri, pj.w, mi, vj.w, w_rel_f, w_rel_x, lf_i,
+                          lxi_ij, ax, av, axi, th);
+        if (HIST && k_in >= 0)
+            A.lxi_out[static_cast<int64_t>(id) * kHistCap + k_in] =
+                make_float4(axi[0], axi[1], axi[2], 0.f);
     }
     const float4 lx = A.lx[id], lvt = A.lvt[id];
     A.lx_out[id] = make_float4(lx.x + ax[0], lx.y + ax[1], lx.z + ax[2], 0.f);
     A.lv_out[id] = make_float4(lvt.x + av[0], lvt.y + av[1], lvt.z + av[2], 0.f);
 #pragma unroll
     for (int c = 0; c < 3; ++c) A.theta[static_cast<int64_t>(c) * P.n + id] += th[c];
+}
+
+// The pair contacts of every sorted slot in the contact kernel's visiting order
+// (run-table stencil walk, the same tests), for the reverse pass.
+__global__ void __launch_bounds__(kBlock)
+k_contact_record(DevParams P, const float4* __restrict__ pos, const int2* __restrict__ table,
+                 int* __restrict__ clist, int* __restrict__ ccnt,
+                 unsigned long long* __restrict__ overflow) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P.n) return;
+    const float4 pi = pos[s];
+    const float ri = pi.w;
+    const float cut = contact_cutoff_sq(ri, P.rmax);
+    int cx, cy, cz;
+    cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+    int cnt = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int nx = cx + dx;
+        if (nx < 0 || nx >= P.grid[0]) continue;
+        int lo[3], hi[3];
+        row_ranges(P, table, nx, cy, cz, lo, hi);
+        for (int t = 0; t < 3; ++t) {
+            for (int j = lo[t]; j < hi[t]; ++j) {
+                const float4 pj = __ldg(&pos[j]);
+                float3 d;
+                const float ns = pair_norm_sq(pi, pj, d);
+                if (ns > cut || j == s) continue;
+                const float dist = pair_dist(sqrtf(ns), ri, pj.w);
+                if (!(dist < 0.f)) continue;
+                if (cnt < kAdjContacts) clist[static_cast<int64_t>(cnt) * P.n + s] = j;
+                ++cnt;
+            }
+        }
+    }
+    if (cnt > kAdjContacts) {
+        atomicAdd(overflow, 1ull);
+        cnt = kAdjContacts;
+    }
+    ccnt[s] = cnt;
 }
 
 // Counts of a spring snapshot by grain id (snapshots keep them by sorted slot).
@@ -328,11 +357,16 @@ void launch_adj_prep(int n, float dt, const float4* vel, const int* ids, const f
     k_adj_prep<<<blocks_for(n), kBlock, 0, st>>>(n, dt, vel, ids, lx, lv, lvt, lf);
 }
 
+void launch_contact_record(const DevParams& P, const float4* pos, const int2* table, int* clist,
+                           int* ccnt, unsigned long long* overflow, cudaStream_t st) {
+    k_contact_record<<<blocks_for(P.n), kBlock, 0, st>>>(P, pos, table, clist, ccnt, overflow);
+}
+
 void launch_adj_step(const DevParams& P, const AdjArgs& a, cudaStream_t st) {
     AdjStep A;
     A.pos = a.pos; A.vel = a.vel; A.ids = a.ids; A.table = a.table;
     A.hist_in = a.hist_in; A.hcnt_in = a.hcnt_in; A.hist_next = a.hist_next;
-    A.hcnt_next = a.hcnt_next; A.lx = a.lx; A.lvt = a.lvt; A.lf = a.lf; A.lxi = a.lxi;
+    A.hcnt_next = a.hcnt_next; A.clist = a.clist; A.ccnt = a.ccnt; A.lx = a.lx; A.lvt = a.lvt; A.lf = a.lf; A.lxi = a.lxi;
     A.lx_out = a.lx_out; A.lv_out = a.lv_out; A.lxi_out = a.lxi_out; A.theta = a.theta;
     A.kt_from_kn = a.kt_from_kn;
     if (P.history) k_adj_step<true><<<blocks_for(P.n), kBlock, 0, st>>>(P, A);

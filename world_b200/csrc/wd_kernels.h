@@ -208,11 +208,15 @@ struct AdjArgs {
     const int2* table;
     const float4* hist_in; const int* hcnt_in;     // springs at t (counts by sorted slot)
     const float4* hist_next; const int* hcnt_next; // springs at t+1 (counts by id)
+    const int* clist; const int* ccnt;             // pair contacts per slot (kAdjContacts)
     const float4* lx; const float4* lvt; const float4* lf; const float4* lxi;
     float4* lx_out; float4* lv_out; float4* lxi_out;
     double* theta;                                  // [3][n], accumulated
     int kt_from_kn;
 };
+constexpr int kAdjContacts = 32;  // pair contacts per grain the reverse pass records
+void launch_contact_record(const DevParams& P, const float4* pos, const int2* table, int* clist,
+                           int* ccnt, unsigned long long* overflow, cudaStream_t st);
 void launch_adj_prep(int n, float dt, const float4* vel, const int* ids, const float4* lx,
                      const float4* lv, float4* lvt, float4* lf, cudaStream_t st);
 void launch_adj_step(const DevParams& P, const AdjArgs& a, cudaStream_t st);

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -144,8 +145,23 @@ struct wd_sim {
         float4* hist = nullptr;
         float time = 0.f;
     };
-    std::vector<Snap> adj_ckpt, adj_seg;
+    std::vector<Snap> adj_ckpt;
     Snap adj_end;
+    // one replayed step: its sorted input state, in-counts, springs, contacts
+    struct TapeStep {
+        float4* pos = nullptr;
+        float4* vel = nullptr;
+        int* ids = nullptr;
+        int* hcnt = nullptr;
+        float4* hist = nullptr;
+        int* cnt_id = nullptr;
+        int* clist = nullptr;
+        int* ccnt = nullptr;
+    };
+    std::vector<TapeStep> adj_tape;
+    unsigned long long* adj_ovf = nullptr;
+    // captured replay / walk-back graphs per (segment length, parity); -1: replay
+    std::map<std::pair<int, int>, cudaGraphExec_t> adj_graphs;
     int64_t adj_steps = 0;
     int adj_every = 0;
     float4* adj_lx[2] = {nullptr, nullptr};
@@ -186,7 +202,13 @@ struct wd_sim {
 
 namespace {
 
+void clear_adj_graphs(wd_sim* s) {
+    for (auto& kv : s->adj_graphs) cudaGraphExecDestroy(kv.second);
+    s->adj_graphs.clear();
+}
+
 void destroy_graphs(wd_sim* s) {
+    clear_adj_graphs(s);
     for (auto& g : s->graph) {
         if (g) cudaGraphExecDestroy(g);
         g = nullptr;
@@ -205,13 +227,32 @@ void free_snap(wd_sim::Snap& q) {
 }
 
 void free_tape(wd_sim* s) {
+    clear_adj_graphs(s);
     for (auto& q : s->adj_ckpt) free_snap(q);
-    for (auto& q : s->adj_seg) free_snap(q);
     free_snap(s->adj_end);
+    for (auto& t : s->adj_tape) {
+        void* ptrs[] = {t.pos, t.vel, t.ids, t.hcnt, t.hist, t.cnt_id, t.clist, t.ccnt};
+        for (void* p : ptrs) cudaFree(p);
+    }
+    cudaFree(s->adj_ovf);
+    s->adj_ovf = nullptr;
     s->adj_ckpt.clear();
-    s->adj_seg.clear();
+    s->adj_tape.clear();
     s->adj_steps = 0;
     s->adj_every = 0;
+}
+
+cudaError_t alloc_tape_step(wd_sim* s, wd_sim::TapeStep& t) {
+    const size_t n = static_cast<size_t>(s->n);
+    cudaError_t e = dalloc(&t.pos, n);
+    if (e == cudaSuccess) e = dalloc(&t.vel, n);
+    if (e == cudaSuccess) e = dalloc(&t.ids, n);
+    if (e == cudaSuccess) e = dalloc(&t.clist, n * wd::kAdjContacts);
+    if (e == cudaSuccess) e = dalloc(&t.ccnt, n);
+    if (e == cudaSuccess && s->P.history) e = dalloc(&t.hcnt, n);
+    if (e == cudaSuccess && s->P.history) e = dalloc(&t.hist, n * wd::kHistCap);
+    if (e == cudaSuccess && s->P.history) e = dalloc(&t.cnt_id, n);
+    return e;
 }
 
 cudaError_t alloc_snap(wd_sim* s, wd_sim::Snap& q) {
@@ -1089,6 +1130,7 @@ int wd_set_dt(wd_sim* sim, float dt) {
         sim->dt = dt;
         sim->P.dt = dt;
         for (DevParams& Q : sim->scene_P) Q.dt = dt;
+        clear_adj_graphs(sim);
         if (sim->d_scene_P) {
             // ordered after the steps already queued, before the next one
             WD_CUDA(cudaMemcpyAsync(sim->d_scene_P, sim->scene_P.data(),
@@ -1551,11 +1593,110 @@ int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* m
 
 // ---- reverse pass -------------------------------------------------------------------
 
+// Replay of one segment from the state restored into A (the checkpoint): each step's
+// sorted input, contacts and springs go to the tape; the springs are read from and
+// written to the tape, not to the handle's own rows.
+cudaError_t adj_replay_body(wd_sim* s, int len, bool capture, cudaStream_t st) {
+    const DevParams& P = s->P;
+    const bool hist = P.history != 0;
+    const int n = s->n;
+    const wd::Skip none{nullptr, 0.f};
+    for (int k = 0; k < len; ++k) {
+        wd_sim::TapeStep& T = s->adj_tape[static_cast<size_t>(k)];
+        wd_sim::TapeStep& T1 = s->adj_tape[static_cast<size_t>(k) + 1];
+        cudaError_t e = enqueue_search(s, none, nullptr, 0, capture, st);
+        if (e != cudaSuccess) return e;
+        wd::launch_gather(P, s->sb, s->posA, s->velA, T.pos, T.vel, T.ids, nullptr, nullptr,
+                          nullptr, nullptr, false, hist ? s->hcnt_slot : nullptr,
+                          hist ? T.hcnt : nullptr, nullptr, nullptr, true, s->counters, nullptr,
+                          nullptr, none, st);
+        wd::launch_contact_record(P, T.pos, s->sb.table, T.clist, T.ccnt, s->adj_ovf, st);
+        if (hist) wd::launch_counts_by_id(n, T.ids, T.hcnt, T.cnt_id, st);
+        wd::ForceArgs fa{};
+        fa.pos = T.pos; fa.vel = T.vel; fa.ids = T.ids; fa.table = s->sb.table;
+        fa.pos_out = s->posA; fa.vel_out = s->velA; fa.ids_out = s->idsA;
+        fa.acc_out = s->acc;
+        fa.hist_in = hist ? T.hist : nullptr;
+        fa.hcnt_in = hist ? T.hcnt : nullptr;
+        fa.hist_out = hist ? T1.hist : nullptr;
+        fa.hcnt_out = hist ? s->hcnt_slot : nullptr;
+        fa.counters = s->counters;
+        wd::launch_force(P, fa, false, none, st);
+    }
+    if (hist)
+        wd::launch_counts_by_id(n, s->idsA, s->hcnt_slot,
+                                s->adj_tape[static_cast<size_t>(len)].cnt_id, st);
+    return cudaGetLastError();
+}
+
+// Walk one segment back, the adjoints starting in buffer `cur`.
+cudaError_t adj_back_body(wd_sim* s, int len, int cur, cudaStream_t st) {
+    const DevParams& P = s->P;
+    const bool hist = P.history != 0;
+    const int n = s->n;
+    const size_t rows = static_cast<size_t>(n) * wd::kHistCap;
+    for (int t = len - 1; t >= 0; --t) {
+        const wd_sim::TapeStep& T = s->adj_tape[static_cast<size_t>(t)];
+        const wd_sim::TapeStep& T1 = s->adj_tape[static_cast<size_t>(t) + 1];
+        if (hist) {
+            cudaError_t e = cudaMemsetAsync(s->adj_lxi[cur ^ 1], 0, rows * sizeof(float4), st);
+            if (e != cudaSuccess) return e;
+        }
+        wd::launch_adj_prep(n, P.dt, T.vel, T.ids, s->adj_lx[cur], s->adj_lv[cur], s->adj_lvt,
+                            s->adj_lf, st);
+        wd::AdjArgs a{};
+        a.pos = T.pos; a.vel = T.vel; a.ids = T.ids; a.table = nullptr;
+        a.hist_in = hist ? T.hist : nullptr;
+        a.hcnt_in = hist ? T.hcnt : nullptr;
+        a.hist_next = hist ? T1.hist : nullptr;
+        a.hcnt_next = hist ? T1.cnt_id : nullptr;
+        a.clist = T.clist; a.ccnt = T.ccnt;
+        a.lx = s->adj_lx[cur]; a.lvt = s->adj_lvt; a.lf = s->adj_lf;
+        a.lxi = hist ? s->adj_lxi[cur] : nullptr;
+        a.lx_out = s->adj_lx[cur ^ 1]; a.lv_out = s->adj_lv[cur ^ 1];
+        a.lxi_out = hist ? s->adj_lxi[cur ^ 1] : nullptr;
+        a.theta = s->adj_theta;
+        a.kt_from_kn = s->cfg.tangential_stiffness > 0.f ? 0 : 1;
+        wd::launch_adj_step(P, a, st);
+        cur ^= 1;
+    }
+    return cudaGetLastError();
+}
+
+// One replay (parity -1) or walk-back segment, from a graph captured once per
+// (length, parity) and kept until the step parameters or the tape change.
+cudaError_t run_adj_graph(wd_sim* s, int len, int parity) {
+    const auto key = std::make_pair(len, parity);
+    auto it = s->adj_graphs.find(key);
+    if (it == s->adj_graphs.end()) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        const cudaError_t ce = parity < 0 ? adj_replay_body(s, len, true, s->stream)
+                                          : adj_back_body(s, len, parity, s->stream);
+        e = cudaStreamEndCapture(s->stream, &g);
+        if (ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return ce;
+        }
+        if (e != cudaSuccess) return e;
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return e;
+        it = s->adj_graphs.emplace(key, exec).first;
+    }
+    return cudaGraphLaunch(it->second, s->stream);
+}
+
 int wd_set_contact_params(wd_sim* sim, float mu, float restitution, float k_n) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_set_contact_params: NULL handle");
     if (sim->scenes != 1) return fail(WD_ERR_INVALID, "wd_set_contact_params: not for a batch of scenes");
     if (!(k_n > 0.f) || !(mu >= 0.f) || !(restitution >= 0.f))
         return fail(WD_ERR_INVALID, "wd_set_contact_params: need mu >= 0, restitution >= 0, k_n > 0");
+    if (sim->cfg.friction == mu && sim->cfg.restitution == restitution &&
+        sim->cfg.normal_stiffness == k_n)
+        return WD_OK;  // unchanged: keep the captured graphs
     int rc = sync_stream(sim);
     if (rc) return rc;
     sim->cfg.friction = mu;
@@ -1567,6 +1708,7 @@ int wd_set_contact_params(wd_sim* sim, float mu, float restitution, float k_n) {
     sim->scene_P[0] = sim->P;
     sim->scene_cfg[0] = sim->cfg;
     sim->graph_dirty = true;
+    clear_adj_graphs(sim);
     return WD_OK;
 }
 
@@ -1577,11 +1719,14 @@ int wd_adjoint_record(wd_sim* sim, int64_t steps, int32_t checkpoint_every) {
     if (steps < 1 || checkpoint_every < 1) return fail(WD_ERR_INVALID, "wd_adjoint_record: steps and checkpoint_every must be >= 1");
     int rc = sync_stream(sim);
     if (rc) return rc;
-    free_tape(sim);
-    const int64_t nck = (steps + checkpoint_every - 1) / checkpoint_every;
-    sim->adj_ckpt.resize(static_cast<size_t>(nck));
-    for (auto& q : sim->adj_ckpt) WD_CUDA(alloc_snap(sim, q));
-    WD_CUDA(alloc_snap(sim, sim->adj_end));
+    // snapshots are kept between windows and grown when a window needs more
+    const size_t nck = static_cast<size_t>((steps + checkpoint_every - 1) / checkpoint_every);
+    sim->adj_steps = 0;
+    for (size_t k = sim->adj_ckpt.size(); k < nck; ++k) {
+        sim->adj_ckpt.emplace_back();
+        WD_CUDA(alloc_snap(sim, sim->adj_ckpt.back()));
+    }
+    if (!sim->adj_end.pos) WD_CUDA(alloc_snap(sim, sim->adj_end));
     int64_t hist_over0 = 0;
     rc = read_counter(sim, wd::kCntHistOverflow, &hist_over0);
     if (rc) return rc;
@@ -1621,11 +1766,13 @@ int wd_adjoint_backward(wd_sim* sim, const float* d_gx, const float* d_gv, float
         WD_CUDA(dalloc(&sim->adj_theta, static_cast<size_t>(3) * n));
     }
     const int every = sim->adj_every;
-    if (sim->adj_seg.size() < static_cast<size_t>(every) + 1) {
-        const size_t old = sim->adj_seg.size();
-        sim->adj_seg.resize(static_cast<size_t>(every) + 1);
-        for (size_t k = old; k < sim->adj_seg.size(); ++k) WD_CUDA(alloc_snap(sim, sim->adj_seg[k]));
+    if (sim->adj_tape.size() < static_cast<size_t>(every) + 1) clear_adj_graphs(sim);
+    for (size_t k = sim->adj_tape.size(); k < static_cast<size_t>(every) + 1; ++k) {
+        sim->adj_tape.emplace_back();
+        WD_CUDA(alloc_tape_step(sim, sim->adj_tape.back()));
     }
+    if (!sim->adj_ovf) WD_CUDA(dalloc(&sim->adj_ovf, 1));
+    WD_CUDA(cudaMemsetAsync(sim->adj_ovf, 0, sizeof(unsigned long long), st));
     unsigned long long saved[wd::kNumCounters];
     WD_CUDA(cudaMemcpyAsync(saved, sim->counters, sizeof(saved), cudaMemcpyDeviceToHost, st));
     int rc = sync_stream(sim);
@@ -1639,63 +1786,40 @@ int wd_adjoint_backward(wd_sim* sim, const float* d_gx, const float* d_gv, float
     WD_CUDA(cudaMemsetAsync(sim->adj_theta, 0, sizeof(double) * 3 * n, st));
     const DevParams& P = sim->P;
     const wd::Skip none{nullptr, 0.f};
-    const int64_t nseg = static_cast<int64_t>(sim->adj_ckpt.size());
+    const size_t rows = static_cast<size_t>(n) * wd::kHistCap;
+    const int64_t nseg = static_cast<int64_t>(sim->adj_ckpt.size() == 0 ? 0 :
+                                              (sim->adj_steps + every - 1) / every);
     for (int64_t seg = nseg - 1; seg >= 0; --seg) {
         const int64_t s0 = seg * every;
         const int len = static_cast<int>(std::min<int64_t>(sim->adj_steps, s0 + every) - s0);
-        // replay the segment from its checkpoint, keeping every step's state
-        WD_CUDA(put_snap(sim, sim->adj_ckpt[static_cast<size_t>(seg)]));
-        for (int k = 0; k < len; ++k) {
-            rc = wd_step(sim, 1);
-            if (rc) return rc;
-            WD_CUDA(take_snap(sim, sim->adj_seg[static_cast<size_t>(k) + 1]));
-        }
-        for (int t = len - 1; t >= 0; --t) {
-            const wd_sim::Snap& now = t == 0 ? sim->adj_ckpt[static_cast<size_t>(seg)]
-                                             : sim->adj_seg[static_cast<size_t>(t)];
-            const wd_sim::Snap& next = sim->adj_seg[static_cast<size_t>(t) + 1];
-            WD_CUDA(put_snap(sim, now));
-            // the step's neighbor search and gather, as the forward ran them
-            wd::launch_search(P, tab(sim, sim->sceneA), sim->posA, sim->idsA, sim->sb, none,
-                              nullptr, 0, sim->counters, st);
-            wd::launch_gather(P, sim->sb, sim->posA, sim->velA, sim->posB, sim->velB, sim->idsB,
-                              nullptr, nullptr, nullptr, nullptr, false,
-                              hist ? sim->hcnt_slot : nullptr, hist ? sim->hcnt_g : nullptr,
-                              nullptr, nullptr, false, sim->counters, nullptr, nullptr, none, st);
-            if (hist) {
-                wd::launch_counts_by_id(n, next.ids, next.hcnt, sim->adj_cnt_next, st);
-                WD_CUDA(cudaMemsetAsync(sim->adj_lxi[cur ^ 1], 0, sizeof(float4) * n * wd::kHistCap, st));
-            }
-            wd::launch_adj_prep(n, P.dt, sim->velB, sim->idsB, sim->adj_lx[cur], sim->adj_lv[cur],
-                                sim->adj_lvt, sim->adj_lf, st);
-            wd::AdjArgs a{};
-            a.pos = sim->posB; a.vel = sim->velB; a.ids = sim->idsB; a.table = sim->sb.table;
-            a.hist_in = hist ? now.hist : nullptr;
-            a.hcnt_in = hist ? sim->hcnt_g : nullptr;
-            a.hist_next = hist ? next.hist : nullptr;
-            a.hcnt_next = hist ? sim->adj_cnt_next : nullptr;
-            a.lx = sim->adj_lx[cur]; a.lvt = sim->adj_lvt; a.lf = sim->adj_lf;
-            a.lxi = hist ? sim->adj_lxi[cur] : nullptr;
-            a.lx_out = sim->adj_lx[cur ^ 1]; a.lv_out = sim->adj_lv[cur ^ 1];
-            a.lxi_out = hist ? sim->adj_lxi[cur ^ 1] : nullptr;
-            a.theta = sim->adj_theta;
-            a.kt_from_kn = sim->cfg.tangential_stiffness > 0.f ? 0 : 1;
-            wd::launch_adj_step(P, a, st);
-            WD_CUDA(cudaGetLastError());
-            cur ^= 1;
-        }
+        // replay the segment from its checkpoint, recording each step's sorted input,
+        // contacts and springs on the tape (the springs live on the tape meanwhile)
+        const wd_sim::Snap& ck = sim->adj_ckpt[static_cast<size_t>(seg)];
+        WD_CUDA(put_snap(sim, ck));
+        if (hist)
+            WD_CUDA(cudaMemcpyAsync(sim->adj_tape[0].hist, ck.hist, rows * sizeof(float4),
+                                    cudaMemcpyDeviceToDevice, st));
+        WD_CUDA(run_adj_graph(sim, len, -1));
+        WD_CUDA(run_adj_graph(sim, len, cur));
+        if (len % 2) cur ^= 1;
     }
     if (d_gx0) wd::launch_f4_to_aos3(n, sim->adj_lx[cur], d_gx0, st);
     if (d_gv0) wd::launch_f4_to_aos3(n, sim->adj_lv[cur], d_gv0, st);
     wd::launch_segment_sums(sim->adj_theta, n, 3, segments(sim), sim->partials, sim->scene_sums, st);
     WD_CUDA(cudaGetLastError());
     double th[3];
+    unsigned long long ovf = 0;
     WD_CUDA(cudaMemcpyAsync(th, sim->scene_sums, sizeof(th), cudaMemcpyDeviceToHost, st));
+    WD_CUDA(cudaMemcpyAsync(&ovf, sim->adj_ovf, sizeof(ovf), cudaMemcpyDeviceToHost, st));
     // back to the window's end, counters as they were
     WD_CUDA(put_snap(sim, sim->adj_end));
     WD_CUDA(cudaMemcpyAsync(sim->counters, saved, sizeof(saved), cudaMemcpyHostToDevice, st));
     rc = sync_stream(sim);
     if (rc) return rc;
+    if (ovf)
+        return fail(WD_ERR_CAPACITY, "wd_adjoint_backward: a grain had more than " +
+                                         std::to_string(wd::kAdjContacts) +
+                                         " pair contacts in one step of the window");
     if (theta3) {
         const float e = sim->cfg.restitution;
         theta3[0] = th[0];
