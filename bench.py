@@ -15,10 +15,11 @@ value  -- device time of K steps (CUDA events on the library's stream around eac
 e2e    -- the same metric through the C ABI with host buffers: each step
           wd_set_state() from pinned host memory, wd_step(1), wd_get_positions() to
           pinned host memory, all inside the timed region.
-neighbor search -- Verlet lists with a skin of 0.1 mean diameters by default
-          (--skin; 0 searches the grid every step as the reference does): the grid
-          search and sort run only when a grain has moved 0.45 skin since the last
-          build; the results are bit-identical either way.
+neighbor search -- Verlet lists, skin and contact-kernel block size chosen by the
+          library's autotuner before the warm-up (--skin S fixes the skin; 0 searches
+          the grid every step as the reference does): the grid search and sort run
+          only when a grain has moved 0.45 skin since the last build; the results are
+          bit-identical either way.
 roofline -- the contact kernel (forces + integrator, the dominant kernel): its
           algorithmic bytes per launch over its average event-timed duration,
           against the measured HBM copy bandwidth.
@@ -71,8 +72,8 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--phase-steps", type=int, default=50)
     ap.add_argument("--skin", type=float, default=-1.0,
-                    help="Verlet-list skin in m (simulation.neighbor_skin); negative: 0.1 x the "
-                         "mean grain diameter; 0: grid search every step, as the reference")
+                    help="Verlet-list skin in m (simulation.neighbor_skin); negative: chosen by "
+                         "the autotuner; 0: grid search every step, as the reference")
     ap.add_argument("--direct", action="store_true",
                     help="launch each step's kernels directly instead of as one CUDA graph "
                          "(for per-kernel profilers, which cannot see inside graphs with "
@@ -277,8 +278,7 @@ def run_ours(args) -> int:
             dist.barrier()
 
     def with_skin(sc):
-        skin = args.skin if args.skin >= 0 else 0.1 * 2.0 * float(np.mean(sc.radius))
-        sc.cfg.neighbor_skin = skin
+        sc.cfg.neighbor_skin = max(args.skin, 0.0)
         return sc
 
     scenes_total = None
@@ -297,6 +297,13 @@ def run_ours(args) -> int:
         scene = with_skin(scene_for(args.workload, n=args.grains, seed=12345 + rank))
         sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
     sim.set_kernel_timing(args.direct)
+    tuned = None
+    if args.skin < 0:
+        # the autotuner picks the skin and the contact kernel's block size (untimed;
+        # the state is restored and the results do not depend on the choice)
+        skin, block = sim.autotune(steps=40)
+        scene.cfg.neighbor_skin = skin
+        tuned = {"neighbor_skin_m": skin, "contact_block": block}
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -429,6 +436,7 @@ def run_ours(args) -> int:
                                "mean_list_length": mean_list} if lists else None,
             "history_entries_per_grain": entries / n,
             "scene_results": scene_results,
+            "autotuned": tuned,
         }
         print(json.dumps(line), flush=True)
     sim.close()

@@ -253,6 +253,17 @@ int wd_compute_max_acceleration(wd_sim* sim, float* max_accel);
  * particles_per_cell grains in a cell (src/find_neighbors_kernel.cu:230-234). No
  * grain is dropped here: the sorted search has no per-cell capacity. */
 int wd_grid_overflow_count(wd_sim* sim, int64_t* count);
+/* Switch the Verlet-list skin of a live handle (0: grid search every step). The
+ * trajectory does not depend on it. Semi-implicit Euler only for a skin > 0. */
+int wd_set_neighbor_skin(wd_sim* sim, float skin);
+/* Autotuner (extension): times `steps` steps for each neighbor skin in {0, 0.05,
+ * 0.1, 0.2, 0.4} mean diameters and contact-kernel block size in {128, 256} from the
+ * same saved state, keeps the fastest and restores the state (results do not depend
+ * on the choice). With cache_path, a line "key skin block" keyed by grain count,
+ * scenes, grid, SM count, history, integrator and launch mode is reused or appended.
+ * skin_out / block_out (may be NULL) receive the choice. */
+int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_out,
+                int32_t* block_out);
 /* Verlet lists (simulation.neighbor_skin > 0): builds so far, kernels one build
  * launches, and the mean list length of the last build (0 without lists). */
 int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length);

@@ -108,5 +108,8 @@ def test_batch_entry_points_take_the_python_argument_forms():
         lib.wd_write_state_file(None, b"x"),
         lib.wd_write_checkpoint(None, b"x"),
         lib.wd_pack_frame(None, None, ptr(d)),
+        lib.wd_set_neighbor_skin(None, 1e-3),
+        lib.wd_autotune(None, 10, None, None, None),
+        lib.wd_list_stats(None, None, None, None),
     ]
     assert all(c == -1 for c in calls), calls

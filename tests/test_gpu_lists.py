@@ -120,3 +120,43 @@ def test_batch_with_lists_equals_searched_batch():
         sb.advance(150)
         sims.append(sb)
     _same(*sims)
+
+
+def test_skin_switch_mid_run_stays_exact():
+    cfg, st, rad = packed_poly(n=1500, seed=27, mu=0.5)
+    cfg.kernel_timing = False
+    ref = ParticleDynamics(cfg, state=st, radius=rad)
+    sw = ParticleDynamics(cfg, state=st, radius=rad)
+    ref.advance(90)
+    sw.advance(30)
+    sw.set_neighbor_skin(0.5e-3)
+    sw.advance(30)
+    sw.set_neighbor_skin(0.0)
+    sw.advance(15)
+    sw.set_neighbor_skin(1e-3)
+    sw.advance(15)
+    _same(ref, sw)
+
+
+def test_autotune_restores_the_state_and_caches(tmp_path):
+    sc = column_collapse(8192, diameters="lognormal", mu=0.5, cic=32)
+    sc.cfg.kernel_timing = False
+    ref = ParticleDynamics(sc.cfg, state=sc.state, radius=sc.radius)
+    tuned = ParticleDynamics(sc.cfg, state=sc.state, radius=sc.radius)
+    ref.advance(20)
+    tuned.advance(20)
+    before = tuned.get_state()
+    t0 = tuned.time
+    cache = tmp_path / "tune.txt"
+    skin, block = tuned.autotune(steps=20, cache=str(cache))
+    assert block in (128, 256) and skin >= 0.0
+    np.testing.assert_array_equal(tuned.get_state(), before)
+    assert tuned.time == t0
+    ref.advance(50)
+    tuned.advance(50)
+    _same(ref, tuned)
+    lines = cache.read_text().splitlines()
+    assert len(lines) == 1 and lines[0].startswith("n=8192,")
+    other = ParticleDynamics(sc.cfg, state=sc.state, radius=sc.radius)
+    assert other.autotune(steps=20, cache=str(cache)) == (np.float32(skin), block)
+    assert len(cache.read_text().splitlines()) == 1

@@ -294,10 +294,10 @@ k_stability(DevParams P0, SceneTab T, const float4* __restrict__ pos,
 }  // namespace
 
 void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip,
-                  cudaStream_t st) {
-    const int nb = blocks_for(P.n);
+                  cudaStream_t st, int block) {
+    const int nb = blocks_for(P.n, block);
     const bool batch = a.scene_params != nullptr;
-#define WD_FORCE(H, PI, B) k_force<H, PI, B><<<nb, kBlock, 0, st>>>(P, a, skip)
+#define WD_FORCE(H, PI, B) k_force<H, PI, B><<<nb, block, 0, st>>>(P, a, skip)
     if (P.history) {
         if (picard) { if (batch) WD_FORCE(true, true, true); else WD_FORCE(true, true, false); }
         else { if (batch) WD_FORCE(true, false, true); else WD_FORCE(true, false, false); }

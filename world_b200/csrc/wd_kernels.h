@@ -123,8 +123,9 @@ struct Segments {
     int total_chunks;
 };
 
+// block: threads per block (a multiple of 32, at most kBlock; the autotuner's choice)
 void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip,
-                  cudaStream_t st);
+                  cudaStream_t st, int block = kBlock);
 
 // Verlet lists (simulation.neighbor_skin > 0, semi-implicit Euler). list_ctrl words:
 // [0] max |x - x_build|^2 since the build (float bits), [1] a list overflowed,
@@ -149,7 +150,8 @@ void launch_list_build(const DevParams& P, SceneTab T, const float4* pos, const 
 void launch_list_copy(int n, const float4* pos, const float4* vel, const int* ids,
                       const int* hcnt, const int* scene, float4* pos_out, float4* vel_out,
                       int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st);
-void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st);
+void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st,
+                       int block = kBlock);
 void launch_list_length(int n, const int* nbr_cnt, unsigned long long* out, cudaStream_t st);
 
 // Total energy per scene at the sorted state (after a search): per-grain FP64 sums,

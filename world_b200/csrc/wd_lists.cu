@@ -289,15 +289,15 @@ void launch_list_copy(int n, const float4* pos, const float4* vel, const int* id
                                                   vel_out, ids_out, hcnt_out, scene_out, skip);
 }
 
-void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st) {
-    const int nb = blocks_for(P.n);
+void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, int block) {
+    const int nb = blocks_for(P.n, block);
     const bool batch = a.scene_params != nullptr;
     if (P.history) {
-        if (batch) k_force_list<true, true><<<nb, kBlock, 0, st>>>(P, a);
-        else k_force_list<true, false><<<nb, kBlock, 0, st>>>(P, a);
+        if (batch) k_force_list<true, true><<<nb, block, 0, st>>>(P, a);
+        else k_force_list<true, false><<<nb, block, 0, st>>>(P, a);
     } else {
-        if (batch) k_force_list<false, true><<<nb, kBlock, 0, st>>>(P, a);
-        else k_force_list<false, false><<<nb, kBlock, 0, st>>>(P, a);
+        if (batch) k_force_list<false, true><<<nb, block, 0, st>>>(P, a);
+        else k_force_list<false, false><<<nb, block, 0, st>>>(P, a);
     }
 }
 

@@ -128,6 +128,7 @@ struct wd_sim {
     // ping-pongs between the A and B buffers; lpar counts the swaps mod 2.
     bool lists = false;
     int lpar = 0;
+    int force_block = wd::kBlock;   // threads per block of the contact kernel
     int* nbr = nullptr;
     int* nbr_cnt = nullptr;
     float4* xbuild = nullptr;
@@ -470,7 +471,7 @@ cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
                           batch ? s->sceneB : nullptr, true, s->counters, s->scene_overflow, s->d_scene_P, none, st);
         if (mid) cudaEventRecord(mid, st);
         fa.hcnt_in = s->hcnt_g;
-        wd::launch_force(P, fa, false, none, st);
+        wd::launch_force(P, fa, false, none, st, s->force_block);
         return cudaGetLastError();
     }
     for (int k = 0; k < s->picard_iters; ++k) {
@@ -491,7 +492,7 @@ cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
         fa.res_slot = s->picard_res + k;
         fa.picard_used = s->picard_used;
         fa.iter = k;
-        wd::launch_force(P, fa, true, skip, st);
+        wd::launch_force(P, fa, true, skip, st, s->force_block);
     }
     return cudaGetLastError();
 }
@@ -571,7 +572,7 @@ cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool captu
     a.scene_params = batch ? s->d_scene_P : nullptr;
     a.scene = s->sceneA;
     a.scene_out = s->sceneB;
-    wd::launch_force_list(P, a, st);
+    wd::launch_force_list(P, a, st, s->force_block);
     return cudaGetLastError();
 }
 
@@ -1566,6 +1567,50 @@ int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* c
     return WD_OK;
 }
 
+// Skin switch on a live handle (the autotuner's knob): list buffers on first use; on
+// entering list mode the current buffers are labelled with the spring parity.
+static int apply_skin(wd_sim* s, float skin) {
+    if (skin < 0.f) return fail(WD_ERR_INVALID, "neighbor skin must be >= 0");
+    if (skin > 0.f && s->picard)
+        return fail(WD_ERR_INVALID, "neighbor lists cover semi-implicit Euler only");
+    const bool lists = skin > 0.f;
+    if (lists && !s->nbr) {
+        const int n = s->n;
+        WD_CUDA(dalloc(&s->nbr, static_cast<size_t>(n) * wd::kNbrCap));
+        WD_CUDA(dalloc(&s->nbr_cnt, n));
+        WD_CUDA(dalloc(&s->xbuild, n));
+        WD_CUDA(dalloc(&s->list_ctrl, wd::kLcWords));
+        WD_CUDA(dalloc(&s->list_len, 1));
+        WD_CUDA(cudaMemsetAsync(s->list_ctrl, 0, sizeof(uint32_t) * wd::kLcWords, s->stream));
+    }
+    if (lists && !s->lists) s->lpar = s->P.history ? s->hist_cur : s->lpar;
+    s->lists = lists;
+    s->cfg.neighbor_skin = skin;
+    s->P.skin = skin;
+    for (size_t k = 0; k < s->scene_P.size(); ++k) {
+        s->scene_P[k].skin = skin;
+        s->scene_cfg[k].neighbor_skin = skin;
+    }
+    if (s->d_scene_P)
+        WD_CUDA(cudaMemcpyAsync(s->d_scene_P, s->scene_P.data(), sizeof(DevParams) * s->scene_P.size(),
+                                cudaMemcpyHostToDevice, s->stream));
+    WD_CUDA(request_list_build(s));
+    s->graph_dirty = true;
+    clear_adj_graphs(s);
+    return sync_stream(s);
+}
+
+static std::string tune_key(const wd_sim* s) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "n=%d,scenes=%d,grid=%dx%dx%d,sm=%d,hist=%d,picard=%d,graph=%d",
+                  s->n, s->scenes, s->cfg.grid[0], s->cfg.grid[1], s->cfg.grid[2], sms,
+                  s->P.history, s->picard ? 1 : 0, s->cfg.kernel_timing ? 0 : 1);
+    return buf;
+}
+
 int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_list_stats: NULL handle");
     if (kernels_each)
@@ -1621,7 +1666,7 @@ cudaError_t adj_replay_body(wd_sim* s, int len, bool capture, cudaStream_t st) {
         fa.hist_out = hist ? T1.hist : nullptr;
         fa.hcnt_out = hist ? s->hcnt_slot : nullptr;
         fa.counters = s->counters;
-        wd::launch_force(P, fa, false, none, st);
+        wd::launch_force(P, fa, false, none, st, s->force_block);
     }
     if (hist)
         wd::launch_counts_by_id(n, s->idsA, s->hcnt_slot,
@@ -1687,6 +1732,113 @@ cudaError_t run_adj_graph(wd_sim* s, int len, int parity) {
         it = s->adj_graphs.emplace(key, exec).first;
     }
     return cudaGraphLaunch(it->second, s->stream);
+}
+
+int wd_set_neighbor_skin(wd_sim* sim, float skin) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_set_neighbor_skin: NULL handle");
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    return apply_skin(sim, skin);
+}
+
+int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_out,
+                int32_t* block_out) {
+    if (!sim || steps < 1) return fail(WD_ERR_INVALID, "wd_autotune: bad argument");
+    const std::string key = tune_key(sim);
+    float best_skin = sim->cfg.neighbor_skin;
+    int best_block = sim->force_block;
+    bool cached = false;
+    if (cache_path) {
+        if (std::FILE* f = std::fopen(cache_path, "r")) {
+            char line[512];
+            while (std::fgets(line, sizeof(line), f)) {
+                char k[300];
+                float sk = 0.f;
+                int bl = 0;
+                if (std::sscanf(line, "%299s %f %d", k, &sk, &bl) == 3 && key == k) {
+                    best_skin = sk;
+                    best_block = bl;
+                    cached = true;
+                }
+            }
+            std::fclose(f);
+        }
+    }
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    if (!cached) {
+        // every candidate gives the same trajectory (lists and the block size change
+        // the schedule, not the arithmetic): time each from the same saved state
+        double mean_r = 0.0;
+        for (float r : sim->radius) mean_r += r;
+        mean_r /= static_cast<double>(sim->radius.size());
+        const float d = static_cast<float>(2.0 * mean_r);
+        std::vector<float> skins = {0.f};
+        if (!sim->picard)
+            for (float f : {0.05f, 0.1f, 0.2f, 0.4f}) skins.push_back(f * d);
+        const int blocks[] = {128, 256};
+        wd_sim::Snap snap;
+        WD_CUDA(alloc_snap(sim, snap));
+        WD_CUDA(take_snap(sim, snap));
+        unsigned long long saved[wd::kNumCounters];
+        WD_CUDA(cudaMemcpyAsync(saved, sim->counters, sizeof(saved), cudaMemcpyDeviceToHost, sim->stream));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float best_ms = INFINITY;
+        for (float sk : skins) {
+            for (int bl : blocks) {
+                rc = apply_skin(sim, sk);
+                if (rc == WD_OK) {
+                    sim->force_block = bl;
+                    sim->graph_dirty = true;
+                    const cudaError_t e = put_snap(sim, snap);
+                    if (e != cudaSuccess) rc = fail(WD_ERR_CUDA, cudaGetErrorString(e));
+                }
+                if (rc == WD_OK) rc = wd_step(sim, 2);  // graphs, first list build
+                if (rc == WD_OK) {
+                    cudaEventRecord(e0, sim->stream);
+                    rc = wd_step(sim, steps);
+                    cudaEventRecord(e1, sim->stream);
+                }
+                if (rc == WD_OK) rc = sync_stream(sim);
+                if (rc != WD_OK) break;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best_skin = sk;
+                    best_block = bl;
+                }
+            }
+            if (rc != WD_OK) break;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc == WD_OK) {
+            const cudaError_t e = put_snap(sim, snap);
+            if (e != cudaSuccess) rc = fail(WD_ERR_CUDA, cudaGetErrorString(e));
+        }
+        if (rc == WD_OK) {
+            cudaMemcpyAsync(sim->counters, saved, sizeof(saved), cudaMemcpyHostToDevice, sim->stream);
+            rc = sync_stream(sim);
+        }
+        free_snap(snap);
+        if (rc) return rc;
+        if (cache_path) {
+            if (std::FILE* f = std::fopen(cache_path, "a")) {
+                std::fprintf(f, "%s %.9g %d\n", key.c_str(), static_cast<double>(best_skin), best_block);
+                std::fclose(f);
+            }
+        }
+    }
+    rc = apply_skin(sim, best_skin);
+    if (rc) return rc;
+    sim->force_block = best_block;
+    sim->graph_dirty = true;
+    if (skin_out) *skin_out = best_skin;
+    if (block_out) *block_out = best_block;
+    return WD_OK;
 }
 
 int wd_set_contact_params(wd_sim* sim, float mu, float restitution, float k_n) {

@@ -328,6 +328,18 @@ class ParticleDynamics:
         check(lib.wd_radix_search_count(self._h, ctypes.byref(c), ctypes.byref(k)))
         return int(c.value), int(k.value)
 
+    def set_neighbor_skin(self, skin: float) -> None:
+        check(lib.wd_set_neighbor_skin(self._h, ctypes.c_float(skin)))
+
+    def autotune(self, steps: int = 50, cache: Optional[str] = None) -> tuple[float, int]:
+        """Pick the neighbor skin and contact-kernel block size by timing (the state is
+        restored afterwards; results do not depend on the choice). Returns them."""
+        sk = ctypes.c_float()
+        bl = ctypes.c_int32()
+        check(lib.wd_autotune(self._h, int(steps), None if cache is None else str(cache).encode(),
+                              ctypes.byref(sk), ctypes.byref(bl)))
+        return float(sk.value), int(bl.value)
+
     def list_stats(self) -> tuple[int, int, float]:
         """(Verlet-list builds so far, kernels each build launches, mean list length)."""
         b = ctypes.c_int64()
