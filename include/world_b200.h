@@ -175,8 +175,18 @@ int wd_get_positions_device(wd_sim* sim, float* d_positions);
 /* Use an external stream (cudaStream_t as void*); NULL restores the own stream. */
 int wd_set_stream(wd_sim* sim, void* stream);
 int wd_get_stream(const wd_sim* sim, void** stream);
-/* Block until all work queued on the handle's stream is done. */
+/* Block until all work queued on the handle's streams (steps and copies) is done. */
 int wd_synchronize(wd_sim* sim);
+/* Asynchronous host I/O (extension): uploads and downloads run on two copy streams,
+ * through double-buffered device staging, ordered against the steps by events, so a
+ * loop of set_state / step / get_positions overlaps the upload of one step with the
+ * step before and the download of the step before that. The host buffers (pinned for
+ * real overlap) must stay valid and unchanged until wd_synchronize. wd_io_join orders
+ * the step stream after every copy issued so far and the copy streams after the step
+ * stream's current point. */
+int wd_set_state_async(wd_sim* sim, const float* state);
+int wd_get_positions_async(wd_sim* sim, float* positions);
+int wd_io_join(wd_sim* sim);
 
 /* ---- files and frames ------------------------------------------------------------ */
 

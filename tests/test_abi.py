@@ -111,5 +111,8 @@ def test_batch_entry_points_take_the_python_argument_forms():
         lib.wd_set_neighbor_skin(None, 1e-3),
         lib.wd_autotune(None, 10, None, None, None),
         lib.wd_list_stats(None, None, None, None),
+        lib.wd_set_state_async(None, ptr(d)),
+        lib.wd_get_positions_async(None, ptr(d)),
+        lib.wd_io_join(None),
     ]
     assert all(c == -1 for c in calls), calls

@@ -201,3 +201,30 @@ def test_checkpoint_resume_is_bit_identical(tmp_path):
     assert frame[3 * a.n] == np.float32(a.time)
     np.testing.assert_array_equal(frame[3 * a.n + 1:], [1, 2, 3, 4, 5])
     a.close(); b.close()
+
+
+def test_async_io_loop_matches_the_synchronous_one():
+    from test_gpu_parity import packed_poly
+    cfg, st, rad = packed_poly(n=1200, seed=41, mu=0.5)
+    a = ParticleDynamics(cfg, state=st, radius=rad)
+    b = ParticleDynamics(cfg, state=st, radius=rad)
+    a.advance(5)
+    b.advance(5)
+    host = a.get_state()
+    rng = np.random.default_rng(2)
+    states = [host + rng.normal(0, 1e-6, host.shape).astype(np.float32) for _ in range(4)]
+    outs_sync, outs_async = [], [np.empty(3 * a.n, np.float32) for _ in range(4)]
+    for s_ in states:
+        a.set_state(s_)
+        a.advance(1)
+        outs_sync.append(a.get_positions())
+    check(lib.wd_io_join(b.handle))
+    for k, s_ in enumerate(states):
+        check(lib.wd_set_state_async(b.handle, ptr(s_)))
+        check(lib.wd_step(b.handle, 1))
+        check(lib.wd_get_positions_async(b.handle, ptr(outs_async[k])))
+    check(lib.wd_synchronize(b.handle))
+    for x, y in zip(outs_sync, outs_async):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(a.get_state(), b.get_state())
+    a.close(); b.close()

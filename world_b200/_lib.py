@@ -76,6 +76,9 @@ SIGNATURES = {
     "wd_pack_frame": ([_p, _p, _p], c_int),
     "wd_list_stats": ([_p, _i64, POINTER(c_int32), _d], c_int),
     "wd_set_neighbor_skin": ([_p, c_float], c_int),
+    "wd_set_state_async": ([_p, _p], c_int),
+    "wd_get_positions_async": ([_p, _p], c_int),
+    "wd_io_join": ([_p], c_int),
     "wd_autotune": ([_p, c_int32, c_char_p, POINTER(c_float), POINTER(c_int32)], c_int),
     "wd_set_contact_params": ([_p, c_float, c_float, c_float], c_int),
     "wd_adjoint_record": ([_p, c_int64, c_int32], c_int),

@@ -126,6 +126,16 @@ struct wd_sim {
 
     // Verlet lists (simulation.neighbor_skin > 0, semi-implicit Euler): the state
     // ping-pongs between the A and B buffers; lpar counts the swaps mod 2.
+    // asynchronous host I/O: uploads on io_up, downloads on io_down, double-buffered
+    // device staging; events order them against the step stream
+    cudaStream_t io_up = nullptr, io_down = nullptr;
+    float* io_in[2] = {nullptr, nullptr};
+    float* io_out[2] = {nullptr, nullptr};
+    cudaEvent_t ev_in_ready[2] = {nullptr, nullptr}, ev_in_free[2] = {nullptr, nullptr};
+    cudaEvent_t ev_out_ready[2] = {nullptr, nullptr}, ev_out_free[2] = {nullptr, nullptr};
+    cudaEvent_t ev_join = nullptr;
+    int io_i = 0, io_o = 0;
+
     bool lists = false;
     int lpar = 0;
     int force_block = wd::kBlock;   // threads per block of the contact kernel
@@ -327,6 +337,16 @@ void free_sim(wd_sim* s) {
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : s->ev_pending) cudaEventDestroy(e);
     free_tape(s);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(s->io_in[b]);
+        cudaFree(s->io_out[b]);
+        cudaEvent_t evs[] = {s->ev_in_ready[b], s->ev_in_free[b], s->ev_out_ready[b], s->ev_out_free[b]};
+        for (cudaEvent_t e : evs)
+            if (e) cudaEventDestroy(e);
+    }
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->io_up) cudaStreamDestroy(s->io_up);
+    if (s->io_down) cudaStreamDestroy(s->io_down);
     void* adj[] = {s->adj_lx[0], s->adj_lx[1], s->adj_lv[0], s->adj_lv[1], s->adj_lxi[0],
                    s->adj_lxi[1], s->adj_lvt, s->adj_lf, s->adj_cnt_next, s->adj_theta};
     for (void* p : adj) cudaFree(p);
@@ -1270,7 +1290,75 @@ int wd_get_stream(const wd_sim* sim, void** stream) {
 
 int wd_synchronize(wd_sim* sim) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_synchronize: NULL handle");
+    if (sim->io_up) WD_CUDA(cudaStreamSynchronize(sim->io_up));
+    if (sim->io_down) WD_CUDA(cudaStreamSynchronize(sim->io_down));
     return sync_stream(sim);
+}
+
+static int io_setup(wd_sim* s) {
+    if (s->io_up) return WD_OK;
+    const size_t n = static_cast<size_t>(s->n);
+    WD_CUDA(cudaStreamCreateWithFlags(&s->io_up, cudaStreamNonBlocking));
+    WD_CUDA(cudaStreamCreateWithFlags(&s->io_down, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+        WD_CUDA(dalloc(&s->io_in[b], 6 * n));
+        WD_CUDA(dalloc(&s->io_out[b], 3 * n));
+        cudaEvent_t* evs[] = {&s->ev_in_ready[b], &s->ev_in_free[b], &s->ev_out_ready[b],
+                              &s->ev_out_free[b]};
+        for (cudaEvent_t* e : evs) WD_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    WD_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+    return WD_OK;
+}
+
+int wd_set_state_async(wd_sim* sim, const float* state) {
+    if (!sim || !state) return fail(WD_ERR_INVALID, "wd_set_state_async: NULL argument");
+    int rc = io_setup(sim);
+    if (rc) return rc;
+    const int i = sim->io_i;
+    sim->io_i ^= 1;
+    const size_t bytes = sizeof(float) * 6 * static_cast<size_t>(sim->n);
+    WD_CUDA(cudaStreamWaitEvent(sim->io_up, sim->ev_in_free[i], 0));
+    WD_CUDA(cudaMemcpyAsync(sim->io_in[i], state, bytes, cudaMemcpyHostToDevice, sim->io_up));
+    WD_CUDA(cudaEventRecord(sim->ev_in_ready[i], sim->io_up));
+    WD_CUDA(cudaStreamWaitEvent(sim->stream, sim->ev_in_ready[i], 0));
+    wd::launch_state_from_aos(sim->n, sim->io_in[i], sim->posA, sim->velA, sim->idsA, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    WD_CUDA(cudaEventRecord(sim->ev_in_free[i], sim->stream));
+    WD_CUDA(request_list_build(sim));
+    return WD_OK;
+}
+
+int wd_get_positions_async(wd_sim* sim, float* positions) {
+    if (!sim || !positions) return fail(WD_ERR_INVALID, "wd_get_positions_async: NULL argument");
+    int rc = io_setup(sim);
+    if (rc) return rc;
+    const int j = sim->io_o;
+    sim->io_o ^= 1;
+    const size_t bytes = sizeof(float) * 3 * static_cast<size_t>(sim->n);
+    WD_CUDA(cudaStreamWaitEvent(sim->stream, sim->ev_out_free[j], 0));
+    wd::launch_positions_to_aos(sim->n, sim->posA, sim->idsA, sim->io_out[j], sim->stream);
+    WD_CUDA(cudaGetLastError());
+    WD_CUDA(cudaEventRecord(sim->ev_out_ready[j], sim->stream));
+    WD_CUDA(cudaStreamWaitEvent(sim->io_down, sim->ev_out_ready[j], 0));
+    WD_CUDA(cudaMemcpyAsync(positions, sim->io_out[j], bytes, cudaMemcpyDeviceToHost, sim->io_down));
+    WD_CUDA(cudaEventRecord(sim->ev_out_free[j], sim->io_down));
+    return WD_OK;
+}
+
+int wd_io_join(wd_sim* sim) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_io_join: NULL handle");
+    int rc = io_setup(sim);
+    if (rc) return rc;
+    // the step stream waits for every copy issued so far, the copy streams for the step stream
+    WD_CUDA(cudaEventRecord(sim->ev_join, sim->io_up));
+    WD_CUDA(cudaStreamWaitEvent(sim->stream, sim->ev_join, 0));
+    WD_CUDA(cudaEventRecord(sim->ev_join, sim->io_down));
+    WD_CUDA(cudaStreamWaitEvent(sim->stream, sim->ev_join, 0));
+    WD_CUDA(cudaEventRecord(sim->ev_join, sim->stream));
+    WD_CUDA(cudaStreamWaitEvent(sim->io_up, sim->ev_join, 0));
+    WD_CUDA(cudaStreamWaitEvent(sim->io_down, sim->ev_join, 0));
+    return WD_OK;
 }
 
 int wd_get_history(wd_sim* sim, int32_t* count, int32_t* partner, float* xi) {
