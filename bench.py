@@ -302,9 +302,9 @@ def run_ours(args) -> int:
     if args.skin < 0:
         # the autotuner picks the skin and the contact kernel's block size (untimed;
         # the state is restored and the results do not depend on the choice)
-        skin, block = sim.autotune(steps=40)
+        skin, _ = sim.autotune(steps=40)
         scene.cfg.neighbor_skin = skin
-        tuned = {"neighbor_skin_m": skin, "contact_block": block}
+        tuned = sim.tuning()
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")

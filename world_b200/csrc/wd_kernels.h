@@ -150,8 +150,9 @@ void launch_list_build(const DevParams& P, SceneTab T, const float4* pos, const 
 void launch_list_copy(int n, const float4* pos, const float4* vel, const int* ids,
                       const int* hcnt, const int* scene, float4* pos_out, float4* vel_out,
                       int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st);
+// min_blocks: the register variant (5: 48 registers, 4: 64 registers per thread)
 void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st,
-                       int block = kBlock);
+                       int block = kBlock, int min_blocks = 5);
 void launch_list_length(int n, const int* nbr_cnt, unsigned long long* out, cudaStream_t st);
 
 // Total energy per scene at the sorted state (after a search): per-grain FP64 sums,

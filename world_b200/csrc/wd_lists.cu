@@ -110,18 +110,25 @@ __device__ __forceinline__ unsigned long long visit_key(const DevParams& P, int 
            static_cast<unsigned>(jd);
 }
 
-template <bool HIST, bool BATCH>
-__global__ void __launch_bounds__(kBlock, 5)
+// MINB resident blocks per SM: 5 caps registers at 48 (more warps, a few spills), 4 at
+// 64 (no spills); the autotuner picks.
+template <bool HIST, bool BATCH, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB)
 k_force_list(DevParams P0, ListArgs A) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = P0.n;
     uint32_t disp_bits = 0u;
     if (s < n) {
+        // every per-slot load issued up front: they are independent, and the kernel is
+        // bound by their latency when lists are short
         const int scene = BATCH ? A.scene[s] : 0;
-        const DevParams& P = BATCH ? A.scene_params[scene] : P0;
         const float4 pi = A.pos[s];
         const float4 vi = A.vel[s];
         const int id = A.ids[s];
+        const int cnt = A.nbr_cnt[s];
+        const float4 xb = A.xbuild[s];
+        const int hcnt_in = HIST ? A.hcnt_in[s] : 0;
+        const DevParams& P = BATCH ? A.scene_params[scene] : P0;
         if (BATCH && P.frozen) {
             A.pos_out[s] = pi;
             A.vel_out[s] = vi;
@@ -137,7 +144,7 @@ k_force_list(DevParams P0, ListArgs A) {
             HistRow h;
             if (HIST) {
                 h.in = A.hist_in + static_cast<int64_t>(id) * kHistCap;
-                h.in_count = A.hcnt_in[s];
+                h.in_count = hcnt_in;
                 h.out = A.hist_out + static_cast<int64_t>(id) * kHistCap;
                 h.out_count = 0;
             }
@@ -147,7 +154,6 @@ k_force_list(DevParams P0, ListArgs A) {
             const float cut = contact_cutoff_sq(ri, P.rmax);
             int cx, cy, cz;
             cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
-            const int cnt = A.nbr_cnt[s];
             bool ordered = true;
             if (cnt <= kNbrCap) {
                 // the list, in its build order, while the contacts arrive in canonical order
@@ -172,40 +178,39 @@ k_force_list(DevParams P0, ListArgs A) {
                     pair_force<HIST>(P, d, norm, dist, vel, mi, vj, jd, f, h, A.counters);
                 }
                 if (!ordered) {
-                    // a cell crossing re-ordered this grain's contacts: sort, then redo
+                    // a cell crossing re-ordered this grain's contacts: redo them in
+                    // canonical order, each pass taking the smallest key above the last
                     f = f_walls;
                     if (HIST) h.out_count = out_walls;
-                    unsigned long long keys[kNbrCap];
-                    int slots[kNbrCap];
-                    int m = 0;
-                    for (int e = 0; e < cnt; ++e) {
-                        const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
-                        const float4 pj = __ldg(&A.pos[j]);
-                        float3 d;
-                        const float ns = pair_norm_sq(pi, pj, d);
-                        if (ns > cut) continue;
-                        const float dist = pair_dist(sqrtf(ns), ri, pj.w);
-                        if (!(dist < 0.f)) continue;
-                        const unsigned long long key = visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j]));
-                        int q = m++;  // m <= cnt <= kNbrCap
-                        while (q > 0 && keys[q - 1] > key) {
-                            keys[q] = keys[q - 1];
-                            slots[q] = slots[q - 1];
-                            --q;
+                    long long done = -1;
+                    for (;;) {
+                        long long best = 0x7fffffffffffffffll;
+                        int bj = -1;
+                        for (int e = 0; e < cnt; ++e) {
+                            const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+                            const float4 pj = __ldg(&A.pos[j]);
+                            float3 d;
+                            const float ns = pair_norm_sq(pi, pj, d);
+                            if (ns > cut) continue;
+                            const float dist = pair_dist(sqrtf(ns), ri, pj.w);
+                            if (!(dist < 0.f)) continue;
+                            const long long key = static_cast<long long>(
+                                visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j])));
+                            if (key > done && key < best) {
+                                best = key;
+                                bj = j;
+                            }
                         }
-                        keys[q] = key;
-                        slots[q] = j;
-                    }
-                    for (int q = 0; q < m; ++q) {
-                        const int j = slots[q];
-                        const float4 pj = __ldg(&A.pos[j]);
+                        if (bj < 0) break;
+                        done = best;
+                        const float4 pj = __ldg(&A.pos[bj]);
                         float3 d;
                         const float ns = pair_norm_sq(pi, pj, d);
                         const float norm = sqrtf(ns);
                         const float dist = pair_dist(norm, ri, pj.w);
-                        const float4 vj = __ldg(&A.vel[j]);
+                        const float4 vj = __ldg(&A.vel[bj]);
                         pair_force<HIST>(P, d, norm, dist, vel, mi, vj,
-                                         static_cast<int>(keys[q] & 0xffffffffull), f, h, A.counters);
+                                         static_cast<int>(best & 0xffffffffll), f, h, A.counters);
                     }
                 }
             } else {
@@ -243,7 +248,6 @@ k_force_list(DevParams P0, ListArgs A) {
             A.ids_out[s] = id;
             if (BATCH) A.scene_out[s] = scene;
             A.acc_out[s] = make_float4(a.x, a.y, a.z, 0.f);
-            const float4 xb = A.xbuild[s];
             const float ex = x1.x - xb.x, ey = x1.y - xb.y, ez = x1.z - xb.z;
             const float d2 = ex * ex + ey * ey + ez * ez;
             // NaN compares above every float: a diverging grain forces a build
@@ -289,16 +293,23 @@ void launch_list_copy(int n, const float4* pos, const float4* vel, const int* id
                                                   vel_out, ids_out, hcnt_out, scene_out, skip);
 }
 
-void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, int block) {
+template <int MINB>
+void force_list_variant(const DevParams& P, const ListArgs& a, cudaStream_t st, int block) {
     const int nb = blocks_for(P.n, block);
     const bool batch = a.scene_params != nullptr;
     if (P.history) {
-        if (batch) k_force_list<true, true><<<nb, block, 0, st>>>(P, a);
-        else k_force_list<true, false><<<nb, block, 0, st>>>(P, a);
+        if (batch) k_force_list<true, true, MINB><<<nb, block, 0, st>>>(P, a);
+        else k_force_list<true, false, MINB><<<nb, block, 0, st>>>(P, a);
     } else {
-        if (batch) k_force_list<false, true><<<nb, block, 0, st>>>(P, a);
-        else k_force_list<false, false><<<nb, block, 0, st>>>(P, a);
+        if (batch) k_force_list<false, true, MINB><<<nb, block, 0, st>>>(P, a);
+        else k_force_list<false, false, MINB><<<nb, block, 0, st>>>(P, a);
     }
+}
+
+void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, int block,
+                       int min_blocks) {
+    if (min_blocks == 4) force_list_variant<4>(P, a, st, block);
+    else force_list_variant<5>(P, a, st, block);
 }
 
 void launch_list_length(int n, const int* nbr_cnt, unsigned long long* out, cudaStream_t st) {

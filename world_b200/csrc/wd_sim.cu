@@ -139,6 +139,7 @@ struct wd_sim {
     bool lists = false;
     int lpar = 0;
     int force_block = wd::kBlock;   // threads per block of the contact kernel
+    int force_minb = 5;             // register variant of the list contact kernel
     int* nbr = nullptr;
     int* nbr_cnt = nullptr;
     float4* xbuild = nullptr;
@@ -592,7 +593,7 @@ cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool captu
     a.scene_params = batch ? s->d_scene_P : nullptr;
     a.scene = s->sceneA;
     a.scene_out = s->sceneB;
-    wd::launch_force_list(P, a, st, s->force_block);
+    wd::launch_force_list(P, a, st, s->force_block, s->force_minb);
     return cudaGetLastError();
 }
 
@@ -1822,6 +1823,14 @@ cudaError_t run_adj_graph(wd_sim* s, int len, int parity) {
     return cudaGraphLaunch(it->second, s->stream);
 }
 
+int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_get_tuning: NULL handle");
+    if (skin) *skin = sim->cfg.neighbor_skin;
+    if (block) *block = sim->force_block;
+    if (variant) *variant = sim->force_minb == 4 ? 64 : 48;
+    return WD_OK;
+}
+
 int wd_set_neighbor_skin(wd_sim* sim, float skin) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_set_neighbor_skin: NULL handle");
     int rc = sync_stream(sim);
@@ -1835,6 +1844,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
     const std::string key = tune_key(sim);
     float best_skin = sim->cfg.neighbor_skin;
     int best_block = sim->force_block;
+    int best_minb = sim->force_minb;
     bool cached = false;
     if (cache_path) {
         if (std::FILE* f = std::fopen(cache_path, "r")) {
@@ -1842,10 +1852,11 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
             while (std::fgets(line, sizeof(line), f)) {
                 char k[300];
                 float sk = 0.f;
-                int bl = 0;
-                if (std::sscanf(line, "%299s %f %d", k, &sk, &bl) == 3 && key == k) {
+                int bl = 0, mb = 5;
+                if (std::sscanf(line, "%299s %f %d %d", k, &sk, &bl, &mb) >= 3 && key == k) {
                     best_skin = sk;
                     best_block = bl;
+                    best_minb = mb == 4 ? 4 : 5;
                     cached = true;
                 }
             }
@@ -1865,6 +1876,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         if (!sim->picard)
             for (float f : {0.05f, 0.1f, 0.2f, 0.4f}) skins.push_back(f * d);
         const int blocks[] = {128, 256};
+        const int variants[] = {5, 4};
         wd_sim::Snap snap;
         WD_CUDA(alloc_snap(sim, snap));
         WD_CUDA(take_snap(sim, snap));
@@ -1875,10 +1887,14 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         cudaEventCreate(&e1);
         float best_ms = INFINITY;
         for (float sk : skins) {
-            for (int bl : blocks) {
+            for (int cand = 0; cand < 4 && rc == WD_OK; ++cand) {
+                const int bl = blocks[cand & 1];
+                const int mb = variants[cand >> 1];
+                if (sk == 0.f && mb != 5) continue;  // the searched kernel has one variant
                 rc = apply_skin(sim, sk);
                 if (rc == WD_OK) {
                     sim->force_block = bl;
+                    sim->force_minb = mb;
                     sim->graph_dirty = true;
                     const cudaError_t e = put_snap(sim, snap);
                     if (e != cudaSuccess) rc = fail(WD_ERR_CUDA, cudaGetErrorString(e));
@@ -1897,6 +1913,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
                     best_ms = ms;
                     best_skin = sk;
                     best_block = bl;
+                    best_minb = mb;
                 }
             }
             if (rc != WD_OK) break;
@@ -1915,7 +1932,8 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         if (rc) return rc;
         if (cache_path) {
             if (std::FILE* f = std::fopen(cache_path, "a")) {
-                std::fprintf(f, "%s %.9g %d\n", key.c_str(), static_cast<double>(best_skin), best_block);
+                std::fprintf(f, "%s %.9g %d %d\n", key.c_str(), static_cast<double>(best_skin),
+                             best_block, best_minb);
                 std::fclose(f);
             }
         }
@@ -1923,6 +1941,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
     rc = apply_skin(sim, best_skin);
     if (rc) return rc;
     sim->force_block = best_block;
+    sim->force_minb = best_minb;
     sim->graph_dirty = true;
     if (skin_out) *skin_out = best_skin;
     if (block_out) *block_out = best_block;

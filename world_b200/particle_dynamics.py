@@ -340,6 +340,16 @@ class ParticleDynamics:
                               ctypes.byref(sk), ctypes.byref(bl)))
         return float(sk.value), int(bl.value)
 
+    def tuning(self) -> dict:
+        """The current schedule: neighbor skin (m), contact-kernel block size, and the
+        list contact kernel's registers per thread."""
+        sk = ctypes.c_float()
+        bl = ctypes.c_int32()
+        rg = ctypes.c_int32()
+        check(lib.wd_get_tuning(self._h, ctypes.byref(sk), ctypes.byref(bl), ctypes.byref(rg)))
+        return {"neighbor_skin_m": float(sk.value), "contact_block": int(bl.value),
+                "contact_registers": int(rg.value)}
+
     def list_stats(self) -> tuple[int, int, float]:
         """(Verlet-list builds so far, kernels each build launches, mean list length)."""
         b = ctypes.c_int64()
