@@ -189,13 +189,14 @@ def measured_hbm_peak() -> tuple[float, str]:
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(workload: str):
+def profiled_traffic(workload: str, kernel: str):
     """DRAM bytes per contact-kernel launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "contact_kernel_traffic.json")
     try:
         with open(path) as f:
             data = json.load(f)
-        return data.get(workload)
+        entry = data.get(workload)
+        return entry.get(kernel) if isinstance(entry, dict) else None
     except (OSError, ValueError):
         return None
 
@@ -430,8 +431,10 @@ def run_ours(args) -> int:
             "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
             "config": workload_config(scene, args, grains=all_grains, scenes=scenes_total),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": profiled_traffic(args.workload),
-                         "kernel": "k_force (contact forces + integrator)",
+                         "frac": achieved / peak,
+                         "traffic": profiled_traffic(args.workload, "k_force_list" if lists else "k_force"),
+                         "kernel": ("k_force_list (contacts from Verlet lists + integrator)" if lists
+                                    else "k_force (contact forces + integrator)"),
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "algorithmic_bytes_per_launch": contact_bytes,
