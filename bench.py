@@ -202,12 +202,14 @@ def profiled_traffic(workload: str, kernel: str):
 
 
 # ------------------------------------------------------------------ CPU side -----
-def cpu_oracle_rate(scene, seconds: float, max_steps: int, warmup: int = 1):
-    """The oracle port on all host cores: (grain-steps/s, steps, elapsed, threads)."""
+def cpu_oracle_rate(scene, seconds: float, max_steps: int, warmup: int = 1,
+                    threads: int | None = None):
+    """The oracle port on the host cores (all unless `threads`): (grain-steps/s, steps,
+    elapsed, threads)."""
     from oracle.oracle import OracleSim, params_from_config
     from world_b200.state_io import grain_properties
     import numpy as np
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     from oracle.oracle import lib as oracle_lib
     oracle_lib().dem_set_num_threads(threads)
     material = np.full(scene.n, scene.cfg.particle_material, np.int32)
@@ -417,9 +419,12 @@ def run_ours(args) -> int:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, steps, elapsed, threads = cpu_oracle_rate(scene, args.cpu_seconds, 10_000)
+        rate1, steps1, elapsed1, _ = cpu_oracle_rate(scene, max(2.0, args.cpu_seconds / 3), 10_000,
+                                                     warmup=0, threads=1)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{steps} steps of the same {n}-grain workload on {threads} host "
-                         f"threads ({elapsed:.1f} s), oracle/dem_oracle.c with OpenMP"}
+                         f"threads ({elapsed:.1f} s), oracle/dem_oracle.c with OpenMP",
+               "one_core": {"value": rate1, "steps": steps1, "seconds": elapsed1}}
 
     if rank == 0:
         line = {
