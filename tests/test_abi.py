@@ -115,5 +115,6 @@ def test_batch_entry_points_take_the_python_argument_forms():
         lib.wd_get_positions_async(None, ptr(d)),
         lib.wd_io_join(None),
         lib.wd_get_tuning(None, None, None, None),
+        lib.wd_set_contact_kernel(None, 256, 0),
     ]
     assert all(c == -1 for c in calls), calls

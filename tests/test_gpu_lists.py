@@ -160,3 +160,57 @@ def test_autotune_restores_the_state_and_caches(tmp_path):
     other = ParticleDynamics(sc.cfg, state=sc.state, radius=sc.radius)
     assert other.autotune(steps=20, cache=str(cache)) == (np.float32(skin), block)
     assert len(cache.read_text().splitlines()) == 1
+
+
+@pytest.mark.parametrize("variant,block", [(0, 256), (64, 128), (48, 64)])
+def test_every_contact_kernel_variant_is_exact(variant, block):
+    cfg, st, rad = packed_poly(n=2500, seed=28, mu=0.5)
+    cfg.kernel_timing = False
+    ref = ParticleDynamics(cfg, state=st, radius=rad)
+    c = cfg.copy()
+    c.neighbor_skin = 0.5e-3
+    var = ParticleDynamics(c, state=st, radius=rad)
+    var.set_contact_kernel(block, variant)
+    ref.advance(150)
+    var.advance(150)
+    _same(ref, var)
+    # viscous friction (no springs) and a batch through the same kernel
+    cfg2, st2, rad2 = packed_poly(n=1500, seed=29, mu=0.5, history=False)
+    cfg2.kernel_timing = False
+    ref2 = ParticleDynamics(cfg2, state=st2, radius=rad2)
+    c2 = cfg2.copy()
+    c2.neighbor_skin = 0.5e-3
+    var2 = ParticleDynamics(c2, state=st2, radius=rad2)
+    var2.set_contact_kernel(block, variant)
+    ref2.advance(120)
+    var2.advance(120)
+    _same(ref2, var2)
+    sb = []
+    for skin in (0.0, 0.5e-3):
+        cfgs = []
+        for cc in (cfg, cfg2.copy()):
+            x = cc.copy()
+            x.history = True
+            x.neighbor_skin = skin
+            cfgs.append(x)
+        b = SceneBatch(cfgs, [st, st2], radii=[rad, rad2])
+        if skin:
+            b.set_contact_kernel(block, variant)
+        b.advance(100)
+        sb.append(b)
+    _same(*sb)
+
+
+def test_dense_contacts_cooperative_kernel_matches_oracle():
+    """Many contacts per warp (several queue flushes) through the cooperative kernel."""
+    cfg, st, rad = packed_poly(n=3000, seed=30, mu=0.6)
+    cfg.neighbor_skin = 0.3e-3
+    cfg.kernel_timing = False
+    cfg.physics.max_force = 50.0      # clamped contacts too
+    _, mass = grain_properties(cfg, np.full(st.shape[0], cfg.particle_material, np.int32), rad)
+    sim = ParticleDynamics(cfg, state=st, radius=rad)
+    sim.set_contact_kernel(256, 0)
+    ref = OracleSim(params_from_config(cfg), st, rad, mass)
+    sim.advance(60)
+    ref.step(60)
+    np.testing.assert_array_equal(sim.get_state(), ref.state)

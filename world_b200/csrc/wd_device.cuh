@@ -95,17 +95,23 @@ __device__ __forceinline__ float damping(const DevParams& P, float m) {
     return ((-2.f * sqrtf(m * P.k_n)) * P.ln_e) / P.damp_den;
 }
 
-// reference src/compute_rhs_kernel.cu:66-78
-__device__ __forceinline__ void viscous_friction(float3& f, float3 vt, float limit, float c) {
+// reference src/compute_rhs_kernel.cu:66-78: the friction force is -term (zero below
+// the 1e-8 m/s cutoff; f - 0 is f exactly).
+__device__ __forceinline__ float3 viscous_term(float3 vt, float limit, float c) {
     float vt_sq = vt.x * vt.x;
     vt_sq = fmaf(vt.y, vt.y, vt_sq);
     vt_sq = fmaf(vt.z, vt.z, vt_sq);
     const float v = sqrtf(vt_sq);
-    if (v < 1e-8f) return;
+    if (v < 1e-8f) return make_float3(0.f, 0.f, 0.f);
     const float mag = fminf(limit, c * v);
-    f.x = f.x - (mag * vt.x) / v;
-    f.y = f.y - (mag * vt.y) / v;
-    f.z = f.z - (mag * vt.z) / v;
+    return make_float3((mag * vt.x) / v, (mag * vt.y) / v, (mag * vt.z) / v);
+}
+
+__device__ __forceinline__ void viscous_friction(float3& f, float3 vt, float limit, float c) {
+    const float3 t = viscous_term(vt, limit, c);
+    f.x = f.x - t.x;
+    f.y = f.y - t.y;
+    f.z = f.z - t.z;
 }
 
 // Tangential spring with per-pair history (Cundall-Strack), capped at mu |F_n| with
@@ -119,17 +125,19 @@ struct HistRow {
     int out_count;
 };
 
-__device__ __forceinline__ void spring_friction(const DevParams& P, float3& f, float3 vt,
-                                                float3 nrm, float limit, int partner,
-                                                HistRow& h, unsigned long long* counters) {
-    float3 xi = make_float3(0.f, 0.f, 0.f);
-    for (int k = 0; k < h.in_count; ++k) {
-        const float4 e = h.in[k];
-        if (__float_as_int(e.w) == partner) {
-            xi = make_float3(e.x, e.y, e.z);
-            break;
-        }
+// Stored spring of `partner` in a row (zero if the contact is new).
+__device__ __forceinline__ float3 find_spring(const float4* row, int count, int partner) {
+    for (int k = 0; k < count; ++k) {
+        const float4 e = row[k];
+        if (__float_as_int(e.w) == partner) return make_float3(e.x, e.y, e.z);
     }
+    return make_float3(0.f, 0.f, 0.f);
+}
+
+// The spring's step: rotate onto the tangent plane, advance by v_t dt, cap at `limit`.
+// Returns the tangential force; xi becomes the new spring.
+__device__ __forceinline__ float3 spring_step(const DevParams& P, float3 vt, float3 nrm,
+                                              float limit, float3& xi) {
     float xn = xi.x * nrm.x;
     xn = fmaf(xi.y, nrm.y, xn);
     xn = fmaf(xi.z, nrm.z, xn);
@@ -148,6 +156,14 @@ __device__ __forceinline__ void spring_friction(const DevParams& P, float3& f, f
         ft.x = ft.x * s; ft.y = ft.y * s; ft.z = ft.z * s;
         xi.x = xi.x * s; xi.y = xi.y * s; xi.z = xi.z * s;
     }
+    return ft;
+}
+
+__device__ __forceinline__ void spring_friction(const DevParams& P, float3& f, float3 vt,
+                                                float3 nrm, float limit, int partner,
+                                                HistRow& h, unsigned long long* counters) {
+    float3 xi = find_spring(h.in, h.in_count, partner);
+    const float3 ft = spring_step(P, vt, nrm, limit, xi);
     f.x = f.x + ft.x;
     f.y = f.y + ft.y;
     f.z = f.z + ft.z;
@@ -237,35 +253,75 @@ __device__ __forceinline__ float contact_cutoff_sq(float ri, float rmax) {
     return rs * rs * 1.001f;
 }
 
-// One pair contact: reference src/compute_rhs_kernel.cu:150-204 (dist < 0 branch).
+// One pair contact's quantities (reference src/compute_rhs_kernel.cu:150-204, dist < 0
+// branch): the normal force fp along nrm, the dashpot term cvn, and the friction t
+// (the spring's force, added, in history mode; the viscous term, subtracted,
+// otherwise). With springs, xi enters as the stored spring and leaves as the new one.
+struct PairTerms {
+    float fp, cvn;
+    float3 nrm, t;
+};
+
 template <bool HIST>
-__device__ __forceinline__ void pair_force(const DevParams& P, float3 d, float norm,
-                                           float dist, float3 vel, float mi, float4 vj,
-                                           int partner, float3& f, HistRow& h,
-                                           unsigned long long* counters) {
-    const float3 nrm = make_float3(d.x / norm, d.y / norm, d.z / norm);
-    const float fp = fmaxf(0.f, fminf(P.max_force, -P.k_n * dist));
-    f.x = fmaf(fp, nrm.x, f.x);
-    f.y = fmaf(fp, nrm.y, f.y);
-    f.z = fmaf(fp, nrm.z, f.z);
+__device__ __forceinline__ PairTerms pair_terms(const DevParams& P, float3 d, float norm,
+                                                float dist, float3 vel, float mi, float4 vj,
+                                                float3& xi) {
+    PairTerms q;
+    q.nrm = make_float3(d.x / norm, d.y / norm, d.z / norm);
+    q.fp = fmaxf(0.f, fminf(P.max_force, -P.k_n * dist));
     const float mj = vj.w;
     const float msum = mi + mj;
     const float mred = (msum > 0.f) ? (mi * mj) / msum : 0.f;
     const float c = damping(P, mred);
     const float3 vr = make_float3(vel.x - vj.x, vel.y - vj.y, vel.z - vj.z);
-    float vn = vr.x * nrm.x;
-    vn = fmaf(vr.y, nrm.y, vn);
-    vn = fmaf(vr.z, nrm.z, vn);
-    const float cvn = c * vn;
-    f.x = fmaf(-cvn, nrm.x, f.x);
-    f.y = fmaf(-cvn, nrm.y, f.y);
-    f.z = fmaf(-cvn, nrm.z, f.z);
-    const float3 vt = make_float3(fmaf(-vn, nrm.x, vr.x), fmaf(-vn, nrm.y, vr.y),
-                                  fmaf(-vn, nrm.z, vr.z));
+    float vn = vr.x * q.nrm.x;
+    vn = fmaf(vr.y, q.nrm.y, vn);
+    vn = fmaf(vr.z, q.nrm.z, vn);
+    q.cvn = c * vn;
+    const float3 vt = make_float3(fmaf(-vn, q.nrm.x, vr.x), fmaf(-vn, q.nrm.y, vr.y),
+                                  fmaf(-vn, q.nrm.z, vr.z));
+    const float limit = P.mu * q.fp;
+    q.t = HIST ? spring_step(P, vt, q.nrm, limit, xi) : viscous_term(vt, limit, c);
+    return q;
+}
+
+// The contact's share of the grain's force, in the reference's order: normal force,
+// dashpot, friction.
+template <bool HIST>
+__device__ __forceinline__ void pair_accumulate(float3& f, const PairTerms& q) {
+    f.x = fmaf(q.fp, q.nrm.x, f.x);
+    f.y = fmaf(q.fp, q.nrm.y, f.y);
+    f.z = fmaf(q.fp, q.nrm.z, f.z);
+    f.x = fmaf(-q.cvn, q.nrm.x, f.x);
+    f.y = fmaf(-q.cvn, q.nrm.y, f.y);
+    f.z = fmaf(-q.cvn, q.nrm.z, f.z);
     if (HIST) {
-        spring_friction(P, f, vt, nrm, P.mu * fp, partner, h, counters);
+        f.x = f.x + q.t.x;
+        f.y = f.y + q.t.y;
+        f.z = f.z + q.t.z;
     } else {
-        viscous_friction(f, vt, P.mu * fp, c);
+        f.x = f.x - q.t.x;
+        f.y = f.y - q.t.y;
+        f.z = f.z - q.t.z;
+    }
+}
+
+// One pair contact accumulated into f, its spring read from and written to h.
+template <bool HIST>
+__device__ __forceinline__ void pair_force(const DevParams& P, float3 d, float norm,
+                                           float dist, float3 vel, float mi, float4 vj,
+                                           int partner, float3& f, HistRow& h,
+                                           unsigned long long* counters) {
+    float3 xi = HIST ? find_spring(h.in, h.in_count, partner) : make_float3(0.f, 0.f, 0.f);
+    const PairTerms q = pair_terms<HIST>(P, d, norm, dist, vel, mi, vj, xi);
+    pair_accumulate<HIST>(f, q);
+    if (HIST) {
+        if (h.out_count < kHistCap) {
+            h.out[h.out_count] = make_float4(xi.x, xi.y, xi.z, __int_as_float(partner));
+            ++h.out_count;
+        } else {
+            atomicAdd(&counters[kCntHistOverflow], 1ull);
+        }
     }
 }
 

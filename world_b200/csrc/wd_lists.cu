@@ -259,6 +259,252 @@ k_force_list(DevParams P0, ListArgs A) {
     if ((threadIdx.x & 31) == 0 && disp_bits != 0u) atomicMax(&A.list_ctrl[kLcDisp], disp_bits);
 }
 
+// Warp-cooperative variant: a contact's work (spring lookup, Coulomb cap, dashpot) is
+// spread over the lanes of the warp instead of running on its grain's lane alone, then
+// every grain accumulates its contacts' terms in order. The per-lane kernel above
+// spends most issue slots on one or two active lanes when contacts are sparse.
+//
+// Per warp: rounds over the list entries (e = 0, 1, ...) find the contacts of the 32
+// grains and queue them (partner slot, owner lane, owner's contact rank); a full queue
+// (kCoopCap) or the last round flushes it: the lanes compute the queued contacts' terms
+// (pair_terms, the springs written to their final rows), each grain's terms land in
+// its own run of the buffer, and each lane accumulates its run in order. Contacts are
+// found in list order, which is the canonical order unless a cell crossing changed it;
+// such a grain redoes its contacts in canonical order on its own lane at the end.
+constexpr int kCoopWarps = kBlock / 32;
+constexpr int kCoopCap = 64;
+
+struct CoopWarp {
+    int qj[kCoopCap];
+    unsigned char qg[kCoopCap];
+    unsigned char qr[kCoopCap];
+    PairTerms terms[kCoopCap];
+    float4 pos[32], vel[32];
+    int id[32], hin[32], outw[32], first[32], off[32], scene[32];
+};
+
+template <bool HIST, bool BATCH>
+__device__ __forceinline__ void coop_flush(const DevParams& P0, const ListArgs& A, CoopWarp& W,
+                                           int q, int lane, int my_count, int& bstart,
+                                           bool reorder, float3& f) {
+    __syncwarp();
+    const int c = my_count - bstart;
+    int off = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, off, o);
+        if (lane >= o) off += y;
+    }
+    off -= c;
+    W.first[lane] = bstart;
+    W.off[lane] = off;
+    __syncwarp();
+    for (int i = lane; i < q; i += 32) {
+        const int j = W.qj[i];
+        const int g = W.qg[i];
+        const int r = W.qr[i];
+        const DevParams& P = BATCH ? A.scene_params[W.scene[g]] : P0;
+        const float4 pi = W.pos[g], vi = W.vel[g];
+        const float4 pj = __ldg(&A.pos[j]);
+        const float4 vj = __ldg(&A.vel[j]);
+        const int jd = __ldg(&A.ids[j]);
+        float3 d;
+        const float ns = pair_norm_sq(pi, pj, d);
+        const float norm = sqrtf(ns);
+        const float dist = pair_dist(norm, pi.w, pj.w);
+        const int gid = W.id[g];
+        float3 xi = HIST ? find_spring(A.hist_in + static_cast<int64_t>(gid) * kHistCap, W.hin[g], jd)
+                         : make_float3(0.f, 0.f, 0.f);
+        W.terms[W.off[g] + (r - W.first[g])] =
+            pair_terms<HIST>(P, d, norm, dist, make_float3(vi.x, vi.y, vi.z), vi.w, vj, xi);
+        if (HIST) {
+            const int slot = W.outw[g] + r;
+            if (slot < kHistCap)
+                A.hist_out[static_cast<int64_t>(gid) * kHistCap + slot] =
+                    make_float4(xi.x, xi.y, xi.z, __int_as_float(jd));
+        }
+    }
+    __syncwarp();
+    if (!reorder)
+        for (int k = 0; k < c; ++k) pair_accumulate<HIST>(f, W.terms[off + k]);
+    __syncwarp();
+    bstart = my_count;
+}
+
+template <bool HIST, bool BATCH>
+__global__ void __launch_bounds__(kBlock, 4)
+k_force_list_coop(DevParams P0, ListArgs A) {
+    __shared__ CoopWarp warps[kCoopWarps];
+    const int lane = threadIdx.x & 31;
+    CoopWarp& W = warps[threadIdx.x >> 5];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = P0.n;
+    const bool active = s < n;
+    // per-slot loads, up front
+    const int scene = (BATCH && active) ? A.scene[s] : 0;
+    const float4 pi = active ? A.pos[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 vi = active ? A.vel[s] : make_float4(0.f, 0.f, 0.f, 1.f);
+    const int id = active ? A.ids[s] : 0;
+    const int cnt_raw = active ? A.nbr_cnt[s] : 0;
+    const float4 xb = active ? A.xbuild[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int hcnt_in = (HIST && active) ? A.hcnt_in[s] : 0;
+    const DevParams& P = BATCH ? A.scene_params[scene] : P0;
+    const bool frozen = BATCH && active && P.frozen;
+    const bool work = active && !frozen;
+    const float3 pos = make_float3(pi.x, pi.y, pi.z);
+    const float3 vel = make_float3(vi.x, vi.y, vi.z);
+    const float ri = pi.w, mi = vi.w;
+    float3 f = make_float3(0.f, 0.f, 0.f);
+    HistRow h;
+    h.in = A.hist_in + static_cast<int64_t>(id) * kHistCap;
+    h.in_count = hcnt_in;
+    h.out = A.hist_out + static_cast<int64_t>(id) * kHistCap;
+    h.out_count = 0;
+    if (work) wall_forces<HIST>(P, pos, vel, ri, mi, f, h, A.counters);
+    const float3 f_walls = f;
+    const int out_walls = HIST ? h.out_count : 0;
+    W.pos[lane] = pi;
+    W.vel[lane] = vi;
+    W.id[lane] = id;
+    W.hin[lane] = hcnt_in;
+    W.outw[lane] = out_walls;
+    W.scene[lane] = scene;
+    const float cut = contact_cutoff_sq(ri, P.rmax);
+    int cx = 0, cy = 0, cz = 0;
+    if (work) cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+    const bool listed = work && cnt_raw <= kNbrCap;
+    const int cnt = listed ? cnt_raw : 0;
+    const int rounds = __reduce_max_sync(0xffffffffu, cnt);
+    int q = 0, my_count = 0, bstart = 0;
+    bool reorder = false;
+    unsigned long long last = 0ull;
+    for (int e = 0; e < rounds; ++e) {
+        bool hit = false;
+        int j = 0;
+        if (e < cnt) {
+            j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+            const float4 pj = __ldg(&A.pos[j]);
+            float3 d;
+            const float ns = pair_norm_sq(pi, pj, d);
+            if (!(ns > cut)) {
+                const float dist = pair_dist(sqrtf(ns), ri, pj.w);
+                if (dist < 0.f) {
+                    hit = true;
+                    const unsigned long long key = visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j]));
+                    if (key < last) reorder = true;
+                    last = key;
+                }
+            }
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, hit);
+        const int add = __popc(b);
+        if (q + add > kCoopCap) {
+            coop_flush<HIST, BATCH>(P0, A, W, q, lane, my_count, bstart, reorder, f);
+            q = 0;
+        }
+        if (hit) {
+            const int at = q + __popc(b & ((1u << lane) - 1u));
+            W.qj[at] = j;
+            W.qg[at] = static_cast<unsigned char>(lane);
+            W.qr[at] = static_cast<unsigned char>(my_count);
+            ++my_count;
+        }
+        q += add;
+    }
+    if (rounds > 0) coop_flush<HIST, BATCH>(P0, A, W, q, lane, my_count, bstart, reorder, f);
+    uint32_t disp_bits = 0u;
+    if (work) {
+        if (!listed) {
+            // list overflow: this step built the lists, so the run table is fresh
+            h.out_count = out_walls;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int nx = cx + dx;
+                if (nx < 0 || nx >= P.grid[0]) continue;
+                int lo[3], hi[3];
+                row_ranges(P, A.table, nx, cy, cz, lo, hi);
+                for (int t = 0; t < 3; ++t) {
+                    for (int j = lo[t]; j < hi[t]; ++j) {
+                        const float4 pj = __ldg(&A.pos[j]);
+                        float3 d;
+                        const float ns = pair_norm_sq(pi, pj, d);
+                        if (ns > cut || j == s) continue;
+                        const float norm = sqrtf(ns);
+                        const float dist = pair_dist(norm, ri, pj.w);
+                        if (!(dist < 0.f)) continue;
+                        const float4 vj = __ldg(&A.vel[j]);
+                        const int partner = HIST ? __ldg(&A.ids[j]) : 0;
+                        pair_force<HIST>(P, d, norm, dist, vel, mi, vj, partner, f, h, A.counters);
+                    }
+                }
+            }
+        } else if (reorder) {
+            // a cell crossing re-ordered this grain's contacts: redo them in canonical
+            // order, each pass taking the smallest key above the last
+            f = f_walls;
+            h.out_count = out_walls;
+            long long done = -1;
+            for (;;) {
+                long long best = 0x7fffffffffffffffll;
+                int bj = -1;
+                for (int e = 0; e < cnt; ++e) {
+                    const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+                    const float4 pj = __ldg(&A.pos[j]);
+                    float3 d;
+                    const float ns = pair_norm_sq(pi, pj, d);
+                    if (ns > cut) continue;
+                    const float dist = pair_dist(sqrtf(ns), ri, pj.w);
+                    if (!(dist < 0.f)) continue;
+                    const long long key =
+                        static_cast<long long>(visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j])));
+                    if (key > done && key < best) {
+                        best = key;
+                        bj = j;
+                    }
+                }
+                if (bj < 0) break;
+                done = best;
+                const float4 pj = __ldg(&A.pos[bj]);
+                float3 d;
+                const float ns = pair_norm_sq(pi, pj, d);
+                const float norm = sqrtf(ns);
+                const float dist = pair_dist(norm, ri, pj.w);
+                const float4 vj = __ldg(&A.vel[bj]);
+                pair_force<HIST>(P, d, norm, dist, vel, mi, vj,
+                                 static_cast<int>(best & 0xffffffffll), f, h, A.counters);
+            }
+        } else if (HIST) {
+            h.out_count = min(out_walls + my_count, kHistCap);
+            if (out_walls + my_count > kHistCap)
+                atomicAdd(&A.counters[kCntHistOverflow],
+                          static_cast<unsigned long long>(out_walls + my_count - kHistCap));
+        }
+        if (HIST) A.hcnt_out[s] = h.out_count;
+        const float3 a = make_float3(f.x / mi, f.y / mi, f.z / mi);
+        const float3 v1 = make_float3(fmaf(P.dt, a.x, vel.x), fmaf(P.dt, a.y, vel.y),
+                                      fmaf(P.dt, a.z, vel.z));
+        const float3 x1 = make_float3(fmaf(P.dt, v1.x, pos.x), fmaf(P.dt, v1.y, pos.y),
+                                      fmaf(P.dt, v1.z, pos.z));
+        A.pos_out[s] = make_float4(x1.x, x1.y, x1.z, ri);
+        A.vel_out[s] = make_float4(v1.x, v1.y, v1.z, mi);
+        A.ids_out[s] = id;
+        if (BATCH) A.scene_out[s] = scene;
+        A.acc_out[s] = make_float4(a.x, a.y, a.z, 0.f);
+        const float ex = x1.x - xb.x, ey = x1.y - xb.y, ez = x1.z - xb.z;
+        const float d2 = ex * ex + ey * ey + ez * ez;
+        disp_bits = d2 >= 0.f ? __float_as_uint(d2) : 0x7f800000u;
+    } else if (frozen) {
+        A.pos_out[s] = pi;
+        A.vel_out[s] = vi;
+        A.ids_out[s] = id;
+        A.scene_out[s] = scene;
+        A.acc_out[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (HIST) A.hcnt_out[s] = 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) disp_bits = max(disp_bits, __shfl_xor_sync(0xffffffffu, disp_bits, o));
+    if (lane == 0 && disp_bits != 0u) atomicMax(&A.list_ctrl[kLcDisp], disp_bits);
+}
+
 __global__ void __launch_bounds__(kBlock)
 k_list_length(int n, const int* __restrict__ cnt, unsigned long long* __restrict__ out) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -308,8 +554,22 @@ void force_list_variant(const DevParams& P, const ListArgs& a, cudaStream_t st, 
 
 void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, int block,
                        int min_blocks) {
-    if (min_blocks == 4) force_list_variant<4>(P, a, st, block);
-    else force_list_variant<5>(P, a, st, block);
+    if (min_blocks == 0) {
+        // warp-cooperative kernel: its shared queues are sized for kBlock threads
+        const int nb = blocks_for(P.n, kBlock);
+        const bool batch = a.scene_params != nullptr;
+        if (P.history) {
+            if (batch) k_force_list_coop<true, true><<<nb, kBlock, 0, st>>>(P, a);
+            else k_force_list_coop<true, false><<<nb, kBlock, 0, st>>>(P, a);
+        } else {
+            if (batch) k_force_list_coop<false, true><<<nb, kBlock, 0, st>>>(P, a);
+            else k_force_list_coop<false, false><<<nb, kBlock, 0, st>>>(P, a);
+        }
+    } else if (min_blocks == 4) {
+        force_list_variant<4>(P, a, st, block);
+    } else {
+        force_list_variant<5>(P, a, st, block);
+    }
 }
 
 void launch_list_length(int n, const int* nbr_cnt, unsigned long long* out, cudaStream_t st) {

@@ -1826,8 +1826,23 @@ cudaError_t run_adj_graph(wd_sim* s, int len, int parity) {
 int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_get_tuning: NULL handle");
     if (skin) *skin = sim->cfg.neighbor_skin;
-    if (block) *block = sim->force_block;
-    if (variant) *variant = sim->force_minb == 4 ? 64 : 48;
+    if (block) *block = sim->force_minb == 0 ? wd::kBlock : sim->force_block;
+    if (variant) *variant = sim->force_minb == 0 ? 0 : (sim->force_minb == 4 ? 64 : 48);
+    return WD_OK;
+}
+
+int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_set_contact_kernel: NULL handle");
+    if (block < 32 || block > wd::kBlock || block % 32)
+        return fail(WD_ERR_INVALID, "wd_set_contact_kernel: block must be a multiple of 32 up to 256");
+    if (variant != 48 && variant != 64 && variant != 0)
+        return fail(WD_ERR_INVALID, "wd_set_contact_kernel: variant must be 48, 64 or 0");
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    sim->force_block = block;
+    sim->force_minb = variant == 0 ? 0 : (variant == 64 ? 4 : 5);
+    sim->graph_dirty = true;
+    clear_adj_graphs(sim);
     return WD_OK;
 }
 
@@ -1856,7 +1871,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
                 if (std::sscanf(line, "%299s %f %d %d", k, &sk, &bl, &mb) >= 3 && key == k) {
                     best_skin = sk;
                     best_block = bl;
-                    best_minb = mb == 4 ? 4 : 5;
+                    best_minb = (mb == 4 || mb == 0) ? mb : 5;
                     cached = true;
                 }
             }
@@ -1875,8 +1890,9 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         std::vector<float> skins = {0.f};
         if (!sim->picard)
             for (float f : {0.05f, 0.1f, 0.2f, 0.4f}) skins.push_back(f * d);
-        const int blocks[] = {128, 256};
-        const int variants[] = {5, 4};
+        // (block, variant): variant 5 / 4 = per-lane list kernel with 48 / 64 registers,
+        // 0 = warp-cooperative list kernel (256 threads)
+        const int cands[][2] = {{128, 5}, {256, 5}, {128, 4}, {256, 4}, {256, 0}};
         wd_sim::Snap snap;
         WD_CUDA(alloc_snap(sim, snap));
         WD_CUDA(take_snap(sim, snap));
@@ -1887,9 +1903,9 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         cudaEventCreate(&e1);
         float best_ms = INFINITY;
         for (float sk : skins) {
-            for (int cand = 0; cand < 4 && rc == WD_OK; ++cand) {
-                const int bl = blocks[cand & 1];
-                const int mb = variants[cand >> 1];
+            for (int cand = 0; cand < 5 && rc == WD_OK; ++cand) {
+                const int bl = cands[cand][0];
+                const int mb = cands[cand][1];
                 if (sk == 0.f && mb != 5) continue;  // the searched kernel has one variant
                 rc = apply_skin(sim, sk);
                 if (rc == WD_OK) {
