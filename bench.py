@@ -451,7 +451,8 @@ def run_ours(args) -> int:
             "gpu_launches": launches,
             "radix_searches_timed": radix_searches,
             "neighbor_lists": {"skin_m": scene.cfg.neighbor_skin, "builds_timed": builds,
-                               "mean_list_length": mean_list} if lists else None,
+                               "mean_list_length": mean_list,
+                               "picard_redos": sim.picard_redo_count()} if lists else None,
             "history_entries_per_grain": entries / n,
             "scene_results": scene_results,
             "autotuned": tuned,

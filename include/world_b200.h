@@ -264,7 +264,7 @@ int wd_compute_max_acceleration(wd_sim* sim, float* max_accel);
  * grain is dropped here: the sorted search has no per-cell capacity. */
 int wd_grid_overflow_count(wd_sim* sim, int64_t* count);
 /* Switch the Verlet-list skin of a live handle (0: grid search every step). The
- * trajectory does not depend on it. Semi-implicit Euler only for a skin > 0. */
+ * trajectory does not depend on it. */
 int wd_set_neighbor_skin(wd_sim* sim, float skin);
 /* Autotuner (extension): times `steps` steps for each neighbor skin in {0, 0.05,
  * 0.1, 0.2, 0.4} mean diameters, contact-kernel block size in {128, 256} and, with
@@ -282,6 +282,9 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
  * (the autotuner's other choices); results do not depend on them. */
 int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant);
 int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant);
+/* Backward Euler / Picard on Verlet lists: steps so far that an iterate took beyond
+ * the lists' validity bound and that were redone with the per-iteration search. */
+int wd_picard_redo_count(wd_sim* sim, int64_t* redos);
 /* Verlet lists (simulation.neighbor_skin > 0): builds so far, kernels one build
  * launches, and the mean list length of the last build (0 without lists). */
 int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length);

@@ -214,3 +214,42 @@ def test_dense_contacts_cooperative_kernel_matches_oracle():
     sim.advance(60)
     ref.step(60)
     np.testing.assert_array_equal(sim.get_state(), ref.state)
+
+
+@pytest.mark.parametrize("timing", [False, True])
+def test_picard_on_lists_equals_picard_with_search(timing):
+    # tolerance-terminated iterations with springs
+    cfg, st, rad = packed_poly(n=2500, seed=31, mu=0.5, picard=True, tol=1e-9)
+    ref, lst = _pair(cfg, st, rad, 80, 0.5e-3, timing)
+    _same(ref, lst)
+    assert ref.picard_stats() == lst.picard_stats()
+    # fixed iteration count, viscous friction
+    cfg2, st2, rad2 = packed_poly(n=2000, seed=32, mu=0.4, history=False, picard=True, tol=0.0)
+    ref2, lst2 = _pair(cfg2, st2, rad2, 60, 0.5e-3, timing)
+    _same(ref2, lst2)
+
+
+def test_picard_redo_when_iterates_leave_the_lists():
+    """A skin so small that iterates leave it every step: each step is redone with the
+    per-iteration search, and the results stay exact."""
+    cfg, st, rad = packed_poly(n=1500, seed=33, mu=0.5, picard=True, tol=1e-9)
+    cfg.kernel_timing = False
+    ref, lst = _pair(cfg, st, rad, 40, 1e-9)
+    _same(ref, lst)
+    assert lst.picard_redo_count() > 0 and ref.picard_redo_count() == 0
+
+
+def test_batched_picard_on_lists():
+    scenes = [packed_poly(n=1200, seed=s, mu=0.4, picard=True, tol=0.0) for s in (34, 35)]
+    sims = []
+    for skin in (0.0, 0.5e-3):
+        cfgs = []
+        for c in (scenes[0][0], scenes[1][0]):
+            cc = c.copy()
+            cc.neighbor_skin = skin
+            cc.kernel_timing = False
+            cfgs.append(cc)
+        b = SceneBatch(cfgs, [sc[1] for sc in scenes], radii=[sc[2] for sc in scenes])
+        b.advance(50)
+        sims.append(b)
+    _same(*sims)

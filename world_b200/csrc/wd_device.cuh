@@ -24,6 +24,7 @@ enum Counter : int {
     kCntMaxAccel = 3,       // scratch for compute_max_acceleration (float bits)
     kCntRadixSearches = 4,  // searches that took the full radix-sort path
     kCntListBuilds = 5,     // Verlet-list builds
+    kCntPicardRedos = 6,    // list-mode Picard steps redone with the per-iteration search
     kNumCounters = 8,
 };
 

@@ -130,7 +130,12 @@ void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip
 // Verlet lists (simulation.neighbor_skin > 0, semi-implicit Euler). list_ctrl words:
 // [0] max |x - x_build|^2 since the build (float bits), [1] a list overflowed,
 // [2] rebuild requested by the host, [3] this step's decision (1.0f: rebuild).
-enum ListCtrl { kLcDisp = 0, kLcOverflow = 1, kLcForce = 2, kLcDecision = 3, kLcWords = 4 };
+// Picard: [4] an iteration started from an iterate 0.45 skin or more from its build
+// position, [5] this step's redo decision (1.0f: redo with the per-iteration search).
+enum ListCtrl {
+    kLcDisp = 0, kLcOverflow = 1, kLcForce = 2, kLcDecision = 3, kLcViol = 4, kLcRedo = 5,
+    kLcWords = 6
+};
 struct ListArgs {
     const float4* pos; const float4* vel; const int* ids;  // state of the step
     const int2* table;                                     // fresh only at a build
@@ -141,6 +146,13 @@ struct ListArgs {
     const int* nbr; const int* nbr_cnt; const float4* xbuild;
     uint32_t* list_ctrl;
     const DevParams* scene_params; const int* scene; int* scene_out;
+    // backward Euler / Picard: the step-start state, the iteration's residual slot,
+    // the iteration counter, the list-validity bound on the iterate, the convergence skip
+    const float4* xn; const float4* vn;
+    uint32_t* res_slot; int* picard_used; int iter;
+    float viol_thr;
+    Skip skip;
+    float4* rhs_vel; int* rhs_ids;    // the iterate's velocity and ids, for the rhs getter
 };
 void launch_list_decide(uint32_t* list_ctrl, float thr_sq, unsigned long long* counters,
                         bool use_cond, cudaGraphConditionalHandle cond, cudaStream_t st);
@@ -152,7 +164,13 @@ void launch_list_copy(int n, const float4* pos, const float4* vel, const int* id
                       int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st);
 // min_blocks: the register variant (5: 48 registers, 4: 64 registers per thread)
 void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st,
-                       int block = kBlock, int min_blocks = 5);
+                       int block = kBlock, int min_blocks = 5, bool picard = false);
+// Picard with lists: the last iterate into the B buffers when the last executed
+// iteration wrote the scratch ones; then the redo decision.
+void launch_list_finalize(int n, const int* picard_used, const float4* xpos,
+                          const float4* xvel, float4* pos, float4* vel, cudaStream_t st);
+void launch_list_picard_check(uint32_t* list_ctrl, unsigned long long* counters, bool use_cond,
+                              cudaGraphConditionalHandle cond, cudaStream_t st);
 void launch_list_length(int n, const int* nbr_cnt, unsigned long long* out, cudaStream_t st);
 
 // Total energy per scene at the sorted state (after a search): per-grain FP64 sums,

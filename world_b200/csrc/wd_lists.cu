@@ -1,4 +1,5 @@
-// wd_lists.cu -- Verlet neighbor lists for the semi-implicit Euler step.
+// wd_lists.cu -- Verlet neighbor lists for the semi-implicit Euler and the backward
+// Euler / Picard steps.
 //
 // The reference searches the grid every step (src/particle_dynamics.cu:264-281). With
 // simulation.neighbor_skin = s > 0 the search runs only when needed: a build sorts the
@@ -16,6 +17,11 @@
 //
 // Between builds the state stays in one order and ping-pongs between two buffers; a
 // build gathers it into the new order, lists the neighbors, and copies it back.
+//
+// Picard iterates every force evaluation of a step on the same lists. Builds start at
+// 0.30 skin instead of 0.45, and each iteration checks that its input iterate is still
+// within 0.45 skin of the build; if one is not, the step is redone from its start
+// state with the per-iteration search, so the results stay those of the searched step.
 #include "wd_kernels.h"
 
 namespace wd {
@@ -112,12 +118,19 @@ __device__ __forceinline__ unsigned long long visit_key(const DevParams& P, int 
 
 // MINB resident blocks per SM: 5 caps registers at 48 (more warps, a few spills), 4 at
 // 64 (no spills); the autotuner picks.
-template <bool HIST, bool BATCH, int MINB>
+// PICARD: one backward-Euler / Picard iteration (src/backward_euler_picard_kernel.cu:4-17):
+// forces at the iterate (pos, vel), integration from the step-start state (xn, vn), the
+// residual max |x_{k+1} - x_k|; an iterate that has left the lists' validity bound marks
+// the step for a redo.
+template <bool HIST, bool BATCH, int MINB, bool PICARD>
 __global__ void __launch_bounds__(kBlock, MINB)
 k_force_list(DevParams P0, ListArgs A) {
+    if (PICARD && skipped(A.skip)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = P0.n;
     uint32_t disp_bits = 0u;
+    uint32_t res_bits = 0u;
+    bool viol = false;
     if (s < n) {
         // every per-slot load issued up front: they are independent, and the kernel is
         // bound by their latency when lists are short
@@ -129,6 +142,15 @@ k_force_list(DevParams P0, ListArgs A) {
         const float4 xb = A.xbuild[s];
         const int hcnt_in = HIST ? A.hcnt_in[s] : 0;
         const DevParams& P = BATCH ? A.scene_params[scene] : P0;
+        if (PICARD) {
+            // the rhs of a Picard step pairs the last iterate's velocity with its forces
+            A.rhs_vel[s] = vi;
+            A.rhs_ids[s] = id;
+            if (A.iter > 0) {
+                const float ex = pi.x - xb.x, ey = pi.y - xb.y, ez = pi.z - xb.z;
+                viol = !(ex * ex + ey * ey + ez * ez < A.viol_thr);
+            }
+        }
         if (BATCH && P.frozen) {
             A.pos_out[s] = pi;
             A.vel_out[s] = vi;
@@ -239,10 +261,22 @@ k_force_list(DevParams P0, ListArgs A) {
             }
             if (HIST) A.hcnt_out[s] = h.out_count;
             const float3 a = make_float3(f.x / mi, f.y / mi, f.z / mi);
-            const float3 v1 = make_float3(fmaf(P.dt, a.x, vel.x), fmaf(P.dt, a.y, vel.y),
-                                          fmaf(P.dt, a.z, vel.z));
-            const float3 x1 = make_float3(fmaf(P.dt, v1.x, pos.x), fmaf(P.dt, v1.y, pos.y),
-                                          fmaf(P.dt, v1.z, pos.z));
+            float3 v1, x1;
+            if (!PICARD) {
+                v1 = make_float3(fmaf(P.dt, a.x, vel.x), fmaf(P.dt, a.y, vel.y),
+                                 fmaf(P.dt, a.z, vel.z));
+                x1 = make_float3(fmaf(P.dt, v1.x, pos.x), fmaf(P.dt, v1.y, pos.y),
+                                 fmaf(P.dt, v1.z, pos.z));
+            } else {
+                const float4 xn = A.xn[s], vn = A.vn[s];
+                v1 = make_float3(fmaf(P.dt, a.x, vn.x), fmaf(P.dt, a.y, vn.y),
+                                 fmaf(P.dt, a.z, vn.z));
+                x1 = make_float3(fmaf(P.dt, v1.x, xn.x), fmaf(P.dt, v1.y, xn.y),
+                                 fmaf(P.dt, v1.z, xn.z));
+                res_bits = max(res_bits, __float_as_uint(fabsf(x1.x - pos.x)));
+                res_bits = max(res_bits, __float_as_uint(fabsf(x1.y - pos.y)));
+                res_bits = max(res_bits, __float_as_uint(fabsf(x1.z - pos.z)));
+            }
             A.pos_out[s] = make_float4(x1.x, x1.y, x1.z, ri);
             A.vel_out[s] = make_float4(v1.x, v1.y, v1.z, mi);
             A.ids_out[s] = id;
@@ -257,6 +291,41 @@ k_force_list(DevParams P0, ListArgs A) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) disp_bits = max(disp_bits, __shfl_xor_sync(0xffffffffu, disp_bits, o));
     if ((threadIdx.x & 31) == 0 && disp_bits != 0u) atomicMax(&A.list_ctrl[kLcDisp], disp_bits);
+    if (PICARD) {
+        // max of non-negative float bits (NaN above +inf, so it is kept)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) res_bits = max(res_bits, __shfl_xor_sync(0xffffffffu, res_bits, o));
+        if ((threadIdx.x & 31) == 0 && res_bits != 0u) atomicMax(A.res_slot, res_bits);
+        if (__any_sync(0xffffffffu, viol) && (threadIdx.x & 31) == 0) atomicOr(&A.list_ctrl[kLcViol], 1u);
+        if (blockIdx.x == 0 && threadIdx.x == 0) *A.picard_used = A.iter + 1;
+    }
+}
+
+// The last executed Picard iteration k wrote the B buffers when k is even and the
+// scratch buffers when k is odd (iterations alternate, starting in B).
+__global__ void __launch_bounds__(kBlock)
+k_list_finalize(int n, const int* __restrict__ used, const float4* __restrict__ xpos,
+                const float4* __restrict__ xvel, float4* __restrict__ pos,
+                float4* __restrict__ vel) {
+    if ((*used & 1) != 0) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    pos[s] = xpos[s];
+    vel[s] = xvel[s];
+}
+
+__global__ void k_list_picard_check(uint32_t* __restrict__ ctrl,
+                                    unsigned long long* __restrict__ counters, int use_cond,
+                                    cudaGraphConditionalHandle cond) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const bool redo = ctrl[kLcViol] != 0u;
+    ctrl[kLcViol] = 0u;
+    ctrl[kLcRedo] = redo ? __float_as_uint(1.f) : 0u;
+    if (redo) {
+        ctrl[kLcForce] = 1u;  // the redo re-sorts the state: build next step
+        counters[kCntPicardRedos] += 1ull;
+    }
+    if (use_cond) cudaGraphSetConditional(cond, redo ? 1u : 0u);
 }
 
 // Warp-cooperative variant: a contact's work (spring lookup, Coulomb cap, dashpot) is
@@ -539,21 +608,37 @@ void launch_list_copy(int n, const float4* pos, const float4* vel, const int* id
                                                   vel_out, ids_out, hcnt_out, scene_out, skip);
 }
 
-template <int MINB>
+template <int MINB, bool PICARD>
 void force_list_variant(const DevParams& P, const ListArgs& a, cudaStream_t st, int block) {
     const int nb = blocks_for(P.n, block);
     const bool batch = a.scene_params != nullptr;
     if (P.history) {
-        if (batch) k_force_list<true, true, MINB><<<nb, block, 0, st>>>(P, a);
-        else k_force_list<true, false, MINB><<<nb, block, 0, st>>>(P, a);
+        if (batch) k_force_list<true, true, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
+        else k_force_list<true, false, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
     } else {
-        if (batch) k_force_list<false, true, MINB><<<nb, block, 0, st>>>(P, a);
-        else k_force_list<false, false, MINB><<<nb, block, 0, st>>>(P, a);
+        if (batch) k_force_list<false, true, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
+        else k_force_list<false, false, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
     }
 }
 
+void launch_list_finalize(int n, const int* picard_used, const float4* xpos,
+                          const float4* xvel, float4* pos, float4* vel, cudaStream_t st) {
+    k_list_finalize<<<blocks_for(n), kBlock, 0, st>>>(n, picard_used, xpos, xvel, pos, vel);
+}
+
+void launch_list_picard_check(uint32_t* list_ctrl, unsigned long long* counters, bool use_cond,
+                              cudaGraphConditionalHandle cond, cudaStream_t st) {
+    k_list_picard_check<<<1, 32, 0, st>>>(list_ctrl, counters, use_cond ? 1 : 0, cond);
+}
+
 void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, int block,
-                       int min_blocks) {
+                       int min_blocks, bool picard) {
+    if (picard) {
+        // the per-lane kernel (the cooperative one has no Picard form)
+        if (min_blocks == 4) force_list_variant<4, true>(P, a, st, block == 0 ? kBlock : block);
+        else force_list_variant<5, true>(P, a, st, block);
+        return;
+    }
     if (min_blocks == 0) {
         // warp-cooperative kernel: its shared queues are sized for kBlock threads
         const int nb = blocks_for(P.n, kBlock);
@@ -566,9 +651,9 @@ void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, i
             else k_force_list_coop<false, false><<<nb, kBlock, 0, st>>>(P, a);
         }
     } else if (min_blocks == 4) {
-        force_list_variant<4>(P, a, st, block);
+        force_list_variant<4, false>(P, a, st, block);
     } else {
-        force_list_variant<5>(P, a, st, block);
+        force_list_variant<5, false>(P, a, st, block);
     }
 }
 

@@ -140,6 +140,13 @@ struct wd_sim {
     int lpar = 0;
     int force_block = wd::kBlock;   // threads per block of the contact kernel
     int force_minb = 5;             // register variant of the list contact kernel
+    // Picard with lists: scratch iterate buffers (and, for a redo's gather, ids / scenes)
+    float4* xpos = nullptr;
+    float4* xvel = nullptr;
+    int* xids = nullptr;
+    int* xscene = nullptr;
+    float4* rhs_vel = nullptr;      // the last iterate's velocity, slot order of rhs_ids
+    int* rhs_ids = nullptr;
     int* nbr = nullptr;
     int* nbr_cnt = nullptr;
     float4* xbuild = nullptr;
@@ -332,7 +339,8 @@ void free_sim(wd_sim* s) {
                     s->sceneC, s->d_seg, s->d_chunk_base, s->grain_vals, s->scene_sums,
                     s->scene_overflow, s->scene_unstable, s->d_node_seg, s->d_node_chunk,
                     s->node_vals, s->chaos_partials, s->chaos_sums, s->grain_sums,
-                    s->chaos_grid, s->nbr, s->nbr_cnt, s->xbuild, s->list_ctrl, s->list_len};
+                    s->chaos_grid, s->nbr, s->nbr_cnt, s->xbuild, s->list_ctrl, s->list_len,
+                    s->xpos, s->xvel, s->xids, s->xscene, s->rhs_vel, s->rhs_ids};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
@@ -539,47 +547,163 @@ void enqueue_list_build(wd_sim* s, wd::Skip gate, cudaStream_t st) {
                          hist ? s->hcnt_slot : nullptr, batch ? s->sceneA : nullptr, gate, st);
 }
 
-// One list-mode step: decide, build if needed, contacts + integration from A into B.
-cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool capture,
-                              cudaEvent_t mid = nullptr) {
-    const DevParams& P = s->P;
-    const bool hist = P.history != 0, batch = s->scenes > 1;
-    const float reach = 0.45f * P.skin;
-    const float thr = reach * reach;
+// Decide and, when needed, build (an IF node in a graph; gated launches otherwise).
+cudaError_t enqueue_list_decide_build(wd_sim* s, float thr, cudaStream_t st, bool capture) {
     if (!capture) {
         wd::launch_list_decide(s->list_ctrl, thr, s->counters, false, 0, st);
         enqueue_list_build(s, wd::Skip{s->list_ctrl + wd::kLcDecision, 0.5f}, st);
-    } else {
-        cudaStreamCaptureStatus status;
-        cudaGraph_t graph = nullptr;
-        const cudaGraphNode_t* deps = nullptr;
-        size_t ndeps = 0;
-        cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
-        if (e != cudaSuccess) return e;
-        cudaGraphConditionalHandle cond;
-        e = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault);
-        if (e != cudaSuccess) return e;
-        wd::launch_list_decide(s->list_ctrl, thr, s->counters, true, cond, st);
-        e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
-        if (e != cudaSuccess) return e;
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = cond;
-        cp.conditional.type = cudaGraphCondTypeIf;
-        cp.conditional.size = 1;
-        cudaGraphNode_t node = nullptr;
-        e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
-        if (e != cudaSuccess) return e;
-        e = cudaStreamBeginCaptureToGraph(s->aux_stream, cp.conditional.phGraph_out[0], nullptr,
-                                          nullptr, 0, cudaStreamCaptureModeRelaxed);
-        if (e != cudaSuccess) return e;
-        enqueue_list_build(s, wd::Skip{nullptr, 0.f}, s->aux_stream);
-        cudaGraph_t captured = nullptr;
-        e = cudaStreamEndCapture(s->aux_stream, &captured);
-        if (e != cudaSuccess) return e;
-        e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
-        if (e != cudaSuccess) return e;
+        return cudaGetLastError();
     }
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle cond;
+    e = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    wd::launch_list_decide(s->list_ctrl, thr, s->counters, true, cond, st);
+    e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamBeginCaptureToGraph(s->aux_stream, cp.conditional.phGraph_out[0], nullptr,
+                                      nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return e;
+    enqueue_list_build(s, wd::Skip{nullptr, 0.f}, s->aux_stream);
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(s->aux_stream, &captured);
+    if (e != cudaSuccess) return e;
+    return cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+// Redo of a list-mode Picard step whose iterates left the lists' validity bound: the
+// step-start state is copied into B and stepped there by the per-iteration search
+// (the scratch buffers take the search's gathered copy).
+cudaError_t enqueue_picard_redo(wd_sim* s, int parity, cudaStream_t st) {
+    const bool hist = s->P.history != 0, batch = s->scenes > 1;
+    const wd::Skip none{nullptr, 0.f};
+    wd::launch_list_copy(s->n, s->posA, s->velA, s->idsA, hist ? s->hcnt_slot : nullptr,
+                         batch ? s->sceneA : nullptr, s->posB, s->velB, s->idsB,
+                         hist ? s->hcnt_g : nullptr, batch ? s->sceneB : nullptr, none, st);
+    float4 *pa = s->posA, *pb = s->posB, *va = s->velA, *vb = s->velB;
+    int *ia = s->idsA, *ib = s->idsB, *ha = s->hcnt_slot, *hb = s->hcnt_g;
+    int *sa = s->sceneA, *sbn = s->sceneB;
+    s->posA = pb; s->velA = vb; s->idsA = ib; s->hcnt_slot = hb; s->sceneA = sbn;
+    s->posB = s->xpos; s->velB = s->xvel; s->idsB = s->xids; s->sceneB = s->xscene;
+    cudaError_t e = enqueue_step(s, parity, st, false, nullptr);
+    // the searched step's rhs pairs its last gathered iterate with the forces
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->rhs_vel, s->xvel, sizeof(float4) * s->n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->rhs_ids, s->xids, sizeof(int) * s->n, cudaMemcpyDeviceToDevice, st);
+    s->posA = pa; s->posB = pb; s->velA = va; s->velB = vb; s->idsA = ia; s->idsB = ib;
+    s->hcnt_slot = ha; s->hcnt_g = hb; s->sceneA = sa; s->sceneB = sbn;
+    return e;
+}
+
+// One list-mode backward Euler / Picard step: decide, build if needed, then the
+// iterations on the lists (iterates alternate between B and the scratch buffers,
+// integrating from the state in A), the last iterate into B, and, when an iterate left
+// the lists' validity bound, the redo. Builds start at 0.30 skin so that iterates
+// rarely reach the 0.45 bound within a step.
+cudaError_t enqueue_step_list_picard(wd_sim* s, int parity, cudaStream_t st, bool capture,
+                                     cudaEvent_t mid) {
+    const DevParams& P = s->P;
+    const bool hist = P.history != 0, batch = s->scenes > 1;
+    const float build_at = 0.30f * P.skin, valid = 0.45f * P.skin;
+    cudaError_t e = enqueue_list_decide_build(s, build_at * build_at, st, capture);
+    if (e != cudaSuccess) return e;
+    if (mid) cudaEventRecord(mid, st);
+    e = cudaMemsetAsync(s->picard_res, 0, sizeof(uint32_t) * s->picard_iters, st);
+    if (e != cudaSuccess) return e;
+    for (int k = 0; k < s->picard_iters; ++k) {
+        wd::ListArgs a{};
+        const bool in_b = k > 0 && ((k - 1) & 1) == 0;
+        a.pos = k == 0 ? s->posA : (in_b ? s->posB : s->xpos);
+        a.vel = k == 0 ? s->velA : (in_b ? s->velB : s->xvel);
+        a.ids = s->idsA; a.table = s->sb.table;
+        a.pos_out = (k & 1) == 0 ? s->posB : s->xpos;
+        a.vel_out = (k & 1) == 0 ? s->velB : s->xvel;
+        a.ids_out = s->idsB; a.acc_out = s->acc;
+        a.hist_in = hist ? s->hist[parity] : nullptr;
+        a.hcnt_in = hist ? s->hcnt_slot : nullptr;
+        a.hist_out = hist ? s->hist[parity ^ 1] : nullptr;
+        a.hcnt_out = hist ? s->hcnt_g : nullptr;
+        a.counters = s->counters;
+        a.nbr = s->nbr; a.nbr_cnt = s->nbr_cnt; a.xbuild = s->xbuild; a.list_ctrl = s->list_ctrl;
+        a.scene_params = batch ? s->d_scene_P : nullptr;
+        a.scene = s->sceneA;
+        a.scene_out = s->sceneB;
+        a.xn = s->posA; a.vn = s->velA;
+        a.res_slot = s->picard_res + k;
+        a.picard_used = s->picard_used;
+        a.iter = k;
+        a.viol_thr = valid * valid;
+        a.skip = wd::Skip{k == 0 ? nullptr : s->picard_res + (k - 1), P.picard_tol};
+        a.rhs_vel = s->rhs_vel;
+        a.rhs_ids = s->rhs_ids;
+        wd::launch_force_list(P, a, st, s->force_block, s->force_minb == 4 ? 4 : 5, true);
+    }
+    wd::launch_list_finalize(s->n, s->picard_used, s->xpos, s->xvel, s->posB, s->velB, st);
+    if (!capture) {
+        wd::launch_list_picard_check(s->list_ctrl, s->counters, false, 0, st);
+        uint32_t redo = 0;
+        e = cudaMemcpyAsync(&redo, s->list_ctrl + wd::kLcRedo, sizeof(redo), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        if (redo) e = enqueue_picard_redo(s, parity, st);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle cond;
+    e = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return e;
+    wd::launch_list_picard_check(s->list_ctrl, s->counters, true, cond, st);
+    e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamBeginCaptureToGraph(s->aux_stream, cp.conditional.phGraph_out[0], nullptr,
+                                      nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return e;
+    const cudaError_t re = enqueue_picard_redo(s, parity, s->aux_stream);
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(s->aux_stream, &captured);
+    if (re != cudaSuccess) return re;
+    if (e != cudaSuccess) return e;
+    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+// One list-mode step: decide, build if needed, contacts + integration from A into B.
+cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool capture,
+                              cudaEvent_t mid = nullptr) {
+    if (s->picard) return enqueue_step_list_picard(s, parity, st, capture, mid);
+    const DevParams& P = s->P;
+    const bool hist = P.history != 0, batch = s->scenes > 1;
+    const float reach = 0.45f * P.skin;
+    cudaError_t e = enqueue_list_decide_build(s, reach * reach, st, capture);
+    if (e != cudaSuccess) return e;
     if (mid) cudaEventRecord(mid, st);
     wd::ListArgs a{};
     a.pos = s->posA; a.vel = s->velA; a.ids = s->idsA; a.table = s->sb.table;
@@ -797,8 +921,16 @@ int alloc_sim(wd_sim* s) {
         WD_CUDA(dalloc(&s->xbuild, n));
         WD_CUDA(dalloc(&s->list_ctrl, wd::kLcWords));
         WD_CUDA(dalloc(&s->list_len, 1));
-        const uint32_t init[wd::kLcWords] = {0u, 0u, 1u, 0u};  // the first step builds
+        const uint32_t init[wd::kLcWords] = {0u, 0u, 1u, 0u, 0u, 0u};  // the first step builds
         WD_CUDA(cudaMemcpy(s->list_ctrl, init, sizeof(init), cudaMemcpyHostToDevice));
+        if (s->picard) {
+            WD_CUDA(dalloc(&s->xpos, n));
+            WD_CUDA(dalloc(&s->xvel, n));
+            WD_CUDA(dalloc(&s->xids, n));
+            WD_CUDA(dalloc(&s->rhs_vel, n));
+            WD_CUDA(dalloc(&s->rhs_ids, n));
+            if (S > 1) WD_CUDA(dalloc(&s->xscene, n));
+        }
     }
     return WD_OK;
 }
@@ -820,6 +952,10 @@ int upload_initial(wd_sim* s, const float* state) {
     WD_CUDA(cudaMemcpy(s->posB, s->posA, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
     WD_CUDA(cudaMemcpy(s->velB, s->velA, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
     WD_CUDA(cudaMemcpy(s->idsB, s->idsA, sizeof(int) * n, cudaMemcpyDeviceToDevice));
+    if (s->rhs_vel) {
+        WD_CUDA(cudaMemcpy(s->rhs_vel, s->velA, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
+        WD_CUDA(cudaMemcpy(s->rhs_ids, s->idsA, sizeof(int) * n, cudaMemcpyDeviceToDevice));
+    }
     WD_CUDA(cudaMemset(s->acc, 0, sizeof(float4) * n));
     if (s->scenes > 1) {
         std::vector<int> sc(n);
@@ -915,7 +1051,7 @@ int create_scenes(const wd::Config* const* cfgs, int S, const int64_t* counts,
     s->dt = c0.dt;
     s->picard = c0.time_integrator != "semi_implicit_euler";
     s->picard_iters = s->picard ? c0.picard_iterations : 1;
-    s->lists = c0.neighbor_skin > 0.f && !s->picard;
+    s->lists = c0.neighbor_skin > 0.f;
     s->num_cells = cells;
     s->scene_off.assign(1, 0);
     s->scene_nodes_off.assign(1, 0);
@@ -1260,7 +1396,9 @@ int wd_get_positions(wd_sim* sim, float* positions) {
 
 int wd_get_rhs(wd_sim* sim, float* rhs) {
     if (!sim || !rhs) return fail(WD_ERR_INVALID, "wd_get_rhs: NULL argument");
-    wd::launch_rhs_to_aos(sim->n, sim->velB, sim->acc, sim->idsB, sim->staging, sim->stream);
+    const bool picard_lists = sim->lists && sim->picard;
+    wd::launch_rhs_to_aos(sim->n, picard_lists ? sim->rhs_vel : sim->velB, sim->acc,
+                          picard_lists ? sim->rhs_ids : sim->idsB, sim->staging, sim->stream);
     WD_CUDA(cudaGetLastError());
     WD_CUDA(cudaMemcpyAsync(rhs, sim->staging, sizeof(float) * 6 * static_cast<size_t>(sim->n),
                             cudaMemcpyDeviceToHost, sim->stream));
@@ -1589,7 +1727,9 @@ int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
     // keys, mover kernel, merge, gather, contact per search; a search that takes the
     // radix path adds 1 + 3 per pass (wd_radix_search_count)
     // list mode: the decision and the contact kernel; builds add wd_list_stats' count
-    *kernels = sim->lists ? 2 : static_cast<int64_t>(5) * sim->picard_iters;
+    // (Picard: the decision, the iterations, the last iterate's copy, the redo check)
+    *kernels = sim->lists ? (sim->picard ? sim->picard_iters + 3 : 2)
+                          : static_cast<int64_t>(5) * sim->picard_iters;
     return WD_OK;
 }
 
@@ -1660,8 +1800,6 @@ int wd_debug_candidates(wd_sim* sim, int64_t* offsets, int32_t* cand, uint8_t* c
 // entering list mode the current buffers are labelled with the spring parity.
 static int apply_skin(wd_sim* s, float skin) {
     if (skin < 0.f) return fail(WD_ERR_INVALID, "neighbor skin must be >= 0");
-    if (skin > 0.f && s->picard)
-        return fail(WD_ERR_INVALID, "neighbor lists cover semi-implicit Euler only");
     const bool lists = skin > 0.f;
     if (lists && !s->nbr) {
         const int n = s->n;
@@ -1671,6 +1809,18 @@ static int apply_skin(wd_sim* s, float skin) {
         WD_CUDA(dalloc(&s->list_ctrl, wd::kLcWords));
         WD_CUDA(dalloc(&s->list_len, 1));
         WD_CUDA(cudaMemsetAsync(s->list_ctrl, 0, sizeof(uint32_t) * wd::kLcWords, s->stream));
+    }
+    if (lists && s->picard && !s->xpos) {
+        const int n = s->n;
+        WD_CUDA(dalloc(&s->xpos, n));
+        WD_CUDA(dalloc(&s->xvel, n));
+        WD_CUDA(dalloc(&s->xids, n));
+        WD_CUDA(dalloc(&s->rhs_vel, n));
+        WD_CUDA(dalloc(&s->rhs_ids, n));
+        // the rhs getter reads these in list mode: start them at the current rhs source
+        WD_CUDA(cudaMemcpyAsync(s->rhs_vel, s->velB, sizeof(float4) * n, cudaMemcpyDeviceToDevice, s->stream));
+        WD_CUDA(cudaMemcpyAsync(s->rhs_ids, s->idsB, sizeof(int) * n, cudaMemcpyDeviceToDevice, s->stream));
+        if (s->scenes > 1) WD_CUDA(dalloc(&s->xscene, n));
     }
     if (lists && !s->lists) s->lpar = s->P.history ? s->hist_cur : s->lpar;
     s->lists = lists;
@@ -1698,6 +1848,11 @@ static std::string tune_key(const wd_sim* s) {
                   s->n, s->scenes, s->cfg.grid[0], s->cfg.grid[1], s->cfg.grid[2], sms,
                   s->P.history, s->picard ? 1 : 0, s->cfg.kernel_timing ? 0 : 1);
     return buf;
+}
+
+int wd_picard_redo_count(wd_sim* sim, int64_t* redos) {
+    if (!sim || !redos) return fail(WD_ERR_INVALID, "wd_picard_redo_count: NULL argument");
+    return read_counter(sim, wd::kCntPicardRedos, redos);
 }
 
 int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length) {
@@ -1888,8 +2043,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         mean_r /= static_cast<double>(sim->radius.size());
         const float d = static_cast<float>(2.0 * mean_r);
         std::vector<float> skins = {0.f};
-        if (!sim->picard)
-            for (float f : {0.05f, 0.1f, 0.2f, 0.4f}) skins.push_back(f * d);
+        for (float f : {0.05f, 0.1f, 0.2f, 0.4f}) skins.push_back(f * d);
         // (block, variant): variant 5 / 4 = per-lane list kernel with 48 / 64 registers,
         // 0 = warp-cooperative list kernel (256 threads)
         const int cands[][2] = {{128, 5}, {256, 5}, {128, 4}, {256, 4}, {256, 0}};
@@ -1907,6 +2061,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
                 const int bl = cands[cand][0];
                 const int mb = cands[cand][1];
                 if (sk == 0.f && mb != 5) continue;  // the searched kernel has one variant
+                if (sim->picard && mb == 0) continue;  // no cooperative Picard kernel
                 rc = apply_skin(sim, sk);
                 if (rc == WD_OK) {
                     sim->force_block = bl;

@@ -356,6 +356,12 @@ class ParticleDynamics:
         many registers, 0: warp-cooperative); results do not depend on them."""
         check(lib.wd_set_contact_kernel(self._h, int(block), int(variant)))
 
+    def picard_redo_count(self) -> int:
+        """Picard steps on lists redone with the per-iteration search so far."""
+        v = ctypes.c_int64()
+        check(lib.wd_picard_redo_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
     def list_stats(self) -> tuple[int, int, float]:
         """(Verlet-list builds so far, kernels each build launches, mean list length)."""
         b = ctypes.c_int64()
