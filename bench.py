@@ -324,6 +324,8 @@ def run_ours(args) -> int:
     torch.cuda.synchronize()
     radix0, radix_each = sim.radix_search_count()
     builds0, build_kernels, _ = sim.list_stats()
+    picard = scene.cfg.time_integrator != "semi_implicit_euler"
+    iters0, redos0 = sim.picard_counts()
     barrier()
     # Each step: an L2 flush (512 MiB write) queued on the library's stream, then the
     # step bracketed by events on that stream. Nothing syncs the host inside the loop,
@@ -340,6 +342,7 @@ def run_ours(args) -> int:
     radix_searches = sim.radix_search_count()[0] - radix0
     builds, _, mean_list = sim.list_stats()
     builds -= builds0
+    iters1, redos1 = sim.picard_counts()
     lists = scene.cfg.neighbor_skin > 0
     # list mode: a build launches the whole search (its radix kernels gated) and the
     # list kernels; otherwise a search adds the radix kernels only when it takes them
@@ -366,6 +369,9 @@ def run_ours(args) -> int:
     sim.set_kernel_timing(args.direct)
     search_ms = float(t1[0] - t0[0]) / args.phase_steps
     contact_ms = float(t1[1] - t0[1]) / args.phase_steps
+    # backward Euler / Picard: the timed contact phase is the whole step, one contact
+    # launch per executed iteration (plus, without lists, each iteration's search)
+    phase_iters = (sim.picard_counts()[0] - iters1) / args.phase_steps if picard else 1.0
     cnt, _, _ = sim.get_history()
     entries = int(cnt.astype(np.int64).sum())
     # contact kernel, algorithmic bytes per launch: read x,r / v,m / id (36 B) and
@@ -376,7 +382,7 @@ def run_ours(args) -> int:
     if lists:
         # plus the list count and the build position (20 B) and the list (4 B / entry)
         contact_bytes += int(20 * n + 4 * mean_list * n)
-    achieved = contact_bytes / (contact_ms / 1e3) / 1e9
+    achieved = contact_bytes * phase_iters / (contact_ms / 1e3) / 1e9
     peak, peak_kind = measured_hbm_peak()
 
     # e2e through the C ABI with pinned host buffers: every step uploads its state and
@@ -443,7 +449,7 @@ def run_ours(args) -> int:
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "algorithmic_bytes_per_launch": contact_bytes,
-                         "kernel_ms": contact_ms, "search_ms": search_ms},
+                         "kernel_ms": contact_ms / phase_iters, "search_ms": search_ms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
                     "d2h_bytes_per_step": 12 * n, "steps": args.e2e_steps},
@@ -451,8 +457,9 @@ def run_ours(args) -> int:
             "gpu_launches": launches,
             "radix_searches_timed": radix_searches,
             "neighbor_lists": {"skin_m": scene.cfg.neighbor_skin, "builds_timed": builds,
-                               "mean_list_length": mean_list,
-                               "picard_redos": sim.picard_redo_count()} if lists else None,
+                               "mean_list_length": mean_list} if lists else None,
+            "picard": {"iterations_per_step": (iters1 - iters0) / args.steps,
+                       "redone_steps_timed": redos1 - redos0} if picard else None,
             "history_entries_per_grain": entries / n,
             "scene_results": scene_results,
             "autotuned": tuned,

@@ -268,8 +268,8 @@ int wd_grid_overflow_count(wd_sim* sim, int64_t* count);
 int wd_set_neighbor_skin(wd_sim* sim, float skin);
 /* Autotuner (extension): times `steps` steps for each neighbor skin in {0, 0.05,
  * 0.1, 0.2, 0.4} mean diameters, contact-kernel block size in {128, 256} and, with
- * lists, its variant (per-lane with 48 or 64 registers, warp-cooperative) from the same
- * saved state, keeps
+ * lists, its variant (per-lane with 48 or 64 registers, warp-cooperative, bulk-staged)
+ * from the same saved state, keeps
  * the fastest and restores the state (results do not depend on the choice). With
  * cache_path, a line "key skin block variant" keyed by grain count,
  * scenes, grid, SM count, history, integrator and launch mode is reused or appended.
@@ -277,14 +277,22 @@ int wd_set_neighbor_skin(wd_sim* sim, float skin);
 int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_out,
                 int32_t* block_out);
 /* The current schedule: neighbor skin, contact-kernel block size, and the list
- * contact kernel variant: 48 or 64 (registers per thread of the per-lane kernel) or 0
- * (the warp-cooperative kernel, 256 threads). wd_set_contact_kernel sets the last two
- * (the autotuner's other choices); results do not depend on them. */
+ * contact kernel variant: 48 or 64 (registers per thread of the per-lane kernel), 0
+ * (the warp-cooperative kernel, 256 threads) or 1 (the bulk-staged persistent kernel,
+ * 256 threads: per-slot arrays copied into shared memory by cp.async.bulk two tiles
+ * ahead). wd_set_contact_kernel sets the last two (the autotuner's other choices);
+ * results do not depend on them. */
 int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant);
 int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant);
-/* Backward Euler / Picard on Verlet lists: steps so far that an iterate took beyond
- * the lists' validity bound and that were redone with the per-iteration search. */
-int wd_picard_redo_count(wd_sim* sim, int64_t* redos);
+/* Verlet lists: steps so far whose contact kernel measured the exact displacement
+ * since the build (reading the build positions). The other steps decide on a bound:
+ * the last exact value plus the largest per-step displacement of each step since. */
+int wd_list_exact_count(wd_sim* sim, int64_t* steps);
+/* Backward Euler / Picard: iterations executed so far (iterations that a converged
+ * step skipped are not counted), and, on Verlet lists, the steps whose iterate went
+ * beyond the lists' validity bound and that were redone with the per-iteration search
+ * (their iterations count twice). */
+int wd_picard_counts(wd_sim* sim, int64_t* iterations, int64_t* redos);
 /* Verlet lists (simulation.neighbor_skin > 0): builds so far, kernels one build
  * launches, and the mean list length of the last build (0 without lists). */
 int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length);

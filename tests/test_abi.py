@@ -116,6 +116,7 @@ def test_batch_entry_points_take_the_python_argument_forms():
         lib.wd_io_join(None),
         lib.wd_get_tuning(None, None, None, None),
         lib.wd_set_contact_kernel(None, 256, 0),
-        lib.wd_picard_redo_count(None, None),
+        lib.wd_picard_counts(None, None, None),
+        lib.wd_list_exact_count(None, None),
     ]
     assert all(c == -1 for c in calls), calls

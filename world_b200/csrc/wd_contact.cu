@@ -117,7 +117,10 @@ k_force(DevParams P0, ForceArgs A, Skip skip) {
         for (int o = 16; o > 0; o >>= 1)
             res_bits = max(res_bits, __shfl_xor_sync(0xffffffffu, res_bits, o));
         if ((threadIdx.x & 31) == 0 && res_bits != 0u) atomicMax(A.res_slot, res_bits);
-        if (blockIdx.x == 0 && threadIdx.x == 0) *A.picard_used = A.iter + 1;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            *A.picard_used = A.iter + 1;
+            A.counters[kCntPicardIters] += 1ull;
+        }
     }
 }
 

@@ -25,7 +25,10 @@ enum Counter : int {
     kCntRadixSearches = 4,  // searches that took the full radix-sort path
     kCntListBuilds = 5,     // Verlet-list builds
     kCntPicardRedos = 6,    // list-mode Picard steps redone with the per-iteration search
-    kNumCounters = 8,
+    kCntPicardIters = 7,    // Picard iterations executed (contact-kernel launches that ran)
+    kCntListExact = 8,      // list steps whose contact kernel read the build positions
+    kCntStageTimeout = 9,   // bulk-staged contact kernel: stages that never completed
+    kNumCounters = 12,
 };
 
 // Everything a step kernel needs, passed by value (baked into the captured graph).

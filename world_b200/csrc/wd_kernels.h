@@ -127,14 +127,17 @@ struct Segments {
 void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip,
                   cudaStream_t st, int block = kBlock);
 
-// Verlet lists (simulation.neighbor_skin > 0, semi-implicit Euler). list_ctrl words:
-// [0] max |x - x_build|^2 since the build (float bits), [1] a list overflowed,
-// [2] rebuild requested by the host, [3] this step's decision (1.0f: rebuild).
-// Picard: [4] an iteration started from an iterate 0.45 skin or more from its build
-// position, [5] this step's redo decision (1.0f: redo with the per-iteration search).
+// Verlet lists (simulation.neighbor_skin > 0). list_ctrl words:
+// [0] max |x - x_build|^2 over the last step's output (float bits; measured only when
+// [7] was set), [1] a list overflowed, [2] rebuild requested by the host, [3] this
+// step's decision (1.0f: rebuild). Picard: [4] an iteration started from an iterate
+// 0.45 skin or more from its build position, [5] this step's redo decision (1.0f: redo
+// with the per-iteration search). [6] max |x_out - x_in|^2 of the last step (float
+// bits), [7] the contact kernel measures [0] this step, [8..9] (double) a bound on
+// max |x - x_build| of the current state.
 enum ListCtrl {
     kLcDisp = 0, kLcOverflow = 1, kLcForce = 2, kLcDecision = 3, kLcViol = 4, kLcRedo = 5,
-    kLcWords = 6
+    kLcStep = 6, kLcExact = 7, kLcBound = 8, kLcWords = 10
 };
 struct ListArgs {
     const float4* pos; const float4* vel; const int* ids;  // state of the step
@@ -153,16 +156,28 @@ struct ListArgs {
     float viol_thr;
     Skip skip;
     float4* rhs_vel; int* rhs_ids;    // the iterate's velocity and ids, for the rhs getter
+    // semi-implicit Euler: the build decision for the next step, made by the kernel's
+    // last block (threshold on max |x - x_build|, block ticket, the build's IF node)
+    float thr; unsigned* tail_count; int use_cond; cudaGraphConditionalHandle cond;
 };
-void launch_list_decide(uint32_t* list_ctrl, float thr_sq, unsigned long long* counters,
+void launch_list_decide(uint32_t* list_ctrl, float thr, bool always_exact,
+                        unsigned long long* counters,
                         bool use_cond, cudaGraphConditionalHandle cond, cudaStream_t st);
+// The sorted state a list build copies back into the step's buffers (one pass with the
+// listing: pos is read there anyway).
+struct ListCopy {
+    const float4* vel; const int* ids; const int* hcnt; const int* scene;
+    float4* pos_out; float4* vel_out; int* ids_out; int* hcnt_out; int* scene_out;
+};
 void launch_list_build(const DevParams& P, SceneTab T, const float4* pos, const int2* table,
-                       int* nbr, int* nbr_cnt, float4* xbuild, uint32_t* list_ctrl, Skip skip,
-                       cudaStream_t st);
+                       int* nbr, int* nbr_cnt, float4* xbuild, uint32_t* list_ctrl,
+                       const ListCopy& cp, Skip skip, cudaStream_t st);
 void launch_list_copy(int n, const float4* pos, const float4* vel, const int* ids,
                       const int* hcnt, const int* scene, float4* pos_out, float4* vel_out,
                       int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st);
-// min_blocks: the register variant (5: 48 registers, 4: 64 registers per thread)
+// min_blocks: the kernel variant. 5 / 4: per-lane kernel with 48 / 64 registers per
+// thread; 0: warp-cooperative; 1: bulk-staged persistent (kBlock threads). Picard runs
+// the per-lane kernel (4 or 5).
 void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st,
                        int block = kBlock, int min_blocks = 5, bool picard = false);
 // Picard with lists: the last iterate into the B buffers when the last executed

@@ -31,58 +31,130 @@ __device__ __forceinline__ bool skipped(const Skip& s) {
     return s.prev_res != nullptr && s.tol > 0.f && __uint_as_float(*s.prev_res) < s.tol;
 }
 
-// One thread: decide whether this step builds, reset the build-relative state, and
-// switch the build's conditional node (graph mode).
-__global__ void k_list_decide(uint32_t* __restrict__ ctrl, float thr_sq,
-                              unsigned long long* __restrict__ counters, int use_cond,
-                              cudaGraphConditionalHandle cond) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const float disp = __uint_as_float(ctrl[kLcDisp]);
-    const bool build = ctrl[kLcForce] != 0u || ctrl[kLcOverflow] != 0u || !(disp < thr_sq);
+// One thread: decide whether this step builds and switch the build's conditional node
+// (graph mode). The decision needs a bound B on max |x - x_build| of the current state:
+// the exact maximum when the last contact kernel measured it (it then read the build
+// positions), otherwise the previous bound plus the largest displacement of the last
+// step (triangle inequality), so that most steps read no build positions. The measured
+// squares carry float rounding of a few ulps, covered by the factor 1 + 2^-16. The
+// next kernel measures exactly when B is within two last-step displacements of the
+// threshold, so a build is triggered by the bound only when the exact value is close.
+// A NaN or infinite displacement makes B infinite: the step builds.
+// One thread. Volatile accesses: the fused form runs in the last block of a contact
+// kernel whose other blocks updated these words with atomics.
+__device__ bool list_decide_core(uint32_t* ctrl_, float thr, int always_exact,
+                                 unsigned long long* counters) {
+    volatile uint32_t* ctrl = ctrl_;
+    volatile double* bound = reinterpret_cast<volatile double*>(ctrl_ + kLcBound);
+    const double grow = 1.0 + 1.0 / 65536.0;
+    const double step = sqrt(static_cast<double>(__uint_as_float(ctrl[kLcStep]))) * grow;
+    double b = ctrl[kLcExact] != 0u
+                   ? sqrt(static_cast<double>(__uint_as_float(ctrl[kLcDisp]))) * grow
+                   : *bound + step;
+    const bool build = ctrl[kLcForce] != 0u || ctrl[kLcOverflow] != 0u || !(b < thr);
     ctrl[kLcDecision] = build ? __float_as_uint(1.f) : 0u;
     if (build) {
-        ctrl[kLcDisp] = 0u;
+        b = 0.0;
         ctrl[kLcOverflow] = 0u;
         ctrl[kLcForce] = 0u;
         counters[kCntListBuilds] += 1ull;
     }
+    *bound = b;
+    ctrl[kLcDisp] = 0u;
+    ctrl[kLcStep] = 0u;
+    const bool exact = always_exact || (!build && !(b + 2.0 * step < thr));
+    ctrl[kLcExact] = exact ? 1u : 0u;
+    if (exact) counters[kCntListExact] += 1ull;
+    return build;
+}
+
+__global__ void k_list_decide(uint32_t* __restrict__ ctrl, float thr, int always_exact,
+                              unsigned long long* __restrict__ counters, int use_cond,
+                              cudaGraphConditionalHandle cond) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const bool build = list_decide_core(ctrl, thr, always_exact, counters);
     if (use_cond) cudaGraphSetConditional(cond, build ? 1u : 0u);
 }
 
+// The decision fused into the tail of a semi-implicit Euler list kernel: the last block
+// to finish (every block's displacement atomics done) decides whether the lists are
+// rebuilt before the next step and switches the build's conditional node. All threads
+// of every block call it. The barrier orders the block's atomics before thread 0's
+// fence and ticket (the grid-barrier pattern: one fence per block, not per thread).
+__device__ __forceinline__ void list_tail_decide(const ListArgs& A) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned ticket = atomicAdd(A.tail_count, 1u);
+        if (ticket == gridDim.x - 1) {
+            __threadfence();
+            const bool build = list_decide_core(A.list_ctrl, A.thr, 0, A.counters);
+            *reinterpret_cast<volatile unsigned*>(A.tail_count) = 0u;
+            if (A.use_cond) cudaGraphSetConditional(A.cond, build ? 1u : 0u);
+        }
+    }
+}
+
 // The list of every grain, from the run table of the build's sorted state: the
-// contact kernel's stencil walk with the skin added to the contact distance.
+// contact kernel's stencil walk with the skin added to the contact distance. The sorted
+// state is copied back into the step's buffers on the way.
 template <bool BATCH>
 __global__ void __launch_bounds__(kBlock)
 k_list_build(DevParams P0, SceneTab T, const float4* __restrict__ pos,
              const int2* __restrict__ table, int* __restrict__ nbr, int* __restrict__ nbr_cnt,
-             float4* __restrict__ xbuild, uint32_t* __restrict__ ctrl, Skip skip) {
+             float4* __restrict__ xbuild, uint32_t* __restrict__ ctrl, ListCopy cp, Skip skip) {
     if (skipped(skip)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = P0.n;
     if (s >= n) return;
     const DevParams& P = scene_params<BATCH>(P0, T, s);
     const float4 pi = pos[s];
+    cp.pos_out[s] = pi;
+    cp.vel_out[s] = cp.vel[s];
+    cp.ids_out[s] = cp.ids[s];
+    if (cp.hcnt) cp.hcnt_out[s] = cp.hcnt[s];
+    if (BATCH) cp.scene_out[s] = cp.scene[s];
     int cx, cy, cz;
     cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
-    int cnt = 0;
-    for (int dx = -1; dx <= 1; ++dx) {
-        const int nx = cx + dx;
-        if (nx < 0 || nx >= P.grid[0]) continue;
-        int lo[3], hi[3];
-        row_ranges(P, table, nx, cy, cz, lo, hi);
-        for (int t = 0; t < 3; ++t) {
-            for (int j = lo[t]; j < hi[t]; ++j) {
-                if (j == s) continue;
-                const float4 pj = __ldg(&pos[j]);
-                float3 d;
-                const float ns = pair_norm_sq(pi, pj, d);
-                const float reach = (pi.w + pj.w) + P.skin;
-                if (ns < reach * reach) {
-                    if (cnt < kNbrCap) nbr[static_cast<int64_t>(cnt) * n + s] = j;
-                    ++cnt;
-                }
+    // the nine rows' slot ranges first (27 independent table loads), then the
+    // candidates two at a time, in the stencil order
+    int lo[9], hi[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int nx = cx + r - 1;
+        if (nx >= 0 && nx < P.grid[0]) {
+            row_ranges(P, table, nx, cy, cz, lo + 3 * r, hi + 3 * r);
+        } else {
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                lo[3 * r + t] = 0;
+                hi[3 * r + t] = 0;
             }
         }
+    }
+    int cnt = 0;
+    auto visit = [&](int j, float4 pj) {
+        if (j == s) return;
+        float3 d;
+        const float ns = pair_norm_sq(pi, pj, d);
+        const float reach = (pi.w + pj.w) + P.skin;
+        if (ns < reach * reach) {
+            if (cnt < kNbrCap) nbr[static_cast<int64_t>(cnt) * n + s] = j;
+            ++cnt;
+        }
+    };
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        int j = lo[r];
+        const int e = hi[r];
+        // an empty row has lo = INT_MAX, hi = 0: the difference does not overflow
+        for (; e - j > 1; j += 2) {
+            const float4 a = __ldg(&pos[j]);
+            const float4 b = __ldg(&pos[j + 1]);
+            visit(j, a);
+            visit(j + 1, b);
+        }
+        if (j < e) visit(j, __ldg(&pos[j]));
     }
     nbr_cnt[s] = cnt;
     xbuild[s] = pi;
@@ -116,6 +188,198 @@ __device__ __forceinline__ unsigned long long visit_key(const DevParams& P, int 
            static_cast<unsigned>(jd);
 }
 
+// |x1 - x0|^2 as float bits; NaN compares above every float, so a diverging grain
+// reports +inf and forces a build.
+__device__ __forceinline__ uint32_t disp_sq_bits(float3 x1, float3 x0) {
+    const float ex = x1.x - x0.x, ey = x1.y - x0.y, ez = x1.z - x0.z;
+    const float d2 = ex * ex + ey * ey + ez * ez;
+    return d2 >= 0.f ? __float_as_uint(d2) : 0x7f800000u;
+}
+__device__ __forceinline__ uint32_t disp_sq_bits(float3 x1, float4 x0) {
+    return disp_sq_bits(x1, make_float3(x0.x, x0.y, x0.z));
+}
+
+// Warp maxima of the displacement measures into list_ctrl (the exact one only on the
+// steps that measure it; the per-step one for semi-implicit Euler).
+template <bool PICARD>
+__device__ __forceinline__ void list_disp_report(uint32_t* ctrl, bool exact, uint32_t disp_bits,
+                                                 uint32_t step_bits) {
+    if (exact) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            disp_bits = max(disp_bits, __shfl_xor_sync(0xffffffffu, disp_bits, o));
+        if ((threadIdx.x & 31) == 0 && disp_bits != 0u) atomicMax(&ctrl[kLcDisp], disp_bits);
+    }
+    if (!PICARD) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            step_bits = max(step_bits, __shfl_xor_sync(0xffffffffu, step_bits, o));
+        if ((threadIdx.x & 31) == 0 && step_bits != 0u) atomicMax(&ctrl[kLcStep], step_bits);
+    }
+}
+
+// One grain of the list contact kernels, its per-slot values already loaded: contacts
+// from the list in canonical order (or the run table when the list overflowed), the
+// integrator, the displacement measures (maxima folded into disp_bits / step_bits /
+// res_bits, viol or-ed). order_out: write the slot's id (and scene) too. Between builds
+// the slot order is fixed and the ids of both state buffers agree, so only the first
+// step after a build (whose gather reordered one buffer) and Picard write them.
+template <bool HIST, bool BATCH, bool PICARD>
+__device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& A, int s, int n,
+                                           int scene, float4 pi, float4 vi, int id, int cnt,
+                                           float4 xb, int hcnt_in, bool exact, bool order_out,
+                                           uint32_t& disp_bits, uint32_t& step_bits,
+                                           uint32_t& res_bits, bool& viol) {
+    const DevParams& P = BATCH ? A.scene_params[scene] : P0;
+    if (PICARD) {
+        // the rhs of a Picard step pairs the last iterate's velocity with its forces
+        A.rhs_vel[s] = vi;
+        A.rhs_ids[s] = id;
+        if (A.iter > 0) {
+            const float ex = pi.x - xb.x, ey = pi.y - xb.y, ez = pi.z - xb.z;
+            viol |= !(ex * ex + ey * ey + ez * ez < A.viol_thr);
+        }
+    }
+    if (BATCH && P.frozen) {
+        A.pos_out[s] = pi;
+        A.vel_out[s] = vi;
+        if (order_out) {
+            A.ids_out[s] = id;
+            A.scene_out[s] = scene;
+        }
+        A.acc_out[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (HIST) A.hcnt_out[s] = 0;
+    } else {
+        const float3 pos = make_float3(pi.x, pi.y, pi.z);
+        const float3 vel = make_float3(vi.x, vi.y, vi.z);
+        const float ri = pi.w, mi = vi.w;
+        float3 f = make_float3(0.f, 0.f, 0.f);
+        HistRow h;
+        if (HIST) {
+            h.in = A.hist_in + static_cast<int64_t>(id) * kHistCap;
+            h.in_count = hcnt_in;
+            h.out = A.hist_out + static_cast<int64_t>(id) * kHistCap;
+            h.out_count = 0;
+        }
+        wall_forces<HIST>(P, pos, vel, ri, mi, f, h, A.counters);
+        const float3 f_walls = f;
+        const int out_walls = HIST ? h.out_count : 0;
+        const float cut = contact_cutoff_sq(ri, P.rmax);
+        int cx, cy, cz;
+        cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+        bool ordered = true;
+        if (cnt <= kNbrCap) {
+            // the list, in its build order, while the contacts arrive in canonical order
+            unsigned long long last = 0ull;
+            for (int e = 0; e < cnt; ++e) {
+                const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+                const float4 pj = __ldg(&A.pos[j]);
+                float3 d;
+                const float ns = pair_norm_sq(pi, pj, d);
+                if (ns > cut) continue;
+                const float norm = sqrtf(ns);
+                const float dist = pair_dist(norm, ri, pj.w);
+                if (!(dist < 0.f)) continue;
+                const int jd = __ldg(&A.ids[j]);
+                const unsigned long long key = visit_key(P, cx, cy, cz, pj, jd);
+                if (key < last) {
+                    ordered = false;
+                    break;
+                }
+                last = key;
+                const float4 vj = __ldg(&A.vel[j]);
+                pair_force<HIST>(P, d, norm, dist, vel, mi, vj, jd, f, h, A.counters);
+            }
+            if (!ordered) {
+                // a cell crossing re-ordered this grain's contacts: redo them in
+                // canonical order, each pass taking the smallest key above the last
+                f = f_walls;
+                if (HIST) h.out_count = out_walls;
+                long long done = -1;
+                for (;;) {
+                    long long best = 0x7fffffffffffffffll;
+                    int bj = -1;
+                    for (int e = 0; e < cnt; ++e) {
+                        const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+                        const float4 pj = __ldg(&A.pos[j]);
+                        float3 d;
+                        const float ns = pair_norm_sq(pi, pj, d);
+                        if (ns > cut) continue;
+                        const float dist = pair_dist(sqrtf(ns), ri, pj.w);
+                        if (!(dist < 0.f)) continue;
+                        const long long key = static_cast<long long>(
+                            visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j])));
+                        if (key > done && key < best) {
+                            best = key;
+                            bj = j;
+                        }
+                    }
+                    if (bj < 0) break;
+                    done = best;
+                    const float4 pj = __ldg(&A.pos[bj]);
+                    float3 d;
+                    const float ns = pair_norm_sq(pi, pj, d);
+                    const float norm = sqrtf(ns);
+                    const float dist = pair_dist(norm, ri, pj.w);
+                    const float4 vj = __ldg(&A.vel[bj]);
+                    pair_force<HIST>(P, d, norm, dist, vel, mi, vj,
+                                     static_cast<int>(best & 0xffffffffll), f, h, A.counters);
+                }
+            }
+        } else {
+            // list overflow: this step built the lists, so the run table is fresh
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int nx = cx + dx;
+                if (nx < 0 || nx >= P.grid[0]) continue;
+                int lo[3], hi[3];
+                row_ranges(P, A.table, nx, cy, cz, lo, hi);
+                for (int t = 0; t < 3; ++t) {
+                    for (int j = lo[t]; j < hi[t]; ++j) {
+                        const float4 pj = __ldg(&A.pos[j]);
+                        float3 d;
+                        const float ns = pair_norm_sq(pi, pj, d);
+                        if (ns > cut || j == s) continue;
+                        const float norm = sqrtf(ns);
+                        const float dist = pair_dist(norm, ri, pj.w);
+                        if (!(dist < 0.f)) continue;
+                        const float4 vj = __ldg(&A.vel[j]);
+                        const int partner = HIST ? __ldg(&A.ids[j]) : 0;
+                        pair_force<HIST>(P, d, norm, dist, vel, mi, vj, partner, f, h,
+                                         A.counters);
+                    }
+                }
+            }
+        }
+        if (HIST) A.hcnt_out[s] = h.out_count;
+        const float3 a = make_float3(f.x / mi, f.y / mi, f.z / mi);
+        float3 v1, x1;
+        if (!PICARD) {
+            v1 = make_float3(fmaf(P.dt, a.x, vel.x), fmaf(P.dt, a.y, vel.y),
+                             fmaf(P.dt, a.z, vel.z));
+            x1 = make_float3(fmaf(P.dt, v1.x, pos.x), fmaf(P.dt, v1.y, pos.y),
+                             fmaf(P.dt, v1.z, pos.z));
+        } else {
+            const float4 xn = A.xn[s], vn = A.vn[s];
+            v1 = make_float3(fmaf(P.dt, a.x, vn.x), fmaf(P.dt, a.y, vn.y),
+                             fmaf(P.dt, a.z, vn.z));
+            x1 = make_float3(fmaf(P.dt, v1.x, xn.x), fmaf(P.dt, v1.y, xn.y),
+                             fmaf(P.dt, v1.z, xn.z));
+            res_bits = max(res_bits, __float_as_uint(fabsf(x1.x - pos.x)));
+            res_bits = max(res_bits, __float_as_uint(fabsf(x1.y - pos.y)));
+            res_bits = max(res_bits, __float_as_uint(fabsf(x1.z - pos.z)));
+        }
+        A.pos_out[s] = make_float4(x1.x, x1.y, x1.z, ri);
+        A.vel_out[s] = make_float4(v1.x, v1.y, v1.z, mi);
+        if (order_out) {
+            A.ids_out[s] = id;
+            if (BATCH) A.scene_out[s] = scene;
+        }
+        A.acc_out[s] = make_float4(a.x, a.y, a.z, 0.f);
+        if (exact) disp_bits = max(disp_bits, disp_sq_bits(x1, xb));
+        if (!PICARD) step_bits = max(step_bits, disp_sq_bits(x1, pos));
+    }
+}
+
 // MINB resident blocks per SM: 5 caps registers at 48 (more warps, a few spills), 4 at
 // 64 (no spills); the autotuner picks.
 // PICARD: one backward-Euler / Picard iteration (src/backward_euler_picard_kernel.cu:4-17):
@@ -128,177 +392,208 @@ k_force_list(DevParams P0, ListArgs A) {
     if (PICARD && skipped(A.skip)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = P0.n;
-    uint32_t disp_bits = 0u;
+    uint32_t disp_bits = 0u, step_bits = 0u;
     uint32_t res_bits = 0u;
     bool viol = false;
+    // every per-slot load issued up front: they are independent, and the kernel is
+    // bound by their latency when lists are short
+    int scene = 0, id = 0, cnt = 0, hcnt_in = 0;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f), vi = pi, xb = pi;
     if (s < n) {
-        // every per-slot load issued up front: they are independent, and the kernel is
-        // bound by their latency when lists are short
-        const int scene = BATCH ? A.scene[s] : 0;
-        const float4 pi = A.pos[s];
-        const float4 vi = A.vel[s];
-        const int id = A.ids[s];
-        const int cnt = A.nbr_cnt[s];
-        const float4 xb = A.xbuild[s];
-        const int hcnt_in = HIST ? A.hcnt_in[s] : 0;
-        const DevParams& P = BATCH ? A.scene_params[scene] : P0;
-        if (PICARD) {
-            // the rhs of a Picard step pairs the last iterate's velocity with its forces
-            A.rhs_vel[s] = vi;
-            A.rhs_ids[s] = id;
-            if (A.iter > 0) {
-                const float ex = pi.x - xb.x, ey = pi.y - xb.y, ez = pi.z - xb.z;
-                viol = !(ex * ex + ey * ey + ez * ez < A.viol_thr);
-            }
-        }
-        if (BATCH && P.frozen) {
-            A.pos_out[s] = pi;
-            A.vel_out[s] = vi;
-            A.ids_out[s] = id;
-            A.scene_out[s] = scene;
-            A.acc_out[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (HIST) A.hcnt_out[s] = 0;
-        } else {
-            const float3 pos = make_float3(pi.x, pi.y, pi.z);
-            const float3 vel = make_float3(vi.x, vi.y, vi.z);
-            const float ri = pi.w, mi = vi.w;
-            float3 f = make_float3(0.f, 0.f, 0.f);
-            HistRow h;
-            if (HIST) {
-                h.in = A.hist_in + static_cast<int64_t>(id) * kHistCap;
-                h.in_count = hcnt_in;
-                h.out = A.hist_out + static_cast<int64_t>(id) * kHistCap;
-                h.out_count = 0;
-            }
-            wall_forces<HIST>(P, pos, vel, ri, mi, f, h, A.counters);
-            const float3 f_walls = f;
-            const int out_walls = HIST ? h.out_count : 0;
-            const float cut = contact_cutoff_sq(ri, P.rmax);
-            int cx, cy, cz;
-            cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
-            bool ordered = true;
-            if (cnt <= kNbrCap) {
-                // the list, in its build order, while the contacts arrive in canonical order
-                unsigned long long last = 0ull;
-                for (int e = 0; e < cnt; ++e) {
-                    const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
-                    const float4 pj = __ldg(&A.pos[j]);
-                    float3 d;
-                    const float ns = pair_norm_sq(pi, pj, d);
-                    if (ns > cut) continue;
-                    const float norm = sqrtf(ns);
-                    const float dist = pair_dist(norm, ri, pj.w);
-                    if (!(dist < 0.f)) continue;
-                    const int jd = __ldg(&A.ids[j]);
-                    const unsigned long long key = visit_key(P, cx, cy, cz, pj, jd);
-                    if (key < last) {
-                        ordered = false;
-                        break;
-                    }
-                    last = key;
-                    const float4 vj = __ldg(&A.vel[j]);
-                    pair_force<HIST>(P, d, norm, dist, vel, mi, vj, jd, f, h, A.counters);
-                }
-                if (!ordered) {
-                    // a cell crossing re-ordered this grain's contacts: redo them in
-                    // canonical order, each pass taking the smallest key above the last
-                    f = f_walls;
-                    if (HIST) h.out_count = out_walls;
-                    long long done = -1;
-                    for (;;) {
-                        long long best = 0x7fffffffffffffffll;
-                        int bj = -1;
-                        for (int e = 0; e < cnt; ++e) {
-                            const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
-                            const float4 pj = __ldg(&A.pos[j]);
-                            float3 d;
-                            const float ns = pair_norm_sq(pi, pj, d);
-                            if (ns > cut) continue;
-                            const float dist = pair_dist(sqrtf(ns), ri, pj.w);
-                            if (!(dist < 0.f)) continue;
-                            const long long key = static_cast<long long>(
-                                visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j])));
-                            if (key > done && key < best) {
-                                best = key;
-                                bj = j;
-                            }
-                        }
-                        if (bj < 0) break;
-                        done = best;
-                        const float4 pj = __ldg(&A.pos[bj]);
-                        float3 d;
-                        const float ns = pair_norm_sq(pi, pj, d);
-                        const float norm = sqrtf(ns);
-                        const float dist = pair_dist(norm, ri, pj.w);
-                        const float4 vj = __ldg(&A.vel[bj]);
-                        pair_force<HIST>(P, d, norm, dist, vel, mi, vj,
-                                         static_cast<int>(best & 0xffffffffll), f, h, A.counters);
-                    }
-                }
-            } else {
-                // list overflow: this step built the lists, so the run table is fresh
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int nx = cx + dx;
-                    if (nx < 0 || nx >= P.grid[0]) continue;
-                    int lo[3], hi[3];
-                    row_ranges(P, A.table, nx, cy, cz, lo, hi);
-                    for (int t = 0; t < 3; ++t) {
-                        for (int j = lo[t]; j < hi[t]; ++j) {
-                            const float4 pj = __ldg(&A.pos[j]);
-                            float3 d;
-                            const float ns = pair_norm_sq(pi, pj, d);
-                            if (ns > cut || j == s) continue;
-                            const float norm = sqrtf(ns);
-                            const float dist = pair_dist(norm, ri, pj.w);
-                            if (!(dist < 0.f)) continue;
-                            const float4 vj = __ldg(&A.vel[j]);
-                            const int partner = HIST ? __ldg(&A.ids[j]) : 0;
-                            pair_force<HIST>(P, d, norm, dist, vel, mi, vj, partner, f, h,
-                                             A.counters);
-                        }
-                    }
-                }
-            }
-            if (HIST) A.hcnt_out[s] = h.out_count;
-            const float3 a = make_float3(f.x / mi, f.y / mi, f.z / mi);
-            float3 v1, x1;
-            if (!PICARD) {
-                v1 = make_float3(fmaf(P.dt, a.x, vel.x), fmaf(P.dt, a.y, vel.y),
-                                 fmaf(P.dt, a.z, vel.z));
-                x1 = make_float3(fmaf(P.dt, v1.x, pos.x), fmaf(P.dt, v1.y, pos.y),
-                                 fmaf(P.dt, v1.z, pos.z));
-            } else {
-                const float4 xn = A.xn[s], vn = A.vn[s];
-                v1 = make_float3(fmaf(P.dt, a.x, vn.x), fmaf(P.dt, a.y, vn.y),
-                                 fmaf(P.dt, a.z, vn.z));
-                x1 = make_float3(fmaf(P.dt, v1.x, xn.x), fmaf(P.dt, v1.y, xn.y),
-                                 fmaf(P.dt, v1.z, xn.z));
-                res_bits = max(res_bits, __float_as_uint(fabsf(x1.x - pos.x)));
-                res_bits = max(res_bits, __float_as_uint(fabsf(x1.y - pos.y)));
-                res_bits = max(res_bits, __float_as_uint(fabsf(x1.z - pos.z)));
-            }
-            A.pos_out[s] = make_float4(x1.x, x1.y, x1.z, ri);
-            A.vel_out[s] = make_float4(v1.x, v1.y, v1.z, mi);
-            A.ids_out[s] = id;
-            if (BATCH) A.scene_out[s] = scene;
-            A.acc_out[s] = make_float4(a.x, a.y, a.z, 0.f);
-            const float ex = x1.x - xb.x, ey = x1.y - xb.y, ez = x1.z - xb.z;
-            const float d2 = ex * ex + ey * ey + ez * ez;
-            // NaN compares above every float: a diverging grain forces a build
-            disp_bits = d2 >= 0.f ? __float_as_uint(d2) : 0x7f800000u;
-        }
+        scene = BATCH ? A.scene[s] : 0;
+        pi = A.pos[s];
+        vi = A.vel[s];
+        id = A.ids[s];
+        cnt = A.nbr_cnt[s];
+        hcnt_in = HIST ? A.hcnt_in[s] : 0;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) disp_bits = max(disp_bits, __shfl_xor_sync(0xffffffffu, disp_bits, o));
-    if ((threadIdx.x & 31) == 0 && disp_bits != 0u) atomicMax(&A.list_ctrl[kLcDisp], disp_bits);
+    // build positions are read only on the steps that measure the exact displacement;
+    // ids only right after a build
+    const bool exact = PICARD || A.list_ctrl[kLcExact] != 0u;
+    const bool order_out = PICARD || A.list_ctrl[kLcDecision] != 0u;
+    if (s < n) {
+        if (exact) xb = A.xbuild[s];
+        list_grain<HIST, BATCH, PICARD>(P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in, exact,
+                                        order_out, disp_bits, step_bits, res_bits, viol);
+    }
+    list_disp_report<PICARD>(A.list_ctrl, exact, disp_bits, step_bits);
+    if (!PICARD) list_tail_decide(A);
     if (PICARD) {
         // max of non-negative float bits (NaN above +inf, so it is kept)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) res_bits = max(res_bits, __shfl_xor_sync(0xffffffffu, res_bits, o));
         if ((threadIdx.x & 31) == 0 && res_bits != 0u) atomicMax(A.res_slot, res_bits);
         if (__any_sync(0xffffffffu, viol) && (threadIdx.x & 31) == 0) atomicOr(&A.list_ctrl[kLcViol], 1u);
-        if (blockIdx.x == 0 && threadIdx.x == 0) *A.picard_used = A.iter + 1;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            *A.picard_used = A.iter + 1;
+            A.counters[kCntPicardIters] += 1ull;
+        }
     }
+}
+
+// ---- bulk-staged list kernel -------------------------------------------------------
+// Persistent warps over tiles of 32 slots. Each warp keeps two tiles in flight: lane 0
+// issues the tile's per-slot arrays (x, v, ids, list count, spring count, scene, and
+// the build positions on measuring steps) as 1-D bulk copies (cp.async.bulk, the TMA
+// engine; no multicast) into the warp's shared stage, completing on an mbarrier; the
+// lanes compute the tile before while the next arrives. The per-slot loads, whose
+// latency binds the per-lane kernel, leave the critical path. Contacts, forces and the
+// integrator are the per-lane kernel's (list_grain), so the results are identical.
+constexpr int kStageWarps = kBlock / 32;
+constexpr int kStageTile = 32;
+struct __align__(16) SlotStage {
+    float4 pos[kStageTile];
+    float4 vel[kStageTile];
+    float4 xb[kStageTile];
+    int ids[kStageTile];
+    int cnt[kStageTile];
+    int hcnt[kStageTile];
+    int scene[kStageTile];
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// global -> this CTA's shared memory, completing `bytes` on bar (16-byte aligned
+// addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for a phase: false after about a second without completion.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > 1000000000ull) return false;
+    return true;
+}
+
+template <bool HIST, bool BATCH>
+__device__ __forceinline__ void stage_issue(const ListArgs& A, int tile, bool exact,
+                                            SlotStage& S, uint64_t* bar) {
+    const int s0 = tile * kStageTile;
+    constexpr uint32_t f4 = kStageTile * sizeof(float4), i4 = kStageTile * sizeof(int);
+    const uint32_t bytes = 2u * f4 + 2u * i4 + (HIST ? i4 : 0u) + (BATCH ? i4 : 0u) +
+                           (exact ? f4 : 0u);
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(S.pos, A.pos + s0, f4, bar);
+    bulk_g2s(S.vel, A.vel + s0, f4, bar);
+    bulk_g2s(S.ids, A.ids + s0, i4, bar);
+    bulk_g2s(S.cnt, A.nbr_cnt + s0, i4, bar);
+    if (HIST) bulk_g2s(S.hcnt, A.hcnt_in + s0, i4, bar);
+    if (BATCH) bulk_g2s(S.scene, A.scene + s0, i4, bar);
+    if (exact) bulk_g2s(S.xb, A.xbuild + s0, f4, bar);
+}
+
+template <bool HIST, bool BATCH>
+__global__ void __launch_bounds__(kBlock, 5)
+k_force_list_staged(DevParams P0, ListArgs A) {
+    __shared__ SlotStage stage[kStageWarps][2];
+    __shared__ uint64_t bars[kStageWarps][2];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int n = P0.n;
+    const int tiles = (n + kStageTile - 1) / kStageTile;
+    const int whole = n / kStageTile;  // tiles with 32 slots go through the stages
+    const int W = gridDim.x * kStageWarps;
+    const int first = blockIdx.x * kStageWarps + w;
+    const bool exact = A.list_ctrl[kLcExact] != 0u;
+    const bool order_out = A.list_ctrl[kLcDecision] != 0u;  // first step after a build
+    SlotStage* S = stage[w];
+    uint64_t* bar = bars[w];
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
+        for (int k = 0; k < 2; ++k)
+            if (first + k * W < whole) stage_issue<HIST, BATCH>(A, first + k * W, exact, S[k], &bar[k]);
+    }
+    __syncwarp();
+    uint32_t disp_bits = 0u, step_bits = 0u, res_bits = 0u;
+    bool viol = false, failed = false;
+    int it = 0;
+    for (int t = first; t < tiles; t += W, ++it) {
+        const int st = it & 1;
+        const int s = t * kStageTile + lane;
+        float4 pi, vi, xb = make_float4(0.f, 0.f, 0.f, 0.f);
+        int id, cnt, hcnt_in = 0, scene = 0;
+        if (t < whole) {
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar[st], (it >> 1) & 1));
+            if (!ok) {
+                failed = true;
+                break;
+            }
+            const SlotStage& T = S[st];
+            pi = T.pos[lane];
+            vi = T.vel[lane];
+            id = T.ids[lane];
+            cnt = T.cnt[lane];
+            if (HIST) hcnt_in = T.hcnt[lane];
+            if (BATCH) scene = T.scene[lane];
+            if (exact) xb = T.xb[lane];
+            __syncwarp();
+            // the stage is read: refill it with the tile two ahead
+            if (lane == 0 && t + 2 * W < whole)
+                stage_issue<HIST, BATCH>(A, t + 2 * W, exact, S[st], &bar[st]);
+        } else {
+            // the ragged last tile: plain loads
+            if (s >= n) break;
+            pi = A.pos[s];
+            vi = A.vel[s];
+            id = A.ids[s];
+            cnt = A.nbr_cnt[s];
+            if (HIST) hcnt_in = A.hcnt_in[s];
+            if (BATCH) scene = A.scene[s];
+            if (exact) xb = A.xbuild[s];
+        }
+        list_grain<HIST, BATCH, false>(P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in, exact,
+                                       order_out, disp_bits, step_bits, res_bits, viol);
+    }
+    if (failed) {
+        // a stage never completed: flag it and drain what this warp still has in flight
+        // (bounded); the step is left unfinished for the host to report
+        if (lane == 0) {
+            atomicAdd(&A.counters[kCntStageTimeout], 1ull);
+            for (int k = 0; k < 2; ++k) {
+                const int t = first + (it + k) * W;
+                if (t < whole) mbar_wait(&bar[(it + k) & 1], ((it + k) >> 1) & 1);
+            }
+        }
+    } else {
+        list_disp_report<false>(A.list_ctrl, exact, disp_bits, step_bits);
+    }
+    list_tail_decide(A);
 }
 
 // The last executed Picard iteration k wrote the B buffers when k is even and the
@@ -415,7 +710,9 @@ k_force_list_coop(DevParams P0, ListArgs A) {
     const float4 vi = active ? A.vel[s] : make_float4(0.f, 0.f, 0.f, 1.f);
     const int id = active ? A.ids[s] : 0;
     const int cnt_raw = active ? A.nbr_cnt[s] : 0;
-    const float4 xb = active ? A.xbuild[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool exact = A.list_ctrl[kLcExact] != 0u;
+    const bool order_out = A.list_ctrl[kLcDecision] != 0u;  // first step after a build
+    const float4 xb = (active && exact) ? A.xbuild[s] : make_float4(0.f, 0.f, 0.f, 0.f);
     const int hcnt_in = (HIST && active) ? A.hcnt_in[s] : 0;
     const DevParams& P = BATCH ? A.scene_params[scene] : P0;
     const bool frozen = BATCH && active && P.frozen;
@@ -481,7 +778,7 @@ k_force_list_coop(DevParams P0, ListArgs A) {
         q += add;
     }
     if (rounds > 0) coop_flush<HIST, BATCH>(P0, A, W, q, lane, my_count, bstart, reorder, f);
-    uint32_t disp_bits = 0u;
+    uint32_t disp_bits = 0u, step_bits = 0u;
     if (work) {
         if (!listed) {
             // list overflow: this step built the lists, so the run table is fresh
@@ -555,23 +852,25 @@ k_force_list_coop(DevParams P0, ListArgs A) {
                                       fmaf(P.dt, v1.z, pos.z));
         A.pos_out[s] = make_float4(x1.x, x1.y, x1.z, ri);
         A.vel_out[s] = make_float4(v1.x, v1.y, v1.z, mi);
-        A.ids_out[s] = id;
-        if (BATCH) A.scene_out[s] = scene;
+        if (order_out) {
+            A.ids_out[s] = id;
+            if (BATCH) A.scene_out[s] = scene;
+        }
         A.acc_out[s] = make_float4(a.x, a.y, a.z, 0.f);
-        const float ex = x1.x - xb.x, ey = x1.y - xb.y, ez = x1.z - xb.z;
-        const float d2 = ex * ex + ey * ey + ez * ez;
-        disp_bits = d2 >= 0.f ? __float_as_uint(d2) : 0x7f800000u;
+        disp_bits = exact ? disp_sq_bits(x1, xb) : 0u;
+        step_bits = disp_sq_bits(x1, pos);
     } else if (frozen) {
         A.pos_out[s] = pi;
         A.vel_out[s] = vi;
-        A.ids_out[s] = id;
-        A.scene_out[s] = scene;
+        if (order_out) {
+            A.ids_out[s] = id;
+            A.scene_out[s] = scene;
+        }
         A.acc_out[s] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (HIST) A.hcnt_out[s] = 0;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) disp_bits = max(disp_bits, __shfl_xor_sync(0xffffffffu, disp_bits, o));
-    if (lane == 0 && disp_bits != 0u) atomicMax(&A.list_ctrl[kLcDisp], disp_bits);
+    list_disp_report<false>(A.list_ctrl, exact, disp_bits, step_bits);
+    list_tail_decide(A);
 }
 
 __global__ void __launch_bounds__(kBlock)
@@ -585,20 +884,22 @@ k_list_length(int n, const int* __restrict__ cnt, unsigned long long* __restrict
 
 }  // namespace
 
-void launch_list_decide(uint32_t* list_ctrl, float thr_sq, unsigned long long* counters,
+void launch_list_decide(uint32_t* list_ctrl, float thr, bool always_exact,
+                        unsigned long long* counters,
                         bool use_cond, cudaGraphConditionalHandle cond, cudaStream_t st) {
-    k_list_decide<<<1, 32, 0, st>>>(list_ctrl, thr_sq, counters, use_cond ? 1 : 0, cond);
+    k_list_decide<<<1, 32, 0, st>>>(list_ctrl, thr, always_exact ? 1 : 0, counters,
+                                    use_cond ? 1 : 0, cond);
 }
 
 void launch_list_build(const DevParams& P, SceneTab T, const float4* pos, const int2* table,
-                       int* nbr, int* nbr_cnt, float4* xbuild, uint32_t* list_ctrl, Skip skip,
-                       cudaStream_t st) {
+                       int* nbr, int* nbr_cnt, float4* xbuild, uint32_t* list_ctrl,
+                       const ListCopy& cp, Skip skip, cudaStream_t st) {
     if (T.params)
         k_list_build<true><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, table, nbr, nbr_cnt,
-                                                                xbuild, list_ctrl, skip);
+                                                                xbuild, list_ctrl, cp, skip);
     else
         k_list_build<false><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, table, nbr, nbr_cnt,
-                                                                 xbuild, list_ctrl, skip);
+                                                                 xbuild, list_ctrl, cp, skip);
 }
 
 void launch_list_copy(int n, const float4* pos, const float4* vel, const int* ids,
@@ -606,6 +907,26 @@ void launch_list_copy(int n, const float4* pos, const float4* vel, const int* id
                       int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st) {
     k_list_copy<<<blocks_for(n), kBlock, 0, st>>>(n, pos, vel, ids, hcnt, scene, pos_out,
                                                   vel_out, ids_out, hcnt_out, scene_out, skip);
+}
+
+template <bool HIST, bool BATCH>
+void force_list_staged(const DevParams& P, const ListArgs& a, cudaStream_t st) {
+    // persistent: as many blocks as fit at once, at most one warp per tile
+    static int per_sm[8] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& occ = per_sm[dev & 7];
+    if (occ == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_force_list_staged<HIST, BATCH>,
+                                                      kBlock, 0);
+        occ = occ < 1 ? 1 : occ;
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (P.n + kStageTile - 1) / kStageTile;
+    const int want = (tiles + kStageWarps - 1) / kStageWarps;
+    const int nb = want < sms * occ ? want : sms * occ;
+    k_force_list_staged<HIST, BATCH><<<nb < 1 ? 1 : nb, kBlock, 0, st>>>(P, a);
 }
 
 template <int MINB, bool PICARD>
@@ -637,6 +958,18 @@ void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, i
         // the per-lane kernel (the cooperative one has no Picard form)
         if (min_blocks == 4) force_list_variant<4, true>(P, a, st, block == 0 ? kBlock : block);
         else force_list_variant<5, true>(P, a, st, block);
+        return;
+    }
+    if (min_blocks == 1) {
+        // bulk-staged persistent kernel (kBlock threads)
+        const bool batch = a.scene_params != nullptr;
+        if (P.history) {
+            if (batch) force_list_staged<true, true>(P, a, st);
+            else force_list_staged<true, false>(P, a, st);
+        } else {
+            if (batch) force_list_staged<false, true>(P, a, st);
+            else force_list_staged<false, false>(P, a, st);
+        }
         return;
     }
     if (min_blocks == 0) {

@@ -152,6 +152,8 @@ struct wd_sim {
     float4* xbuild = nullptr;
     uint32_t* list_ctrl = nullptr;
     unsigned long long* list_len = nullptr;
+    unsigned* tail_count = nullptr;  // block ticket of the contact kernel's fused decision
+    bool need_build = false;         // host-side change: rebuild before the next step
 
     // reverse pass: snapshots of the step state (checkpoints of a recorded window and
     // the states of the segment being replayed) and the adjoint buffers
@@ -217,6 +219,7 @@ struct wd_sim {
     float wct[4] = {0.f, 0.f, 0.f, 0.f};
     std::vector<cudaEvent_t> ev_pool;
     std::vector<cudaEvent_t> ev_pending;  // triples: t0, t1, t2 per timed step
+    std::vector<uint8_t> ev_contact_first;  // per triple: t0-t1 is the contact phase
 };
 
 namespace {
@@ -340,7 +343,7 @@ void free_sim(wd_sim* s) {
                     s->scene_overflow, s->scene_unstable, s->d_node_seg, s->d_node_chunk,
                     s->node_vals, s->chaos_partials, s->chaos_sums, s->grain_sums,
                     s->chaos_grid, s->nbr, s->nbr_cnt, s->xbuild, s->list_ctrl, s->list_len,
-                    s->xpos, s->xvel, s->xids, s->xscene, s->rhs_vel, s->rhs_ids};
+                    s->tail_count, s->xpos, s->xvel, s->xids, s->xscene, s->rhs_vel, s->rhs_ids};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
@@ -420,6 +423,7 @@ void swap_state(wd_sim* s) {
 // The state changed outside a step: the next step rebuilds the lists.
 cudaError_t request_list_build(wd_sim* s) {
     if (!s->lists) return cudaSuccess;
+    s->need_build = true;
     return cudaMemsetAsync(s->list_ctrl + wd::kLcForce, 1, 1, s->stream);
 }
 
@@ -540,31 +544,21 @@ void enqueue_list_build(wd_sim* s, wd::Skip gate, cudaStream_t st) {
                       hist ? s->hcnt_g : nullptr, batch ? s->sceneA : nullptr,
                       batch ? s->sceneB : nullptr, true, s->counters, s->scene_overflow,
                       s->d_scene_P, gate, st);
+    wd::ListCopy cp{s->velB, s->idsB, hist ? s->hcnt_g : nullptr, batch ? s->sceneB : nullptr,
+                    s->posA, s->velA, s->idsA, hist ? s->hcnt_slot : nullptr,
+                    batch ? s->sceneA : nullptr};
     wd::launch_list_build(P, tab(s, s->sceneB), s->posB, s->sb.table, s->nbr, s->nbr_cnt,
-                          s->xbuild, s->list_ctrl, gate, st);
-    wd::launch_list_copy(s->n, s->posB, s->velB, s->idsB, hist ? s->hcnt_g : nullptr,
-                         batch ? s->sceneB : nullptr, s->posA, s->velA, s->idsA,
-                         hist ? s->hcnt_slot : nullptr, batch ? s->sceneA : nullptr, gate, st);
+                          s->xbuild, s->list_ctrl, cp, gate, st);
 }
 
-// Decide and, when needed, build (an IF node in a graph; gated launches otherwise).
-cudaError_t enqueue_list_decide_build(wd_sim* s, float thr, cudaStream_t st, bool capture) {
-    if (!capture) {
-        wd::launch_list_decide(s->list_ctrl, thr, s->counters, false, 0, st);
-        enqueue_list_build(s, wd::Skip{s->list_ctrl + wd::kLcDecision, 0.5f}, st);
-        return cudaGetLastError();
-    }
+// Inside a capture on st: an IF node on `cond` after everything captured so far, its
+// body the list build of the current A buffers.
+cudaError_t capture_if_build(wd_sim* s, cudaStream_t st, cudaGraphConditionalHandle cond) {
     cudaStreamCaptureStatus status;
     cudaGraph_t graph = nullptr;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
     cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
-    if (e != cudaSuccess) return e;
-    cudaGraphConditionalHandle cond;
-    e = cudaGraphConditionalHandleCreate(&cond, graph, 0, cudaGraphCondAssignDefault);
-    if (e != cudaSuccess) return e;
-    wd::launch_list_decide(s->list_ctrl, thr, s->counters, true, cond, st);
-    e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &ndeps);
     if (e != cudaSuccess) return e;
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
@@ -582,6 +576,30 @@ cudaError_t enqueue_list_decide_build(wd_sim* s, float thr, cudaStream_t st, boo
     e = cudaStreamEndCapture(s->aux_stream, &captured);
     if (e != cudaSuccess) return e;
     return cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+// A conditional handle of the graph being captured on st (reset to 0 every launch).
+cudaError_t capture_cond(cudaStream_t st, cudaGraphConditionalHandle* cond) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, nullptr, nullptr);
+    if (e != cudaSuccess) return e;
+    return cudaGraphConditionalHandleCreate(cond, graph, 0, cudaGraphCondAssignDefault);
+}
+
+// Decide and, when needed, build (an IF node in a graph; gated launches otherwise).
+// thr: the build threshold on max |x - x_build| (m).
+cudaError_t enqueue_list_decide_build(wd_sim* s, float thr, cudaStream_t st, bool capture) {
+    if (!capture) {
+        wd::launch_list_decide(s->list_ctrl, thr, s->picard, s->counters, false, 0, st);
+        enqueue_list_build(s, wd::Skip{s->list_ctrl + wd::kLcDecision, 0.5f}, st);
+        return cudaGetLastError();
+    }
+    cudaGraphConditionalHandle cond;
+    cudaError_t e = capture_cond(st, &cond);
+    if (e != cudaSuccess) return e;
+    wd::launch_list_decide(s->list_ctrl, thr, s->picard, s->counters, true, cond, st);
+    return capture_if_build(s, st, cond);
 }
 
 // Redo of a list-mode Picard step whose iterates left the lists' validity bound: the
@@ -619,7 +637,7 @@ cudaError_t enqueue_step_list_picard(wd_sim* s, int parity, cudaStream_t st, boo
     const DevParams& P = s->P;
     const bool hist = P.history != 0, batch = s->scenes > 1;
     const float build_at = 0.30f * P.skin, valid = 0.45f * P.skin;
-    cudaError_t e = enqueue_list_decide_build(s, build_at * build_at, st, capture);
+    cudaError_t e = enqueue_list_decide_build(s, build_at, st, capture);
     if (e != cudaSuccess) return e;
     if (mid) cudaEventRecord(mid, st);
     e = cudaMemsetAsync(s->picard_res, 0, sizeof(uint32_t) * s->picard_iters, st);
@@ -701,11 +719,16 @@ cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool captu
     if (s->picard) return enqueue_step_list_picard(s, parity, st, capture, mid);
     const DevParams& P = s->P;
     const bool hist = P.history != 0, batch = s->scenes > 1;
-    const float reach = 0.45f * P.skin;
-    cudaError_t e = enqueue_list_decide_build(s, reach * reach, st, capture);
-    if (e != cudaSuccess) return e;
-    if (mid) cudaEventRecord(mid, st);
+    cudaGraphConditionalHandle cond = 0;
+    if (capture) {
+        const cudaError_t e = capture_cond(st, &cond);
+        if (e != cudaSuccess) return e;
+    }
     wd::ListArgs a{};
+    a.thr = 0.45f * P.skin;
+    a.tail_count = s->tail_count;
+    a.use_cond = capture ? 1 : 0;
+    a.cond = cond;
     a.pos = s->posA; a.vel = s->velA; a.ids = s->idsA; a.table = s->sb.table;
     a.pos_out = s->posB; a.vel_out = s->velB; a.ids_out = s->idsB; a.acc_out = s->acc;
     a.hist_in = hist ? s->hist[parity] : nullptr;
@@ -718,7 +741,33 @@ cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool captu
     a.scene = s->sceneA;
     a.scene_out = s->sceneB;
     wd::launch_force_list(P, a, st, s->force_block, s->force_minb);
+    if (mid) cudaEventRecord(mid, st);
+    // the build the kernel's last block decided on, of the new state in B, gathered
+    // through the C buffers: the step's input (A, the rhs getter's velocities and ids)
+    // stays as it is
+    float4 *pa = s->posA, *pb = s->posB, *va = s->velA, *vb = s->velB;
+    int *ia = s->idsA, *ib = s->idsB, *ha = s->hcnt_slot, *hb = s->hcnt_g;
+    int *sa = s->sceneA, *sbn = s->sceneB;
+    s->posA = pb; s->velA = vb; s->idsA = ib; s->hcnt_slot = hb; s->sceneA = sbn;
+    s->posB = s->posC; s->velB = s->velC; s->idsB = s->idsC; s->hcnt_g = ha;
+    s->sceneB = s->sceneC;
+    cudaError_t e = cudaSuccess;
+    if (capture) e = capture_if_build(s, st, cond);
+    else enqueue_list_build(s, wd::Skip{s->list_ctrl + wd::kLcDecision, 0.5f}, st);
+    s->posA = pa; s->posB = pb; s->velA = va; s->velB = vb; s->idsA = ia; s->idsB = ib;
+    s->hcnt_slot = ha; s->hcnt_g = hb; s->sceneA = sa; s->sceneB = sbn;
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
+}
+
+// Before a list-mode step: lists that a host-side change invalidated (creation, state
+// upload, snapshot restore, skin switch) are rebuilt outside the step graph, the build
+// counted and the displacement bound reset by a forced decision.
+cudaError_t enqueue_pending_build(wd_sim* s, cudaStream_t st) {
+    if (!s->need_build) return cudaSuccess;
+    s->need_build = false;
+    if (s->picard) return cudaSuccess;  // the Picard step decides at its start
+    return enqueue_list_decide_build(s, 0.45f * s->P.skin, st, false);
 }
 
 cudaError_t enqueue_any_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
@@ -762,11 +811,13 @@ int flush_timings(wd_sim* s) {
         float a = 0.f, b = 0.f;
         cudaEventElapsedTime(&a, s->ev_pending[i], s->ev_pending[i + 1]);
         cudaEventElapsedTime(&b, s->ev_pending[i + 1], s->ev_pending[i + 2]);
+        if (s->ev_contact_first[i / 3]) std::swap(a, b);
         s->wct[0] += a;
         s->wct[1] += b;
     }
     for (cudaEvent_t e : s->ev_pending) s->ev_pool.push_back(e);
     s->ev_pending.clear();
+    s->ev_contact_first.clear();
     return WD_OK;
 }
 
@@ -784,6 +835,8 @@ cudaEvent_t take_event(wd_sim* s) {
 // Timed step (drivers.kernel_timing): direct launches with events around the
 // search and the contact phase; accumulated lazily, no per-step host sync. Picard
 // interleaves search and contact per iteration, so its whole step counts as contact.
+// A semi-implicit Euler list step runs its contact kernel first and the (gated) list
+// build for the next step after it.
 int timed_step(wd_sim* s, int parity) {
     if (s->ev_pending.size() >= 3 * 256) {
         const int rc = flush_timings(s);
@@ -799,18 +852,24 @@ int timed_step(wd_sim* s, int parity) {
     s->ev_pending.push_back(e0);
     s->ev_pending.push_back(e1);
     s->ev_pending.push_back(e2);
+    s->ev_contact_first.push_back(s->lists && !s->picard ? 1 : 0);
     return WD_OK;
+}
+
+// The C state buffers: on-demand searches and the list build's gather scratch.
+cudaError_t alloc_c_buffers(wd_sim* s) {
+    if (s->posC) return cudaSuccess;
+    cudaError_t e = dalloc(&s->posC, s->n);
+    if (e == cudaSuccess) e = dalloc(&s->velC, s->n);
+    if (e == cudaSuccess) e = dalloc(&s->idsC, s->n);
+    if (e == cudaSuccess && s->scenes > 1) e = dalloc(&s->sceneC, s->n);
+    return e;
 }
 
 // Search on the current state into the C buffers (energy, probes).
 int ondemand_search(wd_sim* s) {
     const bool batch = s->scenes > 1;
-    if (!s->posC) {
-        WD_CUDA(dalloc(&s->posC, s->n));
-        WD_CUDA(dalloc(&s->velC, s->n));
-        WD_CUDA(dalloc(&s->idsC, s->n));
-        if (batch) WD_CUDA(dalloc(&s->sceneC, s->n));
-    }
+    WD_CUDA(alloc_c_buffers(s));
     const wd::Skip none{nullptr, 0.f};
     wd::launch_search(s->P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, none, nullptr, 0,
                       s->counters, s->stream);
@@ -824,6 +883,15 @@ int ondemand_search(wd_sim* s) {
 int sync_stream(wd_sim* s) {
     WD_CUDA(cudaStreamSynchronize(s->stream));
     WD_CUDA(cudaGetLastError());
+    if (s->lists && s->force_minb == 1) {
+        // the bulk-staged contact kernel flags stages that never arrived (bounded waits)
+        unsigned long long stalls = 0;
+        WD_CUDA(cudaMemcpy(&stalls, s->counters + wd::kCntStageTimeout, sizeof(stalls),
+                           cudaMemcpyDeviceToHost));
+        if (stalls)
+            return fail(WD_ERR_CUDA, "contact kernel: a bulk copy into shared memory did not "
+                                     "complete within its wait limit; the state is invalid");
+    }
     return WD_OK;
 }
 
@@ -921,8 +989,13 @@ int alloc_sim(wd_sim* s) {
         WD_CUDA(dalloc(&s->xbuild, n));
         WD_CUDA(dalloc(&s->list_ctrl, wd::kLcWords));
         WD_CUDA(dalloc(&s->list_len, 1));
-        const uint32_t init[wd::kLcWords] = {0u, 0u, 1u, 0u, 0u, 0u};  // the first step builds
+        WD_CUDA(dalloc(&s->tail_count, 1));
+        WD_CUDA(cudaMemset(s->tail_count, 0, sizeof(unsigned)));
+        WD_CUDA(alloc_c_buffers(s));
+        uint32_t init[wd::kLcWords] = {};
+        init[wd::kLcForce] = 1u;  // the first step builds
         WD_CUDA(cudaMemcpy(s->list_ctrl, init, sizeof(init), cudaMemcpyHostToDevice));
+        s->need_build = true;
         if (s->picard) {
             WD_CUDA(dalloc(&s->xpos, n));
             WD_CUDA(dalloc(&s->xvel, n));
@@ -1265,6 +1338,7 @@ int wd_step(wd_sim* sim, int64_t nsteps) {
     if (!sim || nsteps < 0) return fail(WD_ERR_INVALID, "wd_step: bad argument");
     for (int64_t k = 0; k < nsteps; ++k) {
         const int parity = sim->lists ? sim->lpar : (sim->P.history ? sim->hist_cur : 0);
+        if (sim->lists) WD_CUDA(enqueue_pending_build(sim, sim->stream));
         if (sim->cfg.kernel_timing) {
             const int rc = timed_step(sim, parity);
             if (rc) return rc;
@@ -1726,9 +1800,10 @@ int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
     if (!sim || !kernels) return fail(WD_ERR_INVALID, "wd_kernels_per_step: NULL argument");
     // keys, mover kernel, merge, gather, contact per search; a search that takes the
     // radix path adds 1 + 3 per pass (wd_radix_search_count)
-    // list mode: the decision and the contact kernel; builds add wd_list_stats' count
-    // (Picard: the decision, the iterations, the last iterate's copy, the redo check)
-    *kernels = sim->lists ? (sim->picard ? sim->picard_iters + 3 : 2)
+    // list mode: the contact kernel (its last block decides the next build); builds add
+    // wd_list_stats' count (Picard: the decision, the iterations, the last iterate's
+    // copy, the redo check)
+    *kernels = sim->lists ? (sim->picard ? sim->picard_iters + 3 : 1)
                           : static_cast<int64_t>(5) * sim->picard_iters;
     return WD_OK;
 }
@@ -1808,7 +1883,10 @@ static int apply_skin(wd_sim* s, float skin) {
         WD_CUDA(dalloc(&s->xbuild, n));
         WD_CUDA(dalloc(&s->list_ctrl, wd::kLcWords));
         WD_CUDA(dalloc(&s->list_len, 1));
+        WD_CUDA(dalloc(&s->tail_count, 1));
+        WD_CUDA(alloc_c_buffers(s));
         WD_CUDA(cudaMemsetAsync(s->list_ctrl, 0, sizeof(uint32_t) * wd::kLcWords, s->stream));
+        WD_CUDA(cudaMemsetAsync(s->tail_count, 0, sizeof(unsigned), s->stream));
     }
     if (lists && s->picard && !s->xpos) {
         const int n = s->n;
@@ -1850,15 +1928,21 @@ static std::string tune_key(const wd_sim* s) {
     return buf;
 }
 
-int wd_picard_redo_count(wd_sim* sim, int64_t* redos) {
-    if (!sim || !redos) return fail(WD_ERR_INVALID, "wd_picard_redo_count: NULL argument");
-    return read_counter(sim, wd::kCntPicardRedos, redos);
+int wd_picard_counts(wd_sim* sim, int64_t* iterations, int64_t* redos) {
+    if (!sim || !iterations || !redos) return fail(WD_ERR_INVALID, "wd_picard_counts: NULL argument");
+    const int rc = read_counter(sim, wd::kCntPicardIters, iterations);
+    return rc ? rc : read_counter(sim, wd::kCntPicardRedos, redos);
+}
+
+int wd_list_exact_count(wd_sim* sim, int64_t* steps) {
+    if (!sim || !steps) return fail(WD_ERR_INVALID, "wd_list_exact_count: NULL argument");
+    return read_counter(sim, wd::kCntListExact, steps);
 }
 
 int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_list_stats: NULL handle");
     if (kernels_each)
-        *kernels_each = sim->lists ? 2 + (1 + 3 * sim->sb.passes) + 1 + 3 : 0;
+        *kernels_each = sim->lists ? 2 + (1 + 3 * sim->sb.passes) + 1 + 2 : 0;
     if (builds) {
         int rc = read_counter(sim, wd::kCntListBuilds, builds);
         if (rc) return rc;
@@ -1981,8 +2065,9 @@ cudaError_t run_adj_graph(wd_sim* s, int len, int parity) {
 int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_get_tuning: NULL handle");
     if (skin) *skin = sim->cfg.neighbor_skin;
-    if (block) *block = sim->force_minb == 0 ? wd::kBlock : sim->force_block;
-    if (variant) *variant = sim->force_minb == 0 ? 0 : (sim->force_minb == 4 ? 64 : 48);
+    if (block) *block = sim->force_minb <= 1 ? wd::kBlock : sim->force_block;
+    if (variant)
+        *variant = sim->force_minb == 0 ? 0 : sim->force_minb == 1 ? 1 : (sim->force_minb == 4 ? 64 : 48);
     return WD_OK;
 }
 
@@ -1990,12 +2075,12 @@ int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_set_contact_kernel: NULL handle");
     if (block < 32 || block > wd::kBlock || block % 32)
         return fail(WD_ERR_INVALID, "wd_set_contact_kernel: block must be a multiple of 32 up to 256");
-    if (variant != 48 && variant != 64 && variant != 0)
-        return fail(WD_ERR_INVALID, "wd_set_contact_kernel: variant must be 48, 64 or 0");
+    if (variant != 48 && variant != 64 && variant != 0 && variant != 1)
+        return fail(WD_ERR_INVALID, "wd_set_contact_kernel: variant must be 48, 64, 0 or 1");
     int rc = sync_stream(sim);
     if (rc) return rc;
     sim->force_block = block;
-    sim->force_minb = variant == 0 ? 0 : (variant == 64 ? 4 : 5);
+    sim->force_minb = variant == 0 ? 0 : variant == 1 ? 1 : (variant == 64 ? 4 : 5);
     sim->graph_dirty = true;
     clear_adj_graphs(sim);
     return WD_OK;
@@ -2026,7 +2111,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
                 if (std::sscanf(line, "%299s %f %d %d", k, &sk, &bl, &mb) >= 3 && key == k) {
                     best_skin = sk;
                     best_block = bl;
-                    best_minb = (mb == 4 || mb == 0) ? mb : 5;
+                    best_minb = (mb == 4 || mb == 0 || mb == 1) ? mb : 5;
                     cached = true;
                 }
             }
@@ -2045,8 +2130,9 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         std::vector<float> skins = {0.f};
         for (float f : {0.05f, 0.1f, 0.2f, 0.4f}) skins.push_back(f * d);
         // (block, variant): variant 5 / 4 = per-lane list kernel with 48 / 64 registers,
-        // 0 = warp-cooperative list kernel (256 threads)
-        const int cands[][2] = {{128, 5}, {256, 5}, {128, 4}, {256, 4}, {256, 0}};
+        // 0 = warp-cooperative list kernel, 1 = bulk-staged persistent list kernel (256
+        // threads each)
+        const int cands[][2] = {{128, 5}, {256, 5}, {128, 4}, {256, 4}, {256, 0}, {256, 1}};
         wd_sim::Snap snap;
         WD_CUDA(alloc_snap(sim, snap));
         WD_CUDA(take_snap(sim, snap));
@@ -2057,11 +2143,11 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         cudaEventCreate(&e1);
         float best_ms = INFINITY;
         for (float sk : skins) {
-            for (int cand = 0; cand < 5 && rc == WD_OK; ++cand) {
+            for (int cand = 0; cand < 6 && rc == WD_OK; ++cand) {
                 const int bl = cands[cand][0];
                 const int mb = cands[cand][1];
                 if (sk == 0.f && mb != 5) continue;  // the searched kernel has one variant
-                if (sim->picard && mb == 0) continue;  // no cooperative Picard kernel
+                if (sim->picard && mb <= 1) continue;  // Picard: the per-lane kernel only
                 rc = apply_skin(sim, sk);
                 if (rc == WD_OK) {
                     sim->force_block = bl;

@@ -342,24 +342,34 @@ class ParticleDynamics:
 
     def tuning(self) -> dict:
         """The current schedule: neighbor skin (m), contact-kernel block size, and the
-        list contact kernel's registers per thread."""
+        list contact kernel's variant."""
         sk = ctypes.c_float()
         bl = ctypes.c_int32()
         rg = ctypes.c_int32()
         check(lib.wd_get_tuning(self._h, ctypes.byref(sk), ctypes.byref(bl), ctypes.byref(rg)))
         return {"neighbor_skin_m": float(sk.value), "contact_block": int(bl.value),
-                "contact_variant": {0: "warp-cooperative", 48: "per-lane, 48 registers",
+                "contact_variant": {0: "warp-cooperative", 1: "bulk-staged persistent",
+                                    48: "per-lane, 48 registers",
                                     64: "per-lane, 64 registers"}.get(int(rg.value), str(rg.value))}
 
     def set_contact_kernel(self, block: int = 256, variant: int = 48) -> None:
         """Contact-kernel block size and list-kernel variant (48 / 64: per-lane with that
-        many registers, 0: warp-cooperative); results do not depend on them."""
+        many registers, 0: warp-cooperative, 1: bulk-staged persistent, whose per-slot
+        arrays arrive in shared memory by bulk copies); results do not depend on them."""
         check(lib.wd_set_contact_kernel(self._h, int(block), int(variant)))
 
-    def picard_redo_count(self) -> int:
-        """Picard steps on lists redone with the per-iteration search so far."""
+    def picard_counts(self) -> tuple[int, int]:
+        """(Picard iterations executed, list-mode steps redone with the per-iteration
+        search) so far."""
+        it, redo = ctypes.c_int64(), ctypes.c_int64()
+        check(lib.wd_picard_counts(self._h, ctypes.byref(it), ctypes.byref(redo)))
+        return int(it.value), int(redo.value)
+
+    def list_exact_count(self) -> int:
+        """Steps so far whose contact kernel measured the exact displacement since the
+        last list build (the others decide on a bound and read no build positions)."""
         v = ctypes.c_int64()
-        check(lib.wd_picard_redo_count(self._h, ctypes.byref(v)))
+        check(lib.wd_list_exact_count(self._h, ctypes.byref(v)))
         return int(v.value)
 
     def list_stats(self) -> tuple[int, int, float]:
