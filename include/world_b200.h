@@ -278,10 +278,10 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
                 int32_t* block_out);
 /* The current schedule: neighbor skin, contact-kernel block size, and the list
  * contact kernel variant: 48 or 64 (registers per thread of the per-lane kernel), 0
- * (the warp-cooperative kernel, 256 threads) or 1 (the bulk-staged persistent kernel,
- * 256 threads: per-slot arrays copied into shared memory by cp.async.bulk two tiles
- * ahead). wd_set_contact_kernel sets the last two (the autotuner's other choices);
- * results do not depend on them. */
+ * (the warp-cooperative kernel, 256 threads) or 1 / 2 (the bulk-staged persistent
+ * kernel, 256 threads, 48 / 64 registers: per-slot arrays copied into shared memory by
+ * cp.async.bulk two tiles ahead). wd_set_contact_kernel sets the last two (the
+ * autotuner's other choices); results do not depend on them. */
 int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant);
 int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant);
 /* Verlet lists: steps so far whose contact kernel measured the exact displacement

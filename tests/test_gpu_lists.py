@@ -182,7 +182,7 @@ def test_autotune_restores_the_state_and_caches(tmp_path):
     assert len(cache.read_text().splitlines()) == 1
 
 
-@pytest.mark.parametrize("variant,block", [(0, 256), (64, 128), (48, 64), (1, 256)])
+@pytest.mark.parametrize("variant,block", [(0, 256), (64, 128), (48, 64), (1, 256), (2, 256)])
 def test_every_contact_kernel_variant_is_exact(variant, block):
     cfg, st, rad = packed_poly(n=2500, seed=28, mu=0.5)
     cfg.kernel_timing = False

@@ -185,7 +185,8 @@ __device__ __forceinline__ void wall_forces(const DevParams& P, float3 pos, floa
                                             float ri, float mi, float3& f, HistRow& h,
                                             unsigned long long* counters) {
     const float k = P.k_n, F = P.max_force;
-    const float c_wall = damping(P, mi);
+    // the dashpot coefficient only where a wall is touched (most grains touch none)
+    auto c_wall = [&]() { return damping(P, mi); };
     f.z = fmaf(-mi, P.gravity, f.z);
     const float p3[3] = {pos.x, pos.y, pos.z};
     const float v3[3] = {vel.x, vel.y, vel.z};
@@ -199,14 +200,15 @@ __device__ __forceinline__ void wall_forces(const DevParams& P, float3 pos, floa
         fa = fa + fl;
         if (a == 0) f.x = fa; else if (a == 1) f.y = fa; else f.z = fa;
         if (dl < 0.f) {
-            fa = fmaf(-c_wall, v3[a], fa);
+            const float cw = c_wall();
+            fa = fmaf(-cw, v3[a], fa);
             if (a == 0) f.x = fa; else if (a == 1) f.y = fa; else f.z = fa;
             if (HIST) {
                 const float3 nrm = make_float3(a == 0 ? 1.f : 0.f, a == 1 ? 1.f : 0.f,
                                                a == 2 ? 1.f : 0.f);
                 spring_friction(P, f, vt, nrm, P.mu * fl, -1 - 2 * a, h, counters);
             } else {
-                viscous_friction(f, vt, P.mu * fl, c_wall);
+                viscous_friction(f, vt, P.mu * fl, cw);
             }
         }
         fa = a == 0 ? f.x : (a == 1 ? f.y : f.z);
@@ -215,14 +217,15 @@ __device__ __forceinline__ void wall_forces(const DevParams& P, float3 pos, floa
         fa = fa - fu;
         if (a == 0) f.x = fa; else if (a == 1) f.y = fa; else f.z = fa;
         if (du < 0.f) {
-            fa = fmaf(-c_wall, v3[a], fa);
+            const float cw = c_wall();
+            fa = fmaf(-cw, v3[a], fa);
             if (a == 0) f.x = fa; else if (a == 1) f.y = fa; else f.z = fa;
             if (HIST) {
                 const float3 nrm = make_float3(a == 0 ? -1.f : 0.f, a == 1 ? -1.f : 0.f,
                                                a == 2 ? -1.f : 0.f);
                 spring_friction(P, f, vt, nrm, P.mu * fu, -2 - 2 * a, h, counters);
             } else {
-                viscous_friction(f, vt, P.mu * fu, c_wall);
+                viscous_friction(f, vt, P.mu * fu, cw);
             }
         }
     }

@@ -176,8 +176,8 @@ void launch_list_copy(int n, const float4* pos, const float4* vel, const int* id
                       const int* hcnt, const int* scene, float4* pos_out, float4* vel_out,
                       int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st);
 // min_blocks: the kernel variant. 5 / 4: per-lane kernel with 48 / 64 registers per
-// thread; 0: warp-cooperative; 1: bulk-staged persistent (kBlock threads). Picard runs
-// the per-lane kernel (4 or 5).
+// thread; 0: warp-cooperative; 1 / 2: bulk-staged persistent (kBlock threads) with 48
+// / 64 registers. Picard runs the per-lane kernel (4 or 5).
 void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st,
                        int block = kBlock, int min_blocks = 5, bool picard = false);
 // Picard with lists: the last iterate into the B buffers when the last executed

@@ -218,6 +218,77 @@ __device__ __forceinline__ void list_disp_report(uint32_t* ctrl, bool exact, uin
     }
 }
 
+// The contacts of a grain whose list entries a cell crossing re-ordered, in canonical
+// order: each pass takes the smallest visiting key above the last. (Inlined: an
+// out-of-line call copies the parameter structs to local memory at kernel entry, which
+// was measured to cost more than the code it moves away.)
+template <bool HIST>
+__device__ __forceinline__ void list_contacts_sorted(const DevParams& P, const ListArgs& A, int s,
+                                                  int n, int cnt, float4 pi, float3 vel,
+                                                  float mi, float cut, int cx, int cy, int cz,
+                                                  float3& f, HistRow& h) {
+    const float ri = pi.w;
+    long long done = -1;
+    for (;;) {
+        long long best = 0x7fffffffffffffffll;
+        int bj = -1;
+        for (int e = 0; e < cnt; ++e) {
+            const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+            const float4 pj = __ldg(&A.pos[j]);
+            float3 d;
+            const float ns = pair_norm_sq(pi, pj, d);
+            if (ns > cut) continue;
+            const float dist = pair_dist(sqrtf(ns), ri, pj.w);
+            if (!(dist < 0.f)) continue;
+            const long long key =
+                static_cast<long long>(visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j])));
+            if (key > done && key < best) {
+                best = key;
+                bj = j;
+            }
+        }
+        if (bj < 0) break;
+        done = best;
+        const float4 pj = __ldg(&A.pos[bj]);
+        float3 d;
+        const float ns = pair_norm_sq(pi, pj, d);
+        const float norm = sqrtf(ns);
+        const float dist = pair_dist(norm, ri, pj.w);
+        const float4 vj = __ldg(&A.vel[bj]);
+        pair_force<HIST>(P, d, norm, dist, vel, mi, vj, static_cast<int>(best & 0xffffffffll),
+                         f, h, A.counters);
+    }
+}
+
+// The contacts of a grain whose list overflowed, from the run table of the build that
+// ran this step (the stencil walk of the searched kernel).
+template <bool HIST>
+__device__ __forceinline__ void list_contacts_table(const DevParams& P, const ListArgs& A, int s,
+                                                 float4 pi, float3 vel, float mi, float cut,
+                                                 int cx, int cy, int cz, float3& f, HistRow& h) {
+    const float ri = pi.w;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int nx = cx + dx;
+        if (nx < 0 || nx >= P.grid[0]) continue;
+        int lo[3], hi[3];
+        row_ranges(P, A.table, nx, cy, cz, lo, hi);
+        for (int t = 0; t < 3; ++t) {
+            for (int j = lo[t]; j < hi[t]; ++j) {
+                const float4 pj = __ldg(&A.pos[j]);
+                float3 d;
+                const float ns = pair_norm_sq(pi, pj, d);
+                if (ns > cut || j == s) continue;
+                const float norm = sqrtf(ns);
+                const float dist = pair_dist(norm, ri, pj.w);
+                if (!(dist < 0.f)) continue;
+                const float4 vj = __ldg(&A.vel[j]);
+                const int partner = HIST ? __ldg(&A.ids[j]) : 0;
+                pair_force<HIST>(P, d, norm, dist, vel, mi, vj, partner, f, h, A.counters);
+            }
+        }
+    }
+}
+
 // One grain of the list contact kernels, its per-slot values already loaded: contacts
 // from the list in canonical order (or the run table when the list overflowed), the
 // integrator, the displacement measures (maxima folded into disp_bits / step_bits /
@@ -265,8 +336,9 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
         const float3 f_walls = f;
         const int out_walls = HIST ? h.out_count : 0;
         const float cut = contact_cutoff_sq(ri, P.rmax);
-        int cx, cy, cz;
-        cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+        // the grain's cell orders its contacts; a grain without list entries needs none
+        int cx = 0, cy = 0, cz = 0;
+        if (cnt > 0) cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
         bool ordered = true;
         if (cnt <= kNbrCap) {
             // the list, in its build order, while the contacts arrive in canonical order
@@ -292,63 +364,14 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
             }
             if (!ordered) {
                 // a cell crossing re-ordered this grain's contacts: redo them in
-                // canonical order, each pass taking the smallest key above the last
+                // canonical order
                 f = f_walls;
                 if (HIST) h.out_count = out_walls;
-                long long done = -1;
-                for (;;) {
-                    long long best = 0x7fffffffffffffffll;
-                    int bj = -1;
-                    for (int e = 0; e < cnt; ++e) {
-                        const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
-                        const float4 pj = __ldg(&A.pos[j]);
-                        float3 d;
-                        const float ns = pair_norm_sq(pi, pj, d);
-                        if (ns > cut) continue;
-                        const float dist = pair_dist(sqrtf(ns), ri, pj.w);
-                        if (!(dist < 0.f)) continue;
-                        const long long key = static_cast<long long>(
-                            visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j])));
-                        if (key > done && key < best) {
-                            best = key;
-                            bj = j;
-                        }
-                    }
-                    if (bj < 0) break;
-                    done = best;
-                    const float4 pj = __ldg(&A.pos[bj]);
-                    float3 d;
-                    const float ns = pair_norm_sq(pi, pj, d);
-                    const float norm = sqrtf(ns);
-                    const float dist = pair_dist(norm, ri, pj.w);
-                    const float4 vj = __ldg(&A.vel[bj]);
-                    pair_force<HIST>(P, d, norm, dist, vel, mi, vj,
-                                     static_cast<int>(best & 0xffffffffll), f, h, A.counters);
-                }
+                list_contacts_sorted<HIST>(P, A, s, n, cnt, pi, vel, mi, cut, cx, cy, cz, f, h);
             }
         } else {
             // list overflow: this step built the lists, so the run table is fresh
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int nx = cx + dx;
-                if (nx < 0 || nx >= P.grid[0]) continue;
-                int lo[3], hi[3];
-                row_ranges(P, A.table, nx, cy, cz, lo, hi);
-                for (int t = 0; t < 3; ++t) {
-                    for (int j = lo[t]; j < hi[t]; ++j) {
-                        const float4 pj = __ldg(&A.pos[j]);
-                        float3 d;
-                        const float ns = pair_norm_sq(pi, pj, d);
-                        if (ns > cut || j == s) continue;
-                        const float norm = sqrtf(ns);
-                        const float dist = pair_dist(norm, ri, pj.w);
-                        if (!(dist < 0.f)) continue;
-                        const float4 vj = __ldg(&A.vel[j]);
-                        const int partner = HIST ? __ldg(&A.ids[j]) : 0;
-                        pair_force<HIST>(P, d, norm, dist, vel, mi, vj, partner, f, h,
-                                         A.counters);
-                    }
-                }
-            }
+            list_contacts_table<HIST>(P, A, s, pi, vel, mi, cut, cx, cy, cz, f, h);
         }
         if (HIST) A.hcnt_out[s] = h.out_count;
         const float3 a = make_float3(f.x / mi, f.y / mi, f.z / mi);
@@ -517,8 +540,12 @@ __device__ __forceinline__ void stage_issue(const ListArgs& A, int tile, bool ex
     if (exact) bulk_g2s(S.xb, A.xbuild + s0, f4, bar);
 }
 
-template <bool HIST, bool BATCH>
-__global__ void __launch_bounds__(kBlock, 5)
+// MINB: resident blocks per SM (5: 48 registers per thread, 4: 64). Tiles: warp w of W
+// takes tiles w, w + W, w + 2W, ... (claiming the last rounds from a shared counter
+// instead was measured slower: the claims serialize on one address just when every
+// warp needs its next tile).
+template <bool HIST, bool BATCH, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB)
 k_force_list_staged(DevParams P0, ListArgs A) {
     __shared__ SlotStage stage[kStageWarps][2];
     __shared__ uint64_t bars[kStageWarps][2];
@@ -532,22 +559,26 @@ k_force_list_staged(DevParams P0, ListArgs A) {
     const bool order_out = A.list_ctrl[kLcDecision] != 0u;  // first step after a build
     SlotStage* S = stage[w];
     uint64_t* bar = bars[w];
+    // tiles of iterations it (cur, in stage it & 1) and it + 1 (nxt), in registers
+    int cur = first, nxt = first + W;
     if (lane == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         mbar_init_fence();
-        for (int k = 0; k < 2; ++k)
-            if (first + k * W < whole) stage_issue<HIST, BATCH>(A, first + k * W, exact, S[k], &bar[k]);
+        if (cur < whole) stage_issue<HIST, BATCH>(A, cur, exact, S[0], &bar[0]);
+        if (nxt < whole) stage_issue<HIST, BATCH>(A, nxt, exact, S[1], &bar[1]);
     }
     __syncwarp();
     uint32_t disp_bits = 0u, step_bits = 0u, res_bits = 0u;
     bool viol = false, failed = false;
     int it = 0;
-    for (int t = first; t < tiles; t += W, ++it) {
+    for (;; ++it) {
         const int st = it & 1;
+        const int t = cur;
+        if (t >= tiles) break;
         const int s = t * kStageTile + lane;
-        float4 pi, vi, xb = make_float4(0.f, 0.f, 0.f, 0.f);
-        int id, cnt, hcnt_in = 0, scene = 0;
+        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f), vi = pi, xb = pi;
+        int id = 0, cnt = 0, hcnt_in = 0, scene = 0;
         if (t < whole) {
             const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar[st], (it >> 1) & 1));
             if (!ok) {
@@ -564,31 +595,36 @@ k_force_list_staged(DevParams P0, ListArgs A) {
             if (exact) xb = T.xb[lane];
             __syncwarp();
             // the stage is read: refill it with the tile two ahead
-            if (lane == 0 && t + 2 * W < whole)
-                stage_issue<HIST, BATCH>(A, t + 2 * W, exact, S[st], &bar[st]);
+            const int tn = nxt + W;
+            if (lane == 0 && tn < whole) stage_issue<HIST, BATCH>(A, tn, exact, S[st], &bar[st]);
+            cur = nxt;
+            nxt = tn;
         } else {
-            // the ragged last tile: plain loads
-            if (s >= n) break;
-            pi = A.pos[s];
-            vi = A.vel[s];
-            id = A.ids[s];
-            cnt = A.nbr_cnt[s];
-            if (HIST) hcnt_in = A.hcnt_in[s];
-            if (BATCH) scene = A.scene[s];
-            if (exact) xb = A.xbuild[s];
+            // the ragged last tile: plain loads, nothing after it
+            cur = nxt;
+            nxt = tiles;
+            if (s < n) {
+                pi = A.pos[s];
+                vi = A.vel[s];
+                id = A.ids[s];
+                cnt = A.nbr_cnt[s];
+                if (HIST) hcnt_in = A.hcnt_in[s];
+                if (BATCH) scene = A.scene[s];
+                if (exact) xb = A.xbuild[s];
+            }
         }
-        list_grain<HIST, BATCH, false>(P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in, exact,
-                                       order_out, disp_bits, step_bits, res_bits, viol);
+        if (s < n)
+            list_grain<HIST, BATCH, false>(P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in,
+                                           exact, order_out, disp_bits, step_bits, res_bits,
+                                           viol);
     }
     if (failed) {
         // a stage never completed: flag it and drain what this warp still has in flight
         // (bounded); the step is left unfinished for the host to report
         if (lane == 0) {
             atomicAdd(&A.counters[kCntStageTimeout], 1ull);
-            for (int k = 0; k < 2; ++k) {
-                const int t = first + (it + k) * W;
-                if (t < whole) mbar_wait(&bar[(it + k) & 1], ((it + k) >> 1) & 1);
-            }
+            if (cur < whole) mbar_wait(&bar[it & 1], (it >> 1) & 1);
+            if (nxt < whole) mbar_wait(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
         }
     } else {
         list_disp_report<false>(A.list_ctrl, exact, disp_bits, step_bits);
@@ -909,7 +945,7 @@ void launch_list_copy(int n, const float4* pos, const float4* vel, const int* id
                                                   vel_out, ids_out, hcnt_out, scene_out, skip);
 }
 
-template <bool HIST, bool BATCH>
+template <bool HIST, bool BATCH, int MINB>
 void force_list_staged(const DevParams& P, const ListArgs& a, cudaStream_t st) {
     // persistent: as many blocks as fit at once, at most one warp per tile
     static int per_sm[8] = {};
@@ -917,8 +953,8 @@ void force_list_staged(const DevParams& P, const ListArgs& a, cudaStream_t st) {
     cudaGetDevice(&dev);
     int& occ = per_sm[dev & 7];
     if (occ == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_force_list_staged<HIST, BATCH>,
-                                                      kBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &occ, k_force_list_staged<HIST, BATCH, MINB>, kBlock, 0);
         occ = occ < 1 ? 1 : occ;
     }
     int sms = 0;
@@ -926,7 +962,7 @@ void force_list_staged(const DevParams& P, const ListArgs& a, cudaStream_t st) {
     const int tiles = (P.n + kStageTile - 1) / kStageTile;
     const int want = (tiles + kStageWarps - 1) / kStageWarps;
     const int nb = want < sms * occ ? want : sms * occ;
-    k_force_list_staged<HIST, BATCH><<<nb < 1 ? 1 : nb, kBlock, 0, st>>>(P, a);
+    k_force_list_staged<HIST, BATCH, MINB><<<nb < 1 ? 1 : nb, kBlock, 0, st>>>(P, a);
 }
 
 template <int MINB, bool PICARD>
@@ -960,15 +996,16 @@ void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, i
         else force_list_variant<5, true>(P, a, st, block);
         return;
     }
-    if (min_blocks == 1) {
-        // bulk-staged persistent kernel (kBlock threads)
+    if (min_blocks == 1 || min_blocks == 2) {
+        // bulk-staged persistent kernel (kBlock threads; 1: 48 registers, 2: 64)
         const bool batch = a.scene_params != nullptr;
+        const bool r64 = min_blocks == 2;
         if (P.history) {
-            if (batch) force_list_staged<true, true>(P, a, st);
-            else force_list_staged<true, false>(P, a, st);
+            if (batch) r64 ? force_list_staged<true, true, 4>(P, a, st) : force_list_staged<true, true, 5>(P, a, st);
+            else r64 ? force_list_staged<true, false, 4>(P, a, st) : force_list_staged<true, false, 5>(P, a, st);
         } else {
-            if (batch) force_list_staged<false, true>(P, a, st);
-            else force_list_staged<false, false>(P, a, st);
+            if (batch) r64 ? force_list_staged<false, true, 4>(P, a, st) : force_list_staged<false, true, 5>(P, a, st);
+            else r64 ? force_list_staged<false, false, 4>(P, a, st) : force_list_staged<false, false, 5>(P, a, st);
         }
         return;
     }

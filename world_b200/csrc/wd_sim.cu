@@ -139,7 +139,7 @@ struct wd_sim {
     bool lists = false;
     int lpar = 0;
     int force_block = wd::kBlock;   // threads per block of the contact kernel
-    int force_minb = 5;             // register variant of the list contact kernel
+    int force_minb = 1;             // list contact kernel variant (1: bulk-staged)
     // Picard with lists: scratch iterate buffers (and, for a redo's gather, ids / scenes)
     float4* xpos = nullptr;
     float4* xvel = nullptr;
@@ -2065,9 +2065,9 @@ cudaError_t run_adj_graph(wd_sim* s, int len, int parity) {
 int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_get_tuning: NULL handle");
     if (skin) *skin = sim->cfg.neighbor_skin;
-    if (block) *block = sim->force_minb <= 1 ? wd::kBlock : sim->force_block;
+    if (block) *block = sim->force_minb <= 2 ? wd::kBlock : sim->force_block;
     if (variant)
-        *variant = sim->force_minb == 0 ? 0 : sim->force_minb == 1 ? 1 : (sim->force_minb == 4 ? 64 : 48);
+        *variant = sim->force_minb <= 2 ? sim->force_minb : (sim->force_minb == 4 ? 64 : 48);
     return WD_OK;
 }
 
@@ -2075,12 +2075,12 @@ int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_set_contact_kernel: NULL handle");
     if (block < 32 || block > wd::kBlock || block % 32)
         return fail(WD_ERR_INVALID, "wd_set_contact_kernel: block must be a multiple of 32 up to 256");
-    if (variant != 48 && variant != 64 && variant != 0 && variant != 1)
-        return fail(WD_ERR_INVALID, "wd_set_contact_kernel: variant must be 48, 64, 0 or 1");
+    if (variant != 48 && variant != 64 && (variant < 0 || variant > 2))
+        return fail(WD_ERR_INVALID, "wd_set_contact_kernel: variant must be 48, 64, 0, 1 or 2");
     int rc = sync_stream(sim);
     if (rc) return rc;
     sim->force_block = block;
-    sim->force_minb = variant == 0 ? 0 : variant == 1 ? 1 : (variant == 64 ? 4 : 5);
+    sim->force_minb = variant <= 2 ? variant : (variant == 64 ? 4 : 5);
     sim->graph_dirty = true;
     clear_adj_graphs(sim);
     return WD_OK;
@@ -2111,7 +2111,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
                 if (std::sscanf(line, "%299s %f %d %d", k, &sk, &bl, &mb) >= 3 && key == k) {
                     best_skin = sk;
                     best_block = bl;
-                    best_minb = (mb == 4 || mb == 0 || mb == 1) ? mb : 5;
+                    best_minb = (mb == 4 || (mb >= 0 && mb <= 2)) ? mb : 5;
                     cached = true;
                 }
             }
@@ -2130,9 +2130,11 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         std::vector<float> skins = {0.f};
         for (float f : {0.05f, 0.1f, 0.2f, 0.4f}) skins.push_back(f * d);
         // (block, variant): variant 5 / 4 = per-lane list kernel with 48 / 64 registers,
-        // 0 = warp-cooperative list kernel, 1 = bulk-staged persistent list kernel (256
-        // threads each)
-        const int cands[][2] = {{128, 5}, {256, 5}, {128, 4}, {256, 4}, {256, 0}, {256, 1}};
+        // 0 = warp-cooperative list kernel, 1 / 2 = bulk-staged persistent list kernel
+        // with 48 / 64 registers (256 threads each)
+        const int cands[][2] = {{128, 5}, {256, 5}, {128, 4}, {256, 4}, {256, 0}, {256, 1},
+                                {256, 2}};
+        const int ncands = static_cast<int>(sizeof(cands) / sizeof(cands[0]));
         wd_sim::Snap snap;
         WD_CUDA(alloc_snap(sim, snap));
         WD_CUDA(take_snap(sim, snap));
@@ -2143,11 +2145,11 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         cudaEventCreate(&e1);
         float best_ms = INFINITY;
         for (float sk : skins) {
-            for (int cand = 0; cand < 6 && rc == WD_OK; ++cand) {
+            for (int cand = 0; cand < ncands && rc == WD_OK; ++cand) {
                 const int bl = cands[cand][0];
                 const int mb = cands[cand][1];
                 if (sk == 0.f && mb != 5) continue;  // the searched kernel has one variant
-                if (sim->picard && mb <= 1) continue;  // Picard: the per-lane kernel only
+                if (sim->picard && mb <= 2) continue;  // Picard: the per-lane kernel only
                 rc = apply_skin(sim, sk);
                 if (rc == WD_OK) {
                     sim->force_block = bl;

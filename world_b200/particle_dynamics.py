@@ -348,14 +348,17 @@ class ParticleDynamics:
         rg = ctypes.c_int32()
         check(lib.wd_get_tuning(self._h, ctypes.byref(sk), ctypes.byref(bl), ctypes.byref(rg)))
         return {"neighbor_skin_m": float(sk.value), "contact_block": int(bl.value),
-                "contact_variant": {0: "warp-cooperative", 1: "bulk-staged persistent",
+                "contact_variant": {0: "warp-cooperative",
+                                    1: "bulk-staged persistent, 48 registers",
+                                    2: "bulk-staged persistent, 64 registers",
                                     48: "per-lane, 48 registers",
                                     64: "per-lane, 64 registers"}.get(int(rg.value), str(rg.value))}
 
     def set_contact_kernel(self, block: int = 256, variant: int = 48) -> None:
         """Contact-kernel block size and list-kernel variant (48 / 64: per-lane with that
-        many registers, 0: warp-cooperative, 1: bulk-staged persistent, whose per-slot
-        arrays arrive in shared memory by bulk copies); results do not depend on them."""
+        many registers, 0: warp-cooperative, 1 / 2: bulk-staged persistent with 48 / 64
+        registers, whose per-slot arrays arrive in shared memory by bulk copies); results
+        do not depend on them."""
         check(lib.wd_set_contact_kernel(self._h, int(block), int(variant)))
 
     def picard_counts(self) -> tuple[int, int]:
