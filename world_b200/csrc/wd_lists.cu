@@ -22,6 +22,8 @@
 // 0.30 skin instead of 0.45, and each iteration checks that its input iterate is still
 // within 0.45 skin of the build; if one is not, the step is redone from its start
 // state with the per-iteration search, so the results stay those of the searched step.
+#include <algorithm>
+
 #include "wd_kernels.h"
 
 namespace wd {
@@ -292,15 +294,16 @@ __device__ __forceinline__ void list_contacts_table(const DevParams& P, const Li
 // One grain of the list contact kernels, its per-slot values already loaded: contacts
 // from the list in canonical order (or the run table when the list overflowed), the
 // integrator, the displacement measures (maxima folded into disp_bits / step_bits /
-// res_bits, viol or-ed). order_out: write the slot's id (and scene) too. Between builds
+// res_bits, viol or-ed). warp_listed: some grain of the calling warp has a list entry
+// (warp-uniform). order_out: write the slot's id (and scene) too. Between builds
 // the slot order is fixed and the ids of both state buffers agree, so only the first
 // step after a build (whose gather reordered one buffer) and Picard write them.
 template <bool HIST, bool BATCH, bool PICARD>
 __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& A, int s, int n,
                                            int scene, float4 pi, float4 vi, int id, int cnt,
                                            float4 xb, int hcnt_in, bool exact, bool order_out,
-                                           uint32_t& disp_bits, uint32_t& step_bits,
-                                           uint32_t& res_bits, bool& viol) {
+                                           bool warp_listed, uint32_t& disp_bits,
+                                           uint32_t& step_bits, uint32_t& res_bits, bool& viol) {
     const DevParams& P = BATCH ? A.scene_params[scene] : P0;
     if (PICARD) {
         // the rhs of a Picard step pairs the last iterate's velocity with its forces
@@ -333,45 +336,49 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
             h.out_count = 0;
         }
         wall_forces<HIST>(P, pos, vel, ri, mi, f, h, A.counters);
-        const float3 f_walls = f;
-        const int out_walls = HIST ? h.out_count : 0;
-        const float cut = contact_cutoff_sq(ri, P.rmax);
-        // the grain's cell orders its contacts; a grain without list entries needs none
-        int cx = 0, cy = 0, cz = 0;
-        if (cnt > 0) cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
-        bool ordered = true;
-        if (cnt <= kNbrCap) {
-            // the list, in its build order, while the contacts arrive in canonical order
-            unsigned long long last = 0ull;
-            for (int e = 0; e < cnt; ++e) {
-                const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
-                const float4 pj = __ldg(&A.pos[j]);
-                float3 d;
-                const float ns = pair_norm_sq(pi, pj, d);
-                if (ns > cut) continue;
-                const float norm = sqrtf(ns);
-                const float dist = pair_dist(norm, ri, pj.w);
-                if (!(dist < 0.f)) continue;
-                const int jd = __ldg(&A.ids[j]);
-                const unsigned long long key = visit_key(P, cx, cy, cz, pj, jd);
-                if (key < last) {
-                    ordered = false;
-                    break;
+        // the list contacts, skipped as a whole by warps in which no grain has a list
+        // entry (ballistic grains: the contact code's registers stay out of their path)
+        if (warp_listed) {
+            const float3 f_walls = f;
+            const int out_walls = HIST ? h.out_count : 0;
+            const float cut = contact_cutoff_sq(ri, P.rmax);
+            // the grain's cell orders its contacts; a grain without list entries needs none
+            int cx = 0, cy = 0, cz = 0;
+            if (cnt > 0) cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+            bool ordered = true;
+            if (cnt <= kNbrCap) {
+                // the list, in its build order, while the contacts arrive in canonical order
+                unsigned long long last = 0ull;
+                for (int e = 0; e < cnt; ++e) {
+                    const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+                    const float4 pj = __ldg(&A.pos[j]);
+                    float3 d;
+                    const float ns = pair_norm_sq(pi, pj, d);
+                    if (ns > cut) continue;
+                    const float norm = sqrtf(ns);
+                    const float dist = pair_dist(norm, ri, pj.w);
+                    if (!(dist < 0.f)) continue;
+                    const int jd = __ldg(&A.ids[j]);
+                    const unsigned long long key = visit_key(P, cx, cy, cz, pj, jd);
+                    if (key < last) {
+                        ordered = false;
+                        break;
+                    }
+                    last = key;
+                    const float4 vj = __ldg(&A.vel[j]);
+                    pair_force<HIST>(P, d, norm, dist, vel, mi, vj, jd, f, h, A.counters);
                 }
-                last = key;
-                const float4 vj = __ldg(&A.vel[j]);
-                pair_force<HIST>(P, d, norm, dist, vel, mi, vj, jd, f, h, A.counters);
+                if (!ordered) {
+                    // a cell crossing re-ordered this grain's contacts: redo them in
+                    // canonical order
+                    f = f_walls;
+                    if (HIST) h.out_count = out_walls;
+                    list_contacts_sorted<HIST>(P, A, s, n, cnt, pi, vel, mi, cut, cx, cy, cz, f, h);
+                }
+            } else {
+                // list overflow: this step built the lists, so the run table is fresh
+                list_contacts_table<HIST>(P, A, s, pi, vel, mi, cut, cx, cy, cz, f, h);
             }
-            if (!ordered) {
-                // a cell crossing re-ordered this grain's contacts: redo them in
-                // canonical order
-                f = f_walls;
-                if (HIST) h.out_count = out_walls;
-                list_contacts_sorted<HIST>(P, A, s, n, cnt, pi, vel, mi, cut, cx, cy, cz, f, h);
-            }
-        } else {
-            // list overflow: this step built the lists, so the run table is fresh
-            list_contacts_table<HIST>(P, A, s, pi, vel, mi, cut, cx, cy, cz, f, h);
         }
         if (HIST) A.hcnt_out[s] = h.out_count;
         const float3 a = make_float3(f.x / mi, f.y / mi, f.z / mi);
@@ -413,31 +420,38 @@ template <bool HIST, bool BATCH, int MINB, bool PICARD>
 __global__ void __launch_bounds__(kBlock, MINB)
 k_force_list(DevParams P0, ListArgs A) {
     if (PICARD && skipped(A.skip)) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = P0.n;
     uint32_t disp_bits = 0u, step_bits = 0u;
     uint32_t res_bits = 0u;
     bool viol = false;
-    // every per-slot load issued up front: they are independent, and the kernel is
-    // bound by their latency when lists are short
-    int scene = 0, id = 0, cnt = 0, hcnt_in = 0;
-    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f), vi = pi, xb = pi;
-    if (s < n) {
-        scene = BATCH ? A.scene[s] : 0;
-        pi = A.pos[s];
-        vi = A.vel[s];
-        id = A.ids[s];
-        cnt = A.nbr_cnt[s];
-        hcnt_in = HIST ? A.hcnt_in[s] : 0;
-    }
     // build positions are read only on the steps that measure the exact displacement;
     // ids only right after a build
     const bool exact = PICARD || A.list_ctrl[kLcExact] != 0u;
     const bool order_out = PICARD || A.list_ctrl[kLcDecision] != 0u;
-    if (s < n) {
-        if (exact) xb = A.xbuild[s];
-        list_grain<HIST, BATCH, PICARD>(P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in, exact,
-                                        order_out, disp_bits, step_bits, res_bits, viol);
+    // a grid-stride loop: semi-implicit Euler launches one wave (its fused build decision
+    // then waits once per block, not once per block of a many-wave grid); Picard launches
+    // one slot per thread
+    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const int s = base + threadIdx.x;
+        const bool live = s < n;
+        // every per-slot load issued up front: they are independent, and the kernel is
+        // bound by their latency when lists are short
+        int scene = 0, id = 0, cnt = 0, hcnt_in = 0;
+        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f), vi = pi, xb = pi;
+        if (live) {
+            scene = BATCH ? A.scene[s] : 0;
+            pi = A.pos[s];
+            vi = A.vel[s];
+            id = A.ids[s];
+            cnt = A.nbr_cnt[s];
+            hcnt_in = HIST ? A.hcnt_in[s] : 0;
+            if (exact) xb = A.xbuild[s];
+        }
+        const bool warp_listed = __any_sync(0xffffffffu, cnt != 0);
+        if (live)
+            list_grain<HIST, BATCH, PICARD>(P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in,
+                                            exact, order_out, warp_listed, disp_bits, step_bits,
+                                            res_bits, viol);
     }
     list_disp_report<PICARD>(A.list_ctrl, exact, disp_bits, step_bits);
     if (!PICARD) list_tail_decide(A);
@@ -613,10 +627,11 @@ k_force_list_staged(DevParams P0, ListArgs A) {
                 if (exact) xb = A.xbuild[s];
             }
         }
+        const bool warp_listed = __any_sync(0xffffffffu, cnt != 0);
         if (s < n)
             list_grain<HIST, BATCH, false>(P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in,
-                                           exact, order_out, disp_bits, step_bits, res_bits,
-                                           viol);
+                                           exact, order_out, warp_listed, disp_bits,
+                                           step_bits, res_bits, viol);
     }
     if (failed) {
         // a stage never completed: flag it and drain what this warp still has in flight
@@ -731,13 +746,12 @@ __device__ __forceinline__ void coop_flush(const DevParams& P0, const ListArgs& 
     bstart = my_count;
 }
 
+// One slot per lane of the warp-cooperative kernel (all lanes of the warp together).
 template <bool HIST, bool BATCH>
-__global__ void __launch_bounds__(kBlock, 4)
-k_force_list_coop(DevParams P0, ListArgs A) {
-    __shared__ CoopWarp warps[kCoopWarps];
+__device__ __forceinline__ void coop_slot(const DevParams& P0, const ListArgs& A, CoopWarp& W, int s, bool exact,
+                                          bool order_out, uint32_t& disp_bits,
+                                          uint32_t& step_bits) {
     const int lane = threadIdx.x & 31;
-    CoopWarp& W = warps[threadIdx.x >> 5];
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = P0.n;
     const bool active = s < n;
     // per-slot loads, up front
@@ -746,8 +760,6 @@ k_force_list_coop(DevParams P0, ListArgs A) {
     const float4 vi = active ? A.vel[s] : make_float4(0.f, 0.f, 0.f, 1.f);
     const int id = active ? A.ids[s] : 0;
     const int cnt_raw = active ? A.nbr_cnt[s] : 0;
-    const bool exact = A.list_ctrl[kLcExact] != 0u;
-    const bool order_out = A.list_ctrl[kLcDecision] != 0u;  // first step after a build
     const float4 xb = (active && exact) ? A.xbuild[s] : make_float4(0.f, 0.f, 0.f, 0.f);
     const int hcnt_in = (HIST && active) ? A.hcnt_in[s] : 0;
     const DevParams& P = BATCH ? A.scene_params[scene] : P0;
@@ -814,66 +826,16 @@ k_force_list_coop(DevParams P0, ListArgs A) {
         q += add;
     }
     if (rounds > 0) coop_flush<HIST, BATCH>(P0, A, W, q, lane, my_count, bstart, reorder, f);
-    uint32_t disp_bits = 0u, step_bits = 0u;
     if (work) {
         if (!listed) {
             // list overflow: this step built the lists, so the run table is fresh
             h.out_count = out_walls;
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int nx = cx + dx;
-                if (nx < 0 || nx >= P.grid[0]) continue;
-                int lo[3], hi[3];
-                row_ranges(P, A.table, nx, cy, cz, lo, hi);
-                for (int t = 0; t < 3; ++t) {
-                    for (int j = lo[t]; j < hi[t]; ++j) {
-                        const float4 pj = __ldg(&A.pos[j]);
-                        float3 d;
-                        const float ns = pair_norm_sq(pi, pj, d);
-                        if (ns > cut || j == s) continue;
-                        const float norm = sqrtf(ns);
-                        const float dist = pair_dist(norm, ri, pj.w);
-                        if (!(dist < 0.f)) continue;
-                        const float4 vj = __ldg(&A.vel[j]);
-                        const int partner = HIST ? __ldg(&A.ids[j]) : 0;
-                        pair_force<HIST>(P, d, norm, dist, vel, mi, vj, partner, f, h, A.counters);
-                    }
-                }
-            }
+            list_contacts_table<HIST>(P, A, s, pi, vel, mi, cut, cx, cy, cz, f, h);
         } else if (reorder) {
-            // a cell crossing re-ordered this grain's contacts: redo them in canonical
-            // order, each pass taking the smallest key above the last
+            // a cell crossing re-ordered this grain's contacts: redo them in canonical order
             f = f_walls;
             h.out_count = out_walls;
-            long long done = -1;
-            for (;;) {
-                long long best = 0x7fffffffffffffffll;
-                int bj = -1;
-                for (int e = 0; e < cnt; ++e) {
-                    const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
-                    const float4 pj = __ldg(&A.pos[j]);
-                    float3 d;
-                    const float ns = pair_norm_sq(pi, pj, d);
-                    if (ns > cut) continue;
-                    const float dist = pair_dist(sqrtf(ns), ri, pj.w);
-                    if (!(dist < 0.f)) continue;
-                    const long long key =
-                        static_cast<long long>(visit_key(P, cx, cy, cz, pj, __ldg(&A.ids[j])));
-                    if (key > done && key < best) {
-                        best = key;
-                        bj = j;
-                    }
-                }
-                if (bj < 0) break;
-                done = best;
-                const float4 pj = __ldg(&A.pos[bj]);
-                float3 d;
-                const float ns = pair_norm_sq(pi, pj, d);
-                const float norm = sqrtf(ns);
-                const float dist = pair_dist(norm, ri, pj.w);
-                const float4 vj = __ldg(&A.vel[bj]);
-                pair_force<HIST>(P, d, norm, dist, vel, mi, vj,
-                                 static_cast<int>(best & 0xffffffffll), f, h, A.counters);
-            }
+            list_contacts_sorted<HIST>(P, A, s, n, cnt, pi, vel, mi, cut, cx, cy, cz, f, h);
         } else if (HIST) {
             h.out_count = min(out_walls + my_count, kHistCap);
             if (out_walls + my_count > kHistCap)
@@ -893,8 +855,8 @@ k_force_list_coop(DevParams P0, ListArgs A) {
             if (BATCH) A.scene_out[s] = scene;
         }
         A.acc_out[s] = make_float4(a.x, a.y, a.z, 0.f);
-        disp_bits = exact ? disp_sq_bits(x1, xb) : 0u;
-        step_bits = disp_sq_bits(x1, pos);
+        if (exact) disp_bits = max(disp_bits, disp_sq_bits(x1, xb));
+        step_bits = max(step_bits, disp_sq_bits(x1, pos));
     } else if (frozen) {
         A.pos_out[s] = pi;
         A.vel_out[s] = vi;
@@ -905,6 +867,20 @@ k_force_list_coop(DevParams P0, ListArgs A) {
         A.acc_out[s] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (HIST) A.hcnt_out[s] = 0;
     }
+}
+
+// Grid-stride over warps of 32 slots (one wave for the fused build decision).
+template <bool HIST, bool BATCH>
+__global__ void __launch_bounds__(kBlock, 4)
+k_force_list_coop(DevParams P0, ListArgs A) {
+    __shared__ CoopWarp warps[kCoopWarps];
+    CoopWarp& W = warps[threadIdx.x >> 5];
+    const bool exact = A.list_ctrl[kLcExact] != 0u;
+    const bool order_out = A.list_ctrl[kLcDecision] != 0u;  // first step after a build
+    uint32_t disp_bits = 0u, step_bits = 0u;
+    for (int base = blockIdx.x * blockDim.x; base < P0.n; base += gridDim.x * blockDim.x)
+        coop_slot<HIST, BATCH>(P0, A, W, base + threadIdx.x, exact, order_out, disp_bits,
+                               step_bits);
     list_disp_report<false>(A.list_ctrl, exact, disp_bits, step_bits);
     list_tail_decide(A);
 }
@@ -965,16 +941,41 @@ void force_list_staged(const DevParams& P, const ListArgs& a, cudaStream_t st) {
     k_force_list_staged<HIST, BATCH, MINB><<<nb < 1 ? 1 : nb, kBlock, 0, st>>>(P, a);
 }
 
+// Blocks of one full wave of a kernel at `block` threads (cached per kernel, device and
+// block size).
+template <auto Kernel>
+int one_wave(int block) {
+    static int cache[8][5] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& occ = cache[dev & 7][(block / 64) % 5];
+    if (occ == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, Kernel, block, 0);
+        occ = occ < 1 ? 1 : occ;
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * occ;
+}
+
+template <bool HIST, bool BATCH, int MINB, bool PICARD>
+void force_list_launch(const DevParams& P, const ListArgs& a, cudaStream_t st, int block) {
+    int nb = blocks_for(P.n, block);
+    // semi-implicit Euler: one wave (grid-stride), so the fused build decision's
+    // per-block wait happens once per resident block
+    if (!PICARD) nb = std::min(nb, one_wave<k_force_list<HIST, BATCH, MINB, PICARD>>(block));
+    k_force_list<HIST, BATCH, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
+}
+
 template <int MINB, bool PICARD>
 void force_list_variant(const DevParams& P, const ListArgs& a, cudaStream_t st, int block) {
-    const int nb = blocks_for(P.n, block);
     const bool batch = a.scene_params != nullptr;
     if (P.history) {
-        if (batch) k_force_list<true, true, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
-        else k_force_list<true, false, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
+        if (batch) force_list_launch<true, true, MINB, PICARD>(P, a, st, block);
+        else force_list_launch<true, false, MINB, PICARD>(P, a, st, block);
     } else {
-        if (batch) k_force_list<false, true, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
-        else k_force_list<false, false, MINB, PICARD><<<nb, block, 0, st>>>(P, a);
+        if (batch) force_list_launch<false, true, MINB, PICARD>(P, a, st, block);
+        else force_list_launch<false, false, MINB, PICARD>(P, a, st, block);
     }
 }
 
@@ -1010,15 +1011,22 @@ void launch_force_list(const DevParams& P, const ListArgs& a, cudaStream_t st, i
         return;
     }
     if (min_blocks == 0) {
-        // warp-cooperative kernel: its shared queues are sized for kBlock threads
+        // warp-cooperative kernel: its shared queues are sized for kBlock threads; one
+        // wave, grid-stride
         const int nb = blocks_for(P.n, kBlock);
         const bool batch = a.scene_params != nullptr;
         if (P.history) {
-            if (batch) k_force_list_coop<true, true><<<nb, kBlock, 0, st>>>(P, a);
-            else k_force_list_coop<true, false><<<nb, kBlock, 0, st>>>(P, a);
+            if (batch) {
+                k_force_list_coop<true, true><<<std::min(nb, one_wave<k_force_list_coop<true, true>>(kBlock)), kBlock, 0, st>>>(P, a);
+            } else {
+                k_force_list_coop<true, false><<<std::min(nb, one_wave<k_force_list_coop<true, false>>(kBlock)), kBlock, 0, st>>>(P, a);
+            }
         } else {
-            if (batch) k_force_list_coop<false, true><<<nb, kBlock, 0, st>>>(P, a);
-            else k_force_list_coop<false, false><<<nb, kBlock, 0, st>>>(P, a);
+            if (batch) {
+                k_force_list_coop<false, true><<<std::min(nb, one_wave<k_force_list_coop<false, true>>(kBlock)), kBlock, 0, st>>>(P, a);
+            } else {
+                k_force_list_coop<false, false><<<std::min(nb, one_wave<k_force_list_coop<false, false>>(kBlock)), kBlock, 0, st>>>(P, a);
+            }
         }
     } else if (min_blocks == 4) {
         force_list_variant<4, false>(P, a, st, block);
