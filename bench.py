@@ -75,6 +75,9 @@ def parse_args():
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="Verlet-list skin in m (simulation.neighbor_skin); negative: chosen by "
                          "the autotuner; 0: grid search every step, as the reference")
+    ap.add_argument("--contact-kernel", default=None, metavar="BLOCK,VARIANT",
+                    help="with --skin >= 0: the list contact kernel (block size, variant 48/64 "
+                         "per-lane, 0 cooperative, 1/2 bulk-staged); default: the library's")
     ap.add_argument("--direct", action="store_true",
                     help="launch each step's kernels directly instead of as one CUDA graph "
                          "(for per-kernel profilers, which cannot see inside graphs with "
@@ -308,6 +311,13 @@ def run_ours(args) -> int:
         skin, _ = sim.autotune(steps=40)
         scene.cfg.neighbor_skin = skin
         tuned = sim.tuning()
+    elif args.contact_kernel:
+        block, variant = (int(v) for v in args.contact_kernel.split(","))
+        sim.set_contact_kernel(block, variant)
+    variant_name = sim.tuning()["contact_variant"]
+    kernel_symbol = ("k_force_list_staged" if variant_name.startswith("bulk-staged") else
+                     "k_force_list_coop" if variant_name.startswith("warp-cooperative") else
+                     "k_force_list")
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -360,6 +370,8 @@ def run_ours(args) -> int:
     # per-phase timing of the same workload for the roofline (direct launches)
     sim.set_kernel_timing(True)
     t0 = sim._timings()
+    phase_builds0 = sim.list_stats()[0]
+    phase_exact0 = sim.list_exact_count()
     with torch.cuda.stream(stream):
         for k in range(args.phase_steps):
             flush.fill_(float(k))
@@ -367,6 +379,8 @@ def run_ours(args) -> int:
     sim.synchronize()
     t1 = sim._timings()
     sim.set_kernel_timing(args.direct)
+    build_frac = (sim.list_stats()[0] - phase_builds0) / args.phase_steps
+    exact_frac = (sim.list_exact_count() - phase_exact0) / args.phase_steps
     search_ms = float(t1[0] - t0[0]) / args.phase_steps
     contact_ms = float(t1[1] - t0[1]) / args.phase_steps
     # backward Euler / Picard: the timed contact phase is the whole step, one contact
@@ -374,14 +388,22 @@ def run_ours(args) -> int:
     phase_iters = (sim.picard_counts()[0] - iters1) / args.phase_steps if picard else 1.0
     cnt, _, _ = sim.get_history()
     entries = int(cnt.astype(np.int64).sum())
-    # contact kernel, algorithmic bytes per launch: read x,r / v,m / id (36 B) and
-    # write x,r / v,m / id / a (52 B) per grain; history rows read and written
-    # (16 B per entry each way) plus the per-grain counts (4 B each way)
+    # contact kernel, algorithmic bytes per launch. Searched step: read x,r / v,m / id
+    # (36 B) and write x,r / v,m / id / a (52 B) per grain. History rows read and
+    # written (16 B per entry each way) plus the per-grain counts (4 B each way).
     hist_bytes = (2 * 16 * entries + 8 * n) if scene.cfg.history else 0
-    contact_bytes = 88 * n + hist_bytes
-    if lists:
-        # plus the list count and the build position (20 B) and the list (4 B / entry)
-        contact_bytes += int(20 * n + 4 * mean_list * n)
+    if not lists:
+        contact_bytes = 88 * n + hist_bytes
+    elif not picard:
+        # lists, semi-implicit Euler: read x,r / v,m / id and the list count (40 B), the
+        # list (4 B per entry), the build position on the steps that measure it; write
+        # x,r / v,m / a (48 B) and the id only on the step after a build
+        contact_bytes = int(88 * n + hist_bytes + 4 * mean_list * n + 16 * n * exact_frac
+                            + 4 * n * build_frac)
+    else:
+        # lists, one Picard iteration: as the searched step plus the list count, the
+        # build position, the step-start state (32 B) and the rhs copy (20 B)
+        contact_bytes = int(88 * n + hist_bytes + 4 * mean_list * n + 72 * n)
     achieved = contact_bytes * phase_iters / (contact_ms / 1e3) / 1e9
     peak, peak_kind = measured_hbm_peak()
 
@@ -443,12 +465,15 @@ def run_ours(args) -> int:
             "config": workload_config(scene, args, grains=all_grains, scenes=scenes_total),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": profiled_traffic(args.workload, "k_force_list" if lists else "k_force"),
-                         "kernel": ("k_force_list (contacts from Verlet lists + integrator)" if lists
+                         "traffic": profiled_traffic(args.workload, kernel_symbol if lists else "k_force"),
+                         "kernel": (f"{kernel_symbol} (contacts from Verlet lists + integrator; "
+                                    f"{variant_name})" if lists
                                     else "k_force (contact forces + integrator)"),
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "algorithmic_bytes_per_launch": contact_bytes,
+                         "measuring_step_fraction": exact_frac if lists else None,
+                         "build_step_fraction": build_frac if lists else None,
                          "kernel_ms": contact_ms / phase_iters, "search_ms": search_ms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
