@@ -19,7 +19,7 @@ e2e    -- the same metric through the C ABI with host buffers: each step
 neighbor search -- Verlet lists, skin and contact-kernel block size chosen by the
           library's autotuner before the warm-up (--skin S fixes the skin; 0 searches
           the grid every step as the reference does): the grid search and sort run
-          only when a grain has moved 0.45 skin since the last build; the results are
+          only when a grain has moved 0.49 skin since the last build; the results are
           bit-identical either way.
 roofline -- the contact kernel (forces + integrator, the dominant kernel): its
           algorithmic bytes per launch over its average event-timed duration,

@@ -6,7 +6,7 @@
 //   simulation.history            false  -> viscous tangential friction (reference)
 //   simulation.neighbor_skin      0      -> neighbor search every step (reference); > 0:
 //                                           Verlet lists with this skin (m), rebuilt when
-//                                           a grain has moved 0.45 skin since the build
+//                                           a grain has moved 0.49 skin since the build
 //   physics.normal_stiffness      0      -> k_n = max_force / particle_radius
 //   physics.tangential_stiffness  0      -> k_t = 2/7 k_n when history is on
 //   physics.density               0      -> masses from the material table

@@ -131,10 +131,17 @@ void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip
 // [0] max |x - x_build|^2 over the last step's output (float bits; measured only when
 // [7] was set), [1] a list overflowed, [2] rebuild requested by the host, [3] this
 // step's decision (1.0f: rebuild). Picard: [4] an iteration started from an iterate
-// 0.45 skin or more from its build position, [5] this step's redo decision (1.0f: redo
+// kListValid skin or more from its build position, [5] this step's redo decision (1.0f: redo
 // with the per-iteration search). [6] max |x_out - x_in|^2 of the last step (float
 // bits), [7] the contact kernel measures [0] this step, [8..9] (double) a bound on
 // max |x - x_build| of the current state.
+// Verlet-list validity: every grain within kListValid skins of its build position.
+// Pairs not listed were >= r_i + r_j + skin apart at the build; after displacements of
+// at most kListValid skin each they are still >= r_i + r_j + 0.02 skin apart (10 um at
+// a 0.5 mm skin, many orders of magnitude above the float rounding of the distance
+// tests). Picard builds earlier, at kPicardBuildAt, so that its iterates rarely leave.
+constexpr float kListValid = 0.49f;
+constexpr float kPicardBuildAt = 0.30f;
 enum ListCtrl {
     kLcDisp = 0, kLcOverflow = 1, kLcForce = 2, kLcDecision = 3, kLcViol = 4, kLcRedo = 5,
     kLcStep = 6, kLcExact = 7, kLcBound = 8, kLcWords = 10

@@ -5,9 +5,10 @@
 // simulation.neighbor_skin = s > 0 the search runs only when needed: a build sorts the
 // grains as the search does, and lists, for every grain, the grains whose centres are
 // closer than r_i + r_j + s, in the contact kernel's canonical visiting order (stencil
-// cell, then grain id). Until some grain has moved 0.45 s from where the build saw it,
-// every contact of every step is in the lists (|d| >= r_i + r_j + s - 0.9 s), so the
-// step computes the same contact set as the searched step.
+// cell, then grain id). Until some grain has moved 0.49 s from where the build saw it
+// (kListValid), every contact of every step is in the lists (a pair not listed is still
+// >= r_i + r_j + 0.02 s apart), so the step computes the same contact set as the
+// searched step.
 //
 // The results are bit-identical to the searched step because forces are accumulated
 // in the same order: the kernel checks that the contacts it meets arrive in canonical
@@ -19,8 +20,8 @@
 // build gathers it into the new order, lists the neighbors, and copies it back.
 //
 // Picard iterates every force evaluation of a step on the same lists. Builds start at
-// 0.30 skin instead of 0.45, and each iteration checks that its input iterate is still
-// within 0.45 skin of the build; if one is not, the step is redone from its start
+// 0.30 skin instead of 0.49, and each iteration checks that its input iterate is still
+// within 0.49 skin of the build; if one is not, the step is redone from its start
 // state with the per-iteration search, so the results stay those of the searched step.
 #include <algorithm>
 

@@ -631,12 +631,12 @@ cudaError_t enqueue_picard_redo(wd_sim* s, int parity, cudaStream_t st) {
 // iterations on the lists (iterates alternate between B and the scratch buffers,
 // integrating from the state in A), the last iterate into B, and, when an iterate left
 // the lists' validity bound, the redo. Builds start at 0.30 skin so that iterates
-// rarely reach the 0.45 bound within a step.
+// rarely reach the validity bound (kListValid) within a step.
 cudaError_t enqueue_step_list_picard(wd_sim* s, int parity, cudaStream_t st, bool capture,
                                      cudaEvent_t mid) {
     const DevParams& P = s->P;
     const bool hist = P.history != 0, batch = s->scenes > 1;
-    const float build_at = 0.30f * P.skin, valid = 0.45f * P.skin;
+    const float build_at = wd::kPicardBuildAt * P.skin, valid = wd::kListValid * P.skin;
     cudaError_t e = enqueue_list_decide_build(s, build_at, st, capture);
     if (e != cudaSuccess) return e;
     if (mid) cudaEventRecord(mid, st);
@@ -725,7 +725,7 @@ cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool captu
         if (e != cudaSuccess) return e;
     }
     wd::ListArgs a{};
-    a.thr = 0.45f * P.skin;
+    a.thr = wd::kListValid * P.skin;
     a.tail_count = s->tail_count;
     a.use_cond = capture ? 1 : 0;
     a.cond = cond;
@@ -767,7 +767,7 @@ cudaError_t enqueue_pending_build(wd_sim* s, cudaStream_t st) {
     if (!s->need_build) return cudaSuccess;
     s->need_build = false;
     if (s->picard) return cudaSuccess;  // the Picard step decides at its start
-    return enqueue_list_decide_build(s, 0.45f * s->P.skin, st, false);
+    return enqueue_list_decide_build(s, wd::kListValid * s->P.skin, st, false);
 }
 
 cudaError_t enqueue_any_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
