@@ -202,3 +202,37 @@ def test_repeated_runs_bit_identical_with_contacts():
         out.append(sim.get_state())
         sim.close()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("moved", [700, 2500, 6000, 8192, 11000])
+def test_mover_sort_many_movers(moved):
+    """Thousands of grains change cell at once: the cluster-wide mover sort (up to 8192
+    movers, eight CTAs over distributed shared memory) and, above that, the radix path
+    give the (cell key, grain id) order of the oracle."""
+    from oracle.oracle import OracleSim, params_from_config
+    from world_b200.state_io import grain_properties
+    cfg, st, rad = packed_poly(n=12000, seed=41, mu=0.3, history=False)
+    cfg.kernel_timing = False
+    sim = ParticleDynamics(cfg, state=st, radius=rad)
+    sim.advance(2)
+    state = sim.get_state().reshape(-1, 6).copy()
+    rng = np.random.default_rng(moved)
+    who = rng.choice(state.shape[0], size=moved, replace=False)
+    cell = (cfg.domain.x_max - cfg.domain.x_min) / cfg.collision_grid_size_x
+    # one cell along x, alternating sides, so that most of them change cell
+    state[who, 0] += np.where(np.arange(moved) % 2 == 0, 1.0, -1.0) * np.float32(cell)
+    sim.set_state(state)
+    radix0 = sim.radix_search_count()[0]
+    skeys, sids = sim.debug_sorted()
+    _, mass = grain_properties(cfg, np.full(st.shape[0], cfg.particle_material, np.int32), rad)
+    keys = OracleSim(params_from_config(cfg), sim.get_state(), rad, mass).cell_keys()
+    order = np.lexsort((np.arange(sim.n), keys))
+    assert np.array_equal(sids, order.astype(np.int32))
+    assert np.array_equal(skeys, keys[order])
+    # above 8192 movers the search takes the radix path
+    took_radix = sim.radix_search_count()[0] > radix0
+    if moved <= 6000:
+        assert not took_radix
+    if moved == 11000:
+        assert took_radix          # grains in the edge cells stay, but > 8192 move
+    sim.close()

@@ -7,7 +7,8 @@
 //   * the key of every grain is the reference's cell mapping; grains are ordered by
 //     (key, grain id): deterministic, no per-cell capacity, nothing dropped;
 //   * between steps few grains change cell, so the search re-sorts only those
-//     ("movers": one-block bitonic sort) and merges them into the still-sorted rest
+//     ("movers": a bitonic sort on one 8-CTA cluster over distributed shared memory)
+//     and merges them into the still-sorted rest
 //     by binary search; the first search, or one with more than kMoverCap movers,
 //     runs a stable LSD radix sort of all keys instead. The choice is made on the
 //     device, so both paths sit in the same CUDA graph and the idle one returns at
@@ -16,6 +17,8 @@
 //     previous search are cleared (O(n), not the reference's O(cells) memset);
 //   * no candidate list is materialised: the contact kernel walks the sorted runs.
 #include <cstdio>
+
+#include <cooperative_groups.h>
 
 #include "wd_kernels.h"
 
@@ -245,48 +248,75 @@ k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict_
     }
 }
 
-// Search pass 2, one block: mover offsets per 256-slot block, the mover count and
-// the path. When the movers fit kMoverCap they are compacted from the bit mask (only
-// blocks that have movers are read) and sorted by (key << 32 | id) with a bitonic
-// network in shared memory; otherwise ctrl[1] selects the radix sort, and when the
-// search runs inside a CUDA graph the radix path's conditional node is switched on.
-__global__ void __launch_bounds__(kMoverThreads)
+// Search pass 2, one thread-block cluster of kMoverCtas CTAs (one CTA per SM, the
+// cluster's shared memories together holding kMoverCap movers, one per thread): mover
+// offsets per 256-slot block, the mover count and the path. When the movers fit
+// kMoverCap they are compacted from the bit mask (only blocks that have movers are
+// read) into the distributed shared memory and sorted by (key << 32 | id) with a
+// bitonic network whose stages across CTAs use remote shared-memory accesses (DSMEM)
+// and a cluster barrier, the others a CTA barrier; otherwise ctrl[1] selects the radix
+// sort, and when the search runs inside a CUDA graph the radix path's conditional node
+// is switched on. (A single CTA did the same network on one SM, issue-bound at about
+// 100 us for 8192 movers.)
+constexpr int kMoverCtas = 8;
+constexpr int kMoverPer = kMoverCap / kMoverCtas;  // elements per CTA: one per thread
+static_assert(kMoverPer == kMoverThreads, "one mover element per thread");
+
+__global__ void __cluster_dims__(kMoverCtas, 1, 1) __launch_bounds__(kMoverThreads)
 k_movers(int n, const int* __restrict__ blk_cnt, int* __restrict__ blk_off, int num_blocks,
          const uint32_t* __restrict__ moved, const uint32_t* __restrict__ newkey,
          const int* __restrict__ ids, unsigned long long* __restrict__ mv_key,
          uint32_t* __restrict__ mv_slot, int* __restrict__ ctrl, int use_cond,
          cudaGraphConditionalHandle cond, unsigned long long* __restrict__ counters, Skip skip) {
-    if (skipped(skip)) return;
-    extern __shared__ unsigned long long smem[];
-    unsigned long long* k = smem;
-    uint32_t* v = reinterpret_cast<uint32_t*>(smem + kMoverCap);
-    __shared__ int s_full;
-    const int chunk = (num_blocks + kMoverThreads - 1) / kMoverThreads;
-    const int b0 = min(static_cast<int>(threadIdx.x) * chunk, num_blocks);
+    namespace cg = cooperative_groups;
+    if (skipped(skip)) return;  // the same flag for every CTA of the cluster
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = static_cast<int>(cluster.block_rank());
+    __shared__ unsigned long long k[kMoverPer];
+    __shared__ uint32_t v[kMoverPer];
+    __shared__ uint32_t cta_total;
+    __shared__ uint32_t s_off, s_m;
+    const int tid = static_cast<int>(threadIdx.x);
+    const int g = rank * kMoverPer + tid;  // the cluster-wide thread, owner of element g
+    const int gthreads = kMoverCtas * kMoverThreads;
+    const int chunk = (num_blocks + gthreads - 1) / gthreads;
+    const int b0 = min(g * chunk, num_blocks);
     const int b1 = min(b0 + chunk, num_blocks);
     uint32_t sum = 0u;
     for (int b = b0; b < b1; ++b) sum += static_cast<uint32_t>(blk_cnt[b]);
     uint32_t total = 0u;
-    const uint32_t first = block_exclusive_scan<kMoverThreads>(sum, &total);
-    uint32_t run = first;
+    const uint32_t first_local = block_exclusive_scan<kMoverThreads>(sum, &total);
+    if (tid == 0) cta_total = total;
+    cluster.sync();  // every CTA's total visible
+    if (tid == 0) {
+        uint32_t off = 0u, m = 0u;
+        for (int r = 0; r < kMoverCtas; ++r) {
+            const uint32_t t = *cluster.map_shared_rank(&cta_total, r);
+            if (r < rank) off += t;
+            m += t;
+        }
+        s_off = off;
+        s_m = m;
+    }
+    cluster.sync();  // remote reads done before any CTA may leave
+    const uint32_t total_all = s_m;
+    uint32_t run = s_off + first_local;
     for (int b = b0; b < b1; ++b) {
         blk_off[b] = static_cast<int>(run);
         run += static_cast<uint32_t>(blk_cnt[b]);
     }
-    const int m = static_cast<int>(total);
-    const int full = total > static_cast<uint32_t>(kMoverCap) ? 1 : 0;
-    if (threadIdx.x == 0) {
+    const int m = static_cast<int>(total_all);
+    const int full = total_all > static_cast<uint32_t>(kMoverCap) ? 1 : 0;
+    if (rank == 0 && tid == 0) {
         blk_off[num_blocks] = m;
         ctrl[0] = m;
         ctrl[1] = full;
         if (use_cond) cudaGraphSetConditional(cond, static_cast<unsigned>(full));
         if (full) atomicAdd(&counters[kCntRadixSearches], 1ull);
-        s_full = full;
     }
-    __syncthreads();
-    if (s_full || m == 0) return;
-    // compaction in slot order
-    run = first;
+    if (full || m == 0) return;  // the same decision in every CTA
+    // compaction in slot order, each mover stored in the CTA that owns its position
+    run = s_off + first_local;
     for (int b = b0; b < b1; ++b) {
         if (blk_cnt[b] == 0) continue;
         const int w0 = b * (kBlock / 32);
@@ -296,42 +326,50 @@ k_movers(int n, const int* __restrict__ blk_cnt, int* __restrict__ blk_off, int 
                 const int lane = __ffs(bits) - 1;
                 bits &= bits - 1u;
                 const int slot = 32 * w + lane;
-                k[run] = (static_cast<unsigned long long>(newkey[slot]) << 32) |
-                         static_cast<uint32_t>(ids[slot]);
-                v[run] = static_cast<uint32_t>(slot);
+                const int owner = static_cast<int>(run) / kMoverPer;
+                const int at = static_cast<int>(run) % kMoverPer;
+                *cluster.map_shared_rank(&k[at], owner) =
+                    (static_cast<unsigned long long>(newkey[slot]) << 32) |
+                    static_cast<uint32_t>(ids[slot]);
+                *cluster.map_shared_rank(&v[at], owner) = static_cast<uint32_t>(slot);
                 ++run;
             }
         }
     }
     int p = 1;
     while (p < m) p <<= 1;
-    for (int i = m + static_cast<int>(threadIdx.x); i < p; i += blockDim.x) {
-        k[i] = ~0ull;
-        v[i] = 0u;
+    if (g >= m && g < p) {
+        k[tid] = ~0ull;
+        v[tid] = 0u;
     }
-    __syncthreads();
+    cluster.sync();  // the compacted movers and the padding visible everywhere
     for (int size = 2; size <= p; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < p; i += blockDim.x) {
-                const int j = i ^ stride;
-                if (j > i) {
-                    const bool up = (i & size) == 0;
-                    const unsigned long long a = k[i], c = k[j];
-                    if ((a > c) == up) {
-                        k[i] = c;
-                        k[j] = a;
-                        const uint32_t t = v[i];
-                        v[i] = v[j];
-                        v[j] = t;
-                    }
+            const int j = g ^ stride;
+            if (g < p && j > g) {
+                const bool up = (g & size) == 0;
+                unsigned long long* kj = cluster.map_shared_rank(&k[j % kMoverPer], j / kMoverPer);
+                uint32_t* vj = cluster.map_shared_rank(&v[j % kMoverPer], j / kMoverPer);
+                const unsigned long long a = k[tid], c = *kj;
+                if ((a > c) == up) {
+                    k[tid] = c;
+                    *kj = a;
+                    const uint32_t t = v[tid];
+                    v[tid] = *vj;
+                    *vj = t;
                 }
             }
-            __syncthreads();
+            // a stage that crosses CTAs, or precedes one, ends at a cluster barrier
+            const bool cross = stride >= kMoverPer;
+            const bool next_cross = stride > 1 ? (stride >> 1) >= kMoverPer
+                                               : ((size << 1) <= p && size >= kMoverPer);
+            if (cross || next_cross) cluster.sync();
+            else __syncthreads();
         }
     }
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        mv_key[i] = k[i];
-        mv_slot[i] = v[i];
+    if (g < m) {
+        mv_key[g] = k[tid];
+        mv_slot[g] = v[tid];
     }
 }
 
@@ -563,7 +601,7 @@ void launch_search_head(const DevParams& P, SceneTab T, const float4* pos, const
                                              sb.num_blocks, sb.slot_keys, sb.table_keys, sb.table,
                                              sb.digit_totals, totals, zero_res, zero_res_count, skip);
     }
-    k_movers<<<1, kMoverThreads, kMoverCap * 12, st>>>(n, sb.blk_cnt, sb.blk_off, sb.num_blocks,
+    k_movers<<<kMoverCtas, kMoverThreads, 0, st>>>(n, sb.blk_cnt, sb.blk_off, sb.num_blocks,
                                                        sb.moved, sb.newkey, ids, sb.mv_key,
                                                        sb.mv_slot, sb.ctrl, use_cond ? 1 : 0,
                                                        cond, counters, skip);
@@ -614,10 +652,7 @@ void launch_search(const DevParams& P, SceneTab T, const float4* pos, const int*
     launch_search_merge(P, ids, sb, skip, st);
 }
 
-cudaError_t search_prepare() {
-    return cudaFuncSetAttribute(k_movers, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                kMoverCap * 12);
-}
+cudaError_t search_prepare() { return cudaSuccess; }
 
 int radix_output(int passes) { return (passes - 1) & 1; }
 
