@@ -344,7 +344,8 @@ k_movers(int n, const int* __restrict__ blk_cnt, int* __restrict__ blk_off, int 
     }
     cluster.sync();  // the compacted movers and the padding visible everywhere
     for (int size = 2; size <= p; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        int stride = size >> 1;
+        for (; stride >= 32; stride >>= 1) {
             const int j = g ^ stride;
             if (g < p && j > g) {
                 const bool up = (g & size) == 0;
@@ -361,11 +362,31 @@ k_movers(int n, const int* __restrict__ blk_cnt, int* __restrict__ blk_off, int 
             }
             // a stage that crosses CTAs, or precedes one, ends at a cluster barrier
             const bool cross = stride >= kMoverPer;
-            const bool next_cross = stride > 1 ? (stride >> 1) >= kMoverPer
-                                               : ((size << 1) <= p && size >= kMoverPer);
+            const bool next_cross = (stride >> 1) >= kMoverPer;
             if (cross || next_cross) cluster.sync();
             else __syncthreads();
         }
+        // strides below 32 pair lanes of one warp: exchanged through shuffles, no barrier
+        // (an element at or above p is padding that sorts last; its lane still shuffles)
+        unsigned long long a = k[tid];
+        uint32_t av = v[tid];
+        const bool up = (g & size) == 0;
+        for (; stride > 0; stride >>= 1) {
+            const unsigned long long c = __shfl_xor_sync(0xffffffffu, a, stride);
+            const uint32_t cv = __shfl_xor_sync(0xffffffffu, av, stride);
+            const bool lower = (g & stride) == 0;  // this lane holds the lower index
+            // ascending: the lower index keeps the smaller key; descending: the larger
+            const bool take = lower == up ? c < a : c > a;
+            if (take && g < p) {
+                a = c;
+                av = cv;
+            }
+        }
+        k[tid] = a;
+        v[tid] = av;
+        // the next size starts with a stride >= 32 (or none): across warps, maybe CTAs
+        if ((size << 1) <= p && size >= kMoverPer) cluster.sync();
+        else __syncthreads();
     }
     if (g < m) {
         mv_key[g] = k[tid];
