@@ -20,7 +20,8 @@ inline int blocks_for(int64_t n, int block = kBlock) {
 }
 
 // Incremental search: at most this many grains may change cell between searches
-// for the mover path (one-block bitonic sort); more falls back to the radix sort.
+// for the mover path (a bitonic sort on one 8-CTA cluster, kMoverThreads per CTA);
+// more falls back to the radix sort.
 constexpr int kMoverCap = 8192;
 constexpr int kMoverThreads = 1024;
 
@@ -59,7 +60,7 @@ struct Skip {
 // A search orders the state slots by (cell key, grain id) into keys[out] (sorted
 // keys), vals[out] (grain ids) and src (source slot of each position). It has three
 // parts, split so a CUDA graph can put the radix path under a conditional node:
-//   head  -- keys of every slot, mover bits, and the one-block mover kernel, which
+//   head  -- keys of every slot, mover bits, and the cluster mover kernel, which
 //            picks the path (ctrl[1]) and sets `cond` when use_cond;
 //   radix -- stable LSD radix sort of all keys (runs when ctrl[1]);
 //   merge -- merges the sorted movers into the still-sorted rest (idle when ctrl[1]).
