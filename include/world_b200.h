@@ -267,7 +267,7 @@ int wd_grid_overflow_count(wd_sim* sim, int64_t* count);
  * trajectory does not depend on it. */
 int wd_set_neighbor_skin(wd_sim* sim, float skin);
 /* Autotuner (extension): times `steps` steps for each neighbor skin in {0, 0.05,
- * 0.1, 0.2, 0.4} mean diameters, contact-kernel block size in {128, 256} and, with
+ * 0.1, 0.15, 0.2, 0.3, 0.4} mean diameters, contact-kernel block size in {128, 256} and, with
  * lists, its variant (per-lane with 48 or 64 registers, warp-cooperative, bulk-staged)
  * from the same saved state, keeps
  * the fastest and restores the state (results do not depend on the choice). With

@@ -2128,7 +2128,7 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
         mean_r /= static_cast<double>(sim->radius.size());
         const float d = static_cast<float>(2.0 * mean_r);
         std::vector<float> skins = {0.f};
-        for (float f : {0.05f, 0.1f, 0.2f, 0.4f}) skins.push_back(f * d);
+        for (float f : {0.05f, 0.1f, 0.15f, 0.2f, 0.3f, 0.4f}) skins.push_back(f * d);
         // (block, variant): variant 5 / 4 = per-lane list kernel with 48 / 64 registers,
         // 0 = warp-cooperative list kernel, 1 / 2 = bulk-staged persistent list kernel
         // with 48 / 64 registers (256 threads each)
