@@ -883,7 +883,7 @@ int ondemand_search(wd_sim* s) {
 int sync_stream(wd_sim* s) {
     WD_CUDA(cudaStreamSynchronize(s->stream));
     WD_CUDA(cudaGetLastError());
-    if (s->lists && s->force_minb == 1) {
+    if (s->lists && (s->force_minb == 1 || s->force_minb == 2)) {
         // the bulk-staged contact kernel flags stages that never arrived (bounded waits)
         unsigned long long stalls = 0;
         WD_CUDA(cudaMemcpy(&stalls, s->counters + wd::kCntStageTimeout, sizeof(stalls),
