@@ -922,34 +922,17 @@ void launch_list_copy(int n, const float4* pos, const float4* vel, const int* id
                                                   vel_out, ids_out, hcnt_out, scene_out, skip);
 }
 
-template <bool HIST, bool BATCH, int MINB>
-void force_list_staged(const DevParams& P, const ListArgs& a, cudaStream_t st) {
-    // persistent: as many blocks as fit at once, at most one warp per tile
-    static int per_sm[8] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int& occ = per_sm[dev & 7];
-    if (occ == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &occ, k_force_list_staged<HIST, BATCH, MINB>, kBlock, 0);
-        occ = occ < 1 ? 1 : occ;
-    }
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int tiles = (P.n + kStageTile - 1) / kStageTile;
-    const int want = (tiles + kStageWarps - 1) / kStageWarps;
-    const int nb = want < sms * occ ? want : sms * occ;
-    k_force_list_staged<HIST, BATCH, MINB><<<nb < 1 ? 1 : nb, kBlock, 0, st>>>(P, a);
-}
-
-// Blocks of one full wave of a kernel at `block` threads (cached per kernel, device and
-// block size).
+// Blocks of one full wave of a kernel at `block` threads (a multiple of 32 up to 256):
+// the SM count times the resident blocks per SM, cached per kernel, device and block
+// size (devices beyond the first 64 query each time).
 template <auto Kernel>
 int one_wave(int block) {
-    static int cache[8][5] = {};
+    constexpr int kDevs = 64;
+    static int cache[kDevs][9] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    int& occ = cache[dev & 7][(block / 64) % 5];
+    int local = 0;
+    int& occ = (dev >= 0 && dev < kDevs) ? cache[dev][(block / 32) % 9] : local;
     if (occ == 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, Kernel, block, 0);
         occ = occ < 1 ? 1 : occ;
@@ -957,6 +940,15 @@ int one_wave(int block) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return sms * occ;
+}
+
+template <bool HIST, bool BATCH, int MINB>
+void force_list_staged(const DevParams& P, const ListArgs& a, cudaStream_t st) {
+    // persistent: as many blocks as fit at once, at most one warp per tile
+    const int tiles = (P.n + kStageTile - 1) / kStageTile;
+    const int want = (tiles + kStageWarps - 1) / kStageWarps;
+    const int nb = std::min(want, one_wave<k_force_list_staged<HIST, BATCH, MINB>>(kBlock));
+    k_force_list_staged<HIST, BATCH, MINB><<<nb < 1 ? 1 : nb, kBlock, 0, st>>>(P, a);
 }
 
 template <bool HIST, bool BATCH, int MINB, bool PICARD>
