@@ -473,8 +473,9 @@ k_force_list(DevParams P0, ListArgs A) {
 // Persistent warps over tiles of 32 slots. Each warp keeps two tiles in flight: lane 0
 // issues the tile's per-slot arrays (x, v, ids, list count, spring count, scene, and
 // the build positions on measuring steps) as 1-D bulk copies (cp.async.bulk, the TMA
-// engine; no multicast) into the warp's shared stage, completing on an mbarrier; the
-// lanes compute the tile before while the next arrives. The per-slot loads, whose
+// engine; each copy reads this GPU's memory into the issuing CTA only) into the warp's
+// shared stage, completing on an mbarrier; the lanes compute the tile before while the
+// next arrives. The per-slot loads, whose
 // latency binds the per-lane kernel, leave the critical path. Contacts, forces and the
 // integrator are the per-lane kernel's (list_grain), so the results are identical.
 constexpr int kStageWarps = kBlock / 32;
