@@ -26,6 +26,16 @@ roofline -- the contact kernel (forces + integrator, the dominant kernel): its
           against the measured HBM copy bandwidth.
 cpu_baseline -- the oracle port (C, OpenMP on all host cores) on a bounded sample
           of the same workload, rank 0 at N = 1 only.
+settled / batched / adjoint -- (N = 1, default workload) the same metric in the
+          contact-bearing regime (the same column after 30,000 steps, when it has
+          collapsed onto the floor), for the two batched ensembles, and the reverse
+          pass's cost, each beside the plain step measured above on the same GPU.
+
+--impl reference: the reference's step has no CPU implementation (it is CUDA only),
+so the reference arm times the oracle port (oracle/dem_oracle.c, the reference's step
+restated in C with OpenMP) on all host cores, on the same workload and config, with
+W untimed and K timed steps (K capped so that the run ends within a few minutes; the
+line says how many ran). It loads no part of libworld_b200.
 
 Multi-GPU: one process per GPU (torchrun), each rank advancing its own ensemble
 member of the same workload (seed 12345 + rank); no collective on the data path,
@@ -72,6 +82,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--phase-steps", type=int, default=50)
+    ap.add_argument("--settled-steps", type=int, default=30000,
+                    help="steps from rest before the contact-bearing (settled) measurement")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the settled, batched and adjoint sub-measurements")
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="Verlet-list skin in m (simulation.neighbor_skin); negative: chosen by "
                          "the autotuner; 0: grid search every step, as the reference")
@@ -92,27 +106,28 @@ def env_int(name: str, default: int) -> int:
         return default
 
 
-def workload_config(scene, args, grains=None, scenes=None) -> dict:
-    c = scene.cfg
+def workload_config(spec, workload: str, grains: int, scenes=None) -> dict:
+    """The workload's description, identical in both arms (`spec` is the scene's
+    ConfigSpec: no library needed)."""
     out = {
-        "workload": args.workload,
-        "grains": grains if grains is not None else scene.n,
-        "integrator": c.time_integrator,
-        "mu": c.physics.friction,
-        "tangential_history": bool(c.history),
+        "workload": workload,
+        "grains": grains,
+        "integrator": spec.time_integrator,
+        "mu": spec.physics.friction,
+        "tangential_history": bool(spec.history),
         "diameters": "lognormal(mean 5 mm, sigma 0.15) clipped [0.7d, 1.4d]"
-        if "1m" in args.workload else "see world_b200/scenes.py",
-        "collision_grid": [c.collision_grid_size_x, c.collision_grid_size_y, c.collision_grid_size_z],
-        "cic_grid": c.density_grid_size_x,
-        "dt": c.dt,
+        if "1m" in workload else "see world_b200/scenes.py",
+        "collision_grid": [spec.collision_grid_size_x, spec.collision_grid_size_y,
+                           spec.collision_grid_size_z],
+        "cic_grid": spec.density_grid_size_x,
+        "dt": spec.dt,
         "l2": "flushed (512 MiB write) before every timed step, flush not timed",
-        "neighbor_skin_m": c.neighbor_skin,
     }
     if scenes is not None:
         out["scenes"] = scenes
         out["diameters"] = "uniform [0.9d, 1.1d]"
         out["collision_grid"] = "per scene (world_b200/scenes.py)"
-        out["mu"] = "per scene" if args.workload == "design_256" else c.physics.friction
+        out["mu"] = "per scene" if workload == "design_256" else spec.physics.friction
     return out
 
 
@@ -205,19 +220,22 @@ def profiled_traffic(workload: str, kernel: str):
 
 
 # ------------------------------------------------------------------ CPU side -----
+def _oracle_sim(scene, threads: int):
+    from oracle.oracle import OracleSim, lib as oracle_lib, params_from_config
+    from world_b200.scenes import grain_properties
+    import numpy as np
+    oracle_lib().dem_set_num_threads(threads)
+    material = np.full(scene.n, scene.spec.particle_material, np.int32)
+    radius, mass = grain_properties(scene.spec, material, scene.radius)
+    return OracleSim(params_from_config(scene.spec), scene.state, radius, mass), \
+        oracle_lib().dem_num_threads()
+
+
 def cpu_oracle_rate(scene, seconds: float, max_steps: int, warmup: int = 1,
                     threads: int | None = None):
     """The oracle port on the host cores (all unless `threads`): (grain-steps/s, steps,
     elapsed, threads)."""
-    from oracle.oracle import OracleSim, params_from_config
-    from world_b200.state_io import grain_properties
-    import numpy as np
-    threads = threads or os.cpu_count() or 1
-    from oracle.oracle import lib as oracle_lib
-    oracle_lib().dem_set_num_threads(threads)
-    material = np.full(scene.n, scene.cfg.particle_material, np.int32)
-    radius, mass = grain_properties(scene.cfg, material, scene.radius)
-    sim = OracleSim(params_from_config(scene.cfg), scene.state, radius, mass)
+    sim, used = _oracle_sim(scene, threads or os.cpu_count() or 1)
     for _ in range(max(0, warmup)):
         sim.step()
     steps = 0
@@ -226,28 +244,44 @@ def cpu_oracle_rate(scene, seconds: float, max_steps: int, warmup: int = 1,
         sim.step()
         steps += 1
     elapsed = time.perf_counter() - t0
-    return scene.n * steps / elapsed, steps, elapsed, oracle_lib().dem_num_threads()
+    return scene.n * steps / elapsed, steps, elapsed, used
 
 
 def run_reference(args) -> int:
+    """The reference arm: the oracle port on all host cores (module docstring)."""
     rank = env_int("RANK", 0)
     if rank != 0:
         return 0
-    from world_b200.scenes import scene_for
+    from world_b200.scenes import BATCHED_WORKLOADS, scene_for
+    if args.workload in BATCHED_WORKLOADS or args.workload == "adjoint_32k":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"the reference arm times single-scene workloads only ({args.workload})"}))
+        return 0
     scene = scene_for(args.workload, n=args.grains, seed=12345)
-    budget = min(60.0, max(10.0, 0.5 * args.steps))
-    rate, steps, elapsed, threads = cpu_oracle_rate(scene, budget, args.steps,
-                                                    warmup=min(args.warmup, 1))
+    sim, threads = _oracle_sim(scene, os.cpu_count() or 1)
+    for _ in range(args.warmup):
+        sim.step()
+    # one step gives the rate; K is capped so the run ends within about four minutes
+    t0 = time.perf_counter()
+    sim.step()
+    first = time.perf_counter() - t0
+    steps = max(1, min(args.steps, int(240.0 / max(first, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step()
+    elapsed = time.perf_counter() - t0
+    rate = scene.n * steps / elapsed
     sample = (f"{steps} of {args.steps} requested steps of the full {scene.n}-grain workload "
-              f"({elapsed:.1f} s, bounded at {budget:.0f} s); the reference has no CPU step, so "
-              "this is its algorithm restated in C (oracle/dem_oracle.c)")
+              f"after {args.warmup} untimed warm-up steps ({elapsed:.1f} s on {threads} host "
+              "threads); the reference's step is CUDA only, so this is its algorithm "
+              "restated in C (oracle/dem_oracle.c)")
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
-        "n_gpus": args.gpus, "steps": steps, "warmup": min(args.warmup, 1),
-        "ms_per_step": 1e3 * elapsed / max(steps, 1), "higher_is_better": True,
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-        "data": "synthetic (seeded column collapse)",
-        "config": workload_config(scene, args),
+        "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
+        "config": workload_config(scene.spec, args.workload, scene.n),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -257,6 +291,150 @@ def run_reference(args) -> int:
 
 
 # ------------------------------------------------------------------ GPU side -----
+def _timed_steps(sim, stream, flush, steps: int) -> float:
+    """Device time (ms) of `steps` steps: each an L2 flush (512 MiB write) queued on the
+    library's stream, then the step bracketed by events on that stream. Nothing syncs
+    the host inside the loop, so launches run ahead of the GPU and the events time only
+    the steps."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            sim.take_step()
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev)
+
+
+def _contact_roofline(sim, stream, flush, spec, phase_steps: int, direct: bool) -> dict:
+    """The contact kernel's algorithmic bytes per launch over its event-timed duration,
+    from a direct-launch pass of `phase_steps` steps of the same workload (L2 flushed
+    before each step)."""
+    import numpy as np
+    import torch
+    n = sim.n
+    lists = sim.tuning()["neighbor_skin_m"] > 0
+    picard = spec.time_integrator != "semi_implicit_euler"
+    sim.set_kernel_timing(True)
+    iters0 = sim.picard_counts()[0]
+    t0 = sim._timings()
+    builds0 = sim.list_stats()[0]
+    exact0 = sim.list_exact_count()
+    with torch.cuda.stream(stream):
+        for k in range(phase_steps):
+            flush.fill_(float(k))
+            sim.take_step()
+    sim.synchronize()
+    t1 = sim._timings()
+    sim.set_kernel_timing(direct)
+    build_frac = (sim.list_stats()[0] - builds0) / phase_steps
+    exact_frac = (sim.list_exact_count() - exact0) / phase_steps
+    search_ms = float(t1[0] - t0[0]) / phase_steps
+    contact_ms = float(t1[1] - t0[1]) / phase_steps
+    # backward Euler / Picard: the timed contact phase is the whole step, one contact
+    # launch per executed iteration (plus, without lists, each iteration's search)
+    phase_iters = (sim.picard_counts()[0] - iters0) / phase_steps if picard else 1.0
+    mean_list = sim.list_stats()[2]
+    cnt, _, _ = sim.get_history()
+    entries = int(cnt.astype(np.int64).sum())
+    # contact kernel, algorithmic bytes per launch. Searched step: read x,r / v,m / id
+    # (36 B) and write x,r / v,m / id / a (52 B) per grain. History rows read and
+    # written (16 B per entry each way) plus the per-grain counts (4 B each way).
+    hist_bytes = (2 * 16 * entries + 8 * n) if spec.history else 0
+    if not lists:
+        contact_bytes = 88 * n + hist_bytes
+    elif not picard:
+        # lists, semi-implicit Euler: read x,r / v,m / id and the list count (40 B), the
+        # list (4 B per entry), the build position on the steps that measure it; write
+        # x,r / v,m / a (48 B) and the id only on the step after a build
+        contact_bytes = int(88 * n + hist_bytes + 4 * mean_list * n + 16 * n * exact_frac
+                            + 4 * n * build_frac)
+    else:
+        # lists, one Picard iteration: as the searched step plus the list count, the
+        # build position, the step-start state (32 B) and the rhs copy (20 B)
+        contact_bytes = int(88 * n + hist_bytes + 4 * mean_list * n + 72 * n)
+    kernel_ms = contact_ms / phase_iters
+    achieved = contact_bytes / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = measured_hbm_peak()
+    variant = sim.tuning()["contact_variant"]
+    symbol = ("k_force_list_staged" if variant.startswith("bulk-staged") else
+              "k_force_list_coop" if variant.startswith("warp-cooperative") else
+              "k_force_list") if lists else "k_force"
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "symbol": symbol,
+            "kernel": (f"{symbol} (contacts from Verlet lists + integrator; {variant})" if lists
+                       else "k_force (contact forces + integrator)"),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+            if peak_kind == "measured" else "fallback 6.65 TB/s",
+            "algorithmic_bytes_per_launch": contact_bytes,
+            "measuring_step_fraction": exact_frac if lists else None,
+            "build_step_fraction": build_frac if lists else None,
+            "kernel_ms": kernel_ms, "search_ms": search_ms,
+            "history_entries_per_grain": entries / n,
+            "mean_list_length": mean_list if lists else None}
+
+
+def _settled(sim, scene, stream, flush, args, plain_value: float, done: int,
+             total_steps: int) -> dict:
+    """The same column once it has collapsed onto the floor: advance the plain run from
+    `done` to `total_steps` steps from rest, re-tune, then time K steps and the contact
+    kernel's roofline as for the headline."""
+    import torch
+    t0 = time.perf_counter()
+    sim.advance(max(0, total_steps - done))
+    sim.synchronize()
+    preroll_s = time.perf_counter() - t0
+    tuned = None
+    if args.skin < 0:
+        sim.autotune(steps=40)
+        tuned = sim.tuning()
+    sim.advance(args.warmup)
+    builds0 = sim.list_stats()[0]
+    ms = _timed_steps(sim, stream, flush, args.steps)
+    builds = sim.list_stats()[0] - builds0
+    value = sim.n * args.steps / (ms / 1e3)
+    roof = _contact_roofline(sim, stream, flush, scene.spec, args.phase_steps, args.direct)
+    torch.cuda.synchronize()
+    return {"value": value, "unit": UNIT, "ms_per_step": ms / args.steps,
+            "steps": args.steps, "after_steps": total_steps,
+            "pre_roll_seconds": preroll_s, "over_plain": value / plain_value,
+            "builds_timed": builds, "mean_list_length": roof["mean_list_length"],
+            "history_entries_per_grain": roof["history_entries_per_grain"],
+            "roofline": {k: roof[k] for k in ("achieved", "peak", "frac", "kernel",
+                                               "algorithmic_bytes_per_launch", "kernel_ms",
+                                               "measuring_step_fraction",
+                                               "build_step_fraction")},
+            "autotuned": tuned}
+
+
+def _batched(workload: str, args, flush, plain_value: float) -> dict:
+    """One batched ensemble on this GPU: every scene in one SceneBatch, the autotuner's
+    schedule, K timed steps with the L2 flushed before each."""
+    import torch
+    from world_b200 import SceneBatch
+    from world_b200.scenes import ensemble_for
+    t0 = time.perf_counter()
+    members = ensemble_for(workload)
+    batch = SceneBatch.from_scenes(members)
+    setup_s = time.perf_counter() - t0
+    batch.autotune(steps=20) if args.skin < 0 else batch.set_neighbor_skin(max(args.skin, 0.0))
+    stream = torch.cuda.ExternalStream(batch.stream_ptr())
+    batch.advance(args.warmup)
+    batch.synchronize()
+    ms = _timed_steps(batch, stream, flush, args.steps)
+    value = batch.n * args.steps / (ms / 1e3)
+    out = {"value": value, "unit": UNIT, "scenes": len(members), "grains": batch.n,
+           "ms_per_step": ms / args.steps, "steps": args.steps, "over_plain": value / plain_value,
+           "setup_seconds": setup_s, "schedule": batch.tuning(),
+           "mean_list_length": batch.list_stats()[2]}
+    batch.close()
+    return out
+
+
 def run_ours(args) -> int:
     import numpy as np
     import torch
@@ -284,40 +462,33 @@ def run_ours(args) -> int:
         if world > 1:
             dist.barrier()
 
-    def with_skin(sc):
-        sc.cfg.neighbor_skin = max(args.skin, 0.0)
-        return sc
-
     scenes_total = None
     if args.workload in BATCHED_WORKLOADS:
         # scenes shared out over the ranks, balanced by grain count; each rank steps
         # its share as one batch
         members = ensemble_for(args.workload)
         mine = shard_scenes([m.n for m in members], world)[rank]
-        skin = with_skin(members[mine[0]]).cfg.neighbor_skin
         for i in mine:
-            members[i].cfg.neighbor_skin = skin
+            members[i].cfg.neighbor_skin = max(args.skin, 0.0)
         sim = SceneBatch.from_scenes([members[i] for i in mine])
         scene = members[mine[0]]
         scenes_total = len(members)
     else:
-        scene = with_skin(scene_for(args.workload, n=args.grains, seed=12345 + rank))
+        scene = scene_for(args.workload, n=args.grains, seed=12345 + rank)
+        scene.cfg.neighbor_skin = max(args.skin, 0.0)
         sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
     sim.set_kernel_timing(args.direct)
     tuned = None
     if args.skin < 0:
         # the autotuner picks the skin and the contact kernel's block size (untimed;
         # the state is restored and the results do not depend on the choice)
-        skin, _ = sim.autotune(steps=40)
-        scene.cfg.neighbor_skin = skin
+        sim.autotune(steps=40)
         tuned = sim.tuning()
     elif args.contact_kernel:
         block, variant = (int(v) for v in args.contact_kernel.split(","))
         sim.set_contact_kernel(block, variant)
-    variant_name = sim.tuning()["contact_variant"]
-    kernel_symbol = ("k_force_list_staged" if variant_name.startswith("bulk-staged") else
-                     "k_force_list_coop" if variant_name.startswith("warp-cooperative") else
-                     "k_force_list")
+    skin = sim.tuning()["neighbor_skin_m"]
+    lists = skin > 0
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -329,36 +500,23 @@ def run_ours(args) -> int:
     sampler = ClockSampler(range(world) if world > 1 else [local]) if rank == 0 else None
     if sampler:
         sampler.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
     torch.cuda.synchronize()
     radix0, radix_each = sim.radix_search_count()
     builds0, build_kernels, _ = sim.list_stats()
-    picard = scene.cfg.time_integrator != "semi_implicit_euler"
+    picard = scene.spec.time_integrator != "semi_implicit_euler"
     iters0, redos0 = sim.picard_counts()
     barrier()
-    # Each step: an L2 flush (512 MiB write) queued on the library's stream, then the
-    # step bracketed by events on that stream. Nothing syncs the host inside the loop,
-    # so launches run ahead of the GPU and the events time only the step.
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            ev[k][0].record(stream)
-            sim.take_step()
-            ev[k][1].record(stream)
-    torch.cuda.synchronize()
+    local_ms = _timed_steps(sim, stream, flush, args.steps)
     barrier()
     clocks = sampler.stop() if sampler else None
     radix_searches = sim.radix_search_count()[0] - radix0
     builds, _, mean_list = sim.list_stats()
     builds -= builds0
     iters1, redos1 = sim.picard_counts()
-    lists = scene.cfg.neighbor_skin > 0
     # list mode: a build launches the whole search (its radix kernels gated) and the
     # list kernels; otherwise a search adds the radix kernels only when it takes them
     launches = sim.kernels_per_step() * args.steps + (
         builds * build_kernels if lists else radix_searches * radix_each)
-    local_ms = sum(a.elapsed_time(b) for a, b in ev)
     total_ms = max_over_ranks(local_ms)
     all_grains = n
     if world > 1:
@@ -367,45 +525,8 @@ def run_ours(args) -> int:
         all_grains = int(t.item())
     value = all_grains * args.steps / (total_ms / 1e3)
 
-    # per-phase timing of the same workload for the roofline (direct launches)
-    sim.set_kernel_timing(True)
-    t0 = sim._timings()
-    phase_builds0 = sim.list_stats()[0]
-    phase_exact0 = sim.list_exact_count()
-    with torch.cuda.stream(stream):
-        for k in range(args.phase_steps):
-            flush.fill_(float(k))
-            sim.take_step()
-    sim.synchronize()
-    t1 = sim._timings()
-    sim.set_kernel_timing(args.direct)
-    build_frac = (sim.list_stats()[0] - phase_builds0) / args.phase_steps
-    exact_frac = (sim.list_exact_count() - phase_exact0) / args.phase_steps
-    search_ms = float(t1[0] - t0[0]) / args.phase_steps
-    contact_ms = float(t1[1] - t0[1]) / args.phase_steps
-    # backward Euler / Picard: the timed contact phase is the whole step, one contact
-    # launch per executed iteration (plus, without lists, each iteration's search)
-    phase_iters = (sim.picard_counts()[0] - iters1) / args.phase_steps if picard else 1.0
-    cnt, _, _ = sim.get_history()
-    entries = int(cnt.astype(np.int64).sum())
-    # contact kernel, algorithmic bytes per launch. Searched step: read x,r / v,m / id
-    # (36 B) and write x,r / v,m / id / a (52 B) per grain. History rows read and
-    # written (16 B per entry each way) plus the per-grain counts (4 B each way).
-    hist_bytes = (2 * 16 * entries + 8 * n) if scene.cfg.history else 0
-    if not lists:
-        contact_bytes = 88 * n + hist_bytes
-    elif not picard:
-        # lists, semi-implicit Euler: read x,r / v,m / id and the list count (40 B), the
-        # list (4 B per entry), the build position on the steps that measure it; write
-        # x,r / v,m / a (48 B) and the id only on the step after a build
-        contact_bytes = int(88 * n + hist_bytes + 4 * mean_list * n + 16 * n * exact_frac
-                            + 4 * n * build_frac)
-    else:
-        # lists, one Picard iteration: as the searched step plus the list count, the
-        # build position, the step-start state (32 B) and the rhs copy (20 B)
-        contact_bytes = int(88 * n + hist_bytes + 4 * mean_list * n + 72 * n)
-    achieved = contact_bytes * phase_iters / (contact_ms / 1e3) / 1e9
-    peak, peak_kind = measured_hbm_peak()
+    roof = _contact_roofline(sim, stream, flush, scene.spec, args.phase_steps, args.direct)
+    roof["traffic"] = profiled_traffic(args.workload, roof["symbol"])
 
     # e2e through the C ABI with pinned host buffers: every step uploads its state and
     # downloads its positions; the asynchronous calls overlap the upload of one step
@@ -444,6 +565,21 @@ def run_ours(args) -> int:
         scene_results = {"scenes": int(len(energies)), "energy_sum_J": float(np.sum(energies)),
                          "energy_min_J": float(np.min(energies))}
 
+    # contact-bearing regime, batched ensembles and the reverse pass beside the plain
+    # step (one GPU, default workload only)
+    extras = world == 1 and not args.no_extras and args.workload == "collapse_1m_sie_mu05" \
+        and args.grains is None
+    settled = batched = adjoint = None
+    if extras:
+        # steps from rest so far: warm-up, timed, roofline pass, and the last e2e step
+        # (each e2e step restarts from the same uploaded state)
+        done = args.warmup + args.steps + args.phase_steps + 1
+        settled = _settled(sim, scene, stream, flush, args, value, done, args.settled_steps)
+    sim.close()
+    if extras:
+        batched = {w: _batched(w, args, flush, value) for w in BATCHED_WORKLOADS}
+        adjoint = adjoint_measure(args, plain_value=value)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, steps, elapsed, threads = cpu_oracle_rate(scene, args.cpu_seconds, 10_000)
@@ -455,6 +591,10 @@ def run_ours(args) -> int:
                "one_core": {"value": rate1, "steps": steps1, "seconds": elapsed1}}
 
     if rank == 0:
+        roofline = {k: roof[k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic",
+                                         "kernel", "peak_source", "algorithmic_bytes_per_launch",
+                                         "measuring_step_fraction", "build_step_fraction",
+                                         "kernel_ms", "search_ms")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -462,58 +602,45 @@ def run_ours(args) -> int:
             "scaling": "strong" if scenes_total else "weak", "vs_baseline": None,
             "dtype": "fp32",
             "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
-            "config": workload_config(scene, args, grains=all_grains, scenes=scenes_total),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak,
-                         "traffic": profiled_traffic(args.workload, kernel_symbol if lists else "k_force"),
-                         "kernel": (f"{kernel_symbol} (contacts from Verlet lists + integrator; "
-                                    f"{variant_name})" if lists
-                                    else "k_force (contact forces + integrator)"),
-                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
-                         if peak_kind == "measured" else "fallback 6.65 TB/s",
-                         "algorithmic_bytes_per_launch": contact_bytes,
-                         "measuring_step_fraction": exact_frac if lists else None,
-                         "build_step_fraction": build_frac if lists else None,
-                         "kernel_ms": contact_ms / phase_iters, "search_ms": search_ms},
+            "config": workload_config(scene.spec, args.workload, all_grains, scenes=scenes_total),
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
                     "d2h_bytes_per_step": 12 * n, "steps": args.e2e_steps},
             "clocks": clocks,
             "gpu_launches": launches,
             "radix_searches_timed": radix_searches,
-            "neighbor_lists": {"skin_m": scene.cfg.neighbor_skin, "builds_timed": builds,
+            "neighbor_lists": {"skin_m": skin, "builds_timed": builds,
                                "mean_list_length": mean_list} if lists else None,
             "picard": {"iterations_per_step": (iters1 - iters0) / args.steps,
                        "redone_steps_timed": redos1 - redos0} if picard else None,
-            "history_entries_per_grain": entries / n,
+            "history_entries_per_grain": roof["history_entries_per_grain"],
             "scene_results": scene_results,
             "autotuned": tuned,
+            "settled": settled,
+            "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
     del flush
     if world > 1:
         dist.destroy_process_group()
     return 0
 
 
-def run_adjoint(args) -> int:
+def adjoint_measure(args, plain_value: float | None = None) -> dict:
     """Gradient of a density loss over a 200-step window of the 32,768-grain column
     after 12,000 steps (0.12 s: the lower layers have reached the floor and the column
-    is collapsing; before about 2,700 steps the lattice falls without a contact): loss = mean((rho_64^3(T) - rho_target)^2), target
-    from the same window with mu = 0.4, e = 0.6; gradients in v0 and (mu, e, k_n).
-    Reports the window's reverse pass in grain-steps/s and its cost relative to the
-    plain forward window on the same GPU. One GPU."""
-    import numpy as np
+    is collapsing; before about 2,700 steps the lattice falls without a contact): loss =
+    mean((rho_64^3(T) - rho_target)^2), target from the same window with mu = 0.4,
+    e = 0.6; gradients in v0 and (mu, e, k_n). The window's reverse pass in grain-steps/s
+    and its cost relative to the plain forward window on the same GPU."""
     import torch
 
     from world_b200 import ParticleDynamics
     from world_b200.adjoint import deposit, window
     from world_b200.scenes import column_collapse
 
-    if env_int("RANK", 0) != 0:
-        return 0
-    torch.cuda.set_device(env_int("LOCAL_RANK", 0))
     scene = column_collapse(32768, diameters="uniform", cic=64)
     cfg = scene.cfg
     cfg.kernel_timing = False
@@ -567,22 +694,42 @@ def run_adjoint(args) -> int:
     gradient()   # untimed: allocates the checkpoints and the tape, captures the graphs
     tv0, theta, loss, rec_ms, bwd_ms = gradient()
     n = sim.n
-    line = {
-        "metric": "adjoint grain-steps/s, 200-step window at 32,768 grains FP32",
-        "value": n * steps / (bwd_ms / 1e3), "unit": "grain-steps/s", "n_gpus": 1,
-        "steps": steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "fp32",
-        "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
-        "config": {"workload": "adjoint_32k", "grains": n, "pre_roll_steps": pre_roll,
-                   "window_steps": steps, "checkpoint_every": every, "cic_grid": 64,
-                   "loss": "mean((rho_T - rho_target)^2), target mu=0.4 e=0.6"},
+    sim.close()
+    out = {
+        "value": n * steps / (bwd_ms / 1e3), "unit": "grain-steps/s (reverse pass)",
+        "grains": n, "pre_roll_steps": pre_roll, "window_steps": steps,
+        "checkpoint_every": every, "cic_grid": 64,
+        "loss_definition": "mean((rho_T - rho_target)^2), target mu=0.4 e=0.6",
         "forward_window_ms": fwd_ms, "record_ms": rec_ms, "backward_ms": bwd_ms,
         "record_over_forward": rec_ms / fwd_ms, "backward_over_forward": bwd_ms / fwd_ms,
+        "gradient_over_forward": (rec_ms + bwd_ms) / fwd_ms,
         "loss": float(loss.detach()),
         "grad_theta": theta.grad.tolist(),
         "grad_v0_norm": float(tv0.grad.norm()),
     }
+    if plain_value is not None:
+        out["forward_window_grain_steps_per_s"] = n * steps / (fwd_ms / 1e3)
+    return out
+
+
+def run_adjoint(args) -> int:
+    """--workload adjoint_32k: adjoint_measure() as its own line. One GPU."""
+    import torch
+    if env_int("RANK", 0) != 0:
+        return 0
+    torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+    out = adjoint_measure(args)
+    line = {"metric": "adjoint grain-steps/s, 200-step window at 32,768 grains FP32",
+            "value": out["value"], "unit": "grain-steps/s", "n_gpus": 1,
+            "steps": out["window_steps"], "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "fp32", "data": "synthetic (seeded column collapse, world_b200/scenes.py)",
+            "config": {"workload": "adjoint_32k", "grains": out["grains"],
+                       "pre_roll_steps": out["pre_roll_steps"],
+                       "window_steps": out["window_steps"],
+                       "checkpoint_every": out["checkpoint_every"], "cic_grid": 64,
+                       "loss": out["loss_definition"]}}
+    line.update({k: v for k, v in out.items() if k not in ("value", "unit")})
     print(json.dumps(line), flush=True)
-    sim.close()
     return 0
 
 

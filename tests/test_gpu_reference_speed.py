@@ -19,68 +19,15 @@ import time
 import numpy as np
 import pytest
 
-from cases import write_state
 from conftest import scaled_error
+from scale_cases import compat_column
 from world_b200 import ParticleDynamics, load_config
-from world_b200.scenes import column_collapse
 
 pytestmark = pytest.mark.gpu
 
-YAML = """\
-simulation:
-  dt: 1.0e-5
-  collision_grid_size_x: 453
-  collision_grid_size_y: 453
-  collision_grid_size_z: 226
-  particles_per_cell: 8
-  threads_per_block: 256
-  density_grid_size_x: 128
-  density_grid_size_y: 128
-  density_grid_size_z: 128
-domain:
-  x_min: {xlo}
-  x_max: {xhi}
-  y_min: {xlo}
-  y_max: {xhi}
-  z_min: 0.0
-  z_max: {zhi}
-physics:
-  gravity: 9.81
-  particle_radius: 0.0025
-  max_force: 250.0
-  floor_z: 0.0
-  ceiling_z: {zhi}
-  wall_x_min: {xlo}
-  wall_x_max: {xhi}
-  wall_y_min: {xlo}
-  wall_y_max: {xhi}
-  restitution: 0.5
-  friction: 0.5
-materials:
-  masses: [0.0, {mass}]
-initialization:
-  type: file
-  state_path: {state_path}
-  particle_material: 1
-drivers:
-  kernel_timing: false
-time_integration:
-  solver: semi_implicit_euler
-  picard_iterations: 3
-"""
-
 
 def _compat_collapse(tmp_path):
-    sc = column_collapse(1 << 20, diameters="mono", mu=0.5, history=False, cic=128)
-    lx = sc.cfg.domain.x_max - sc.cfg.domain.x_min
-    mass = 2500.0 * 4.0 / 3.0 * np.pi * 0.0025 ** 3
-    state_path = tmp_path / "c1.bin"
-    write_state(str(state_path), sc.state)
-    yaml_path = tmp_path / "c1.yaml"
-    yaml_path.write_text(YAML.format(xlo=repr(-0.5 * lx), xhi=repr(0.5 * lx),
-                                     zhi=repr(float(sc.cfg.domain.z_max)),
-                                     mass=repr(float(np.float32(mass))),
-                                     state_path=state_path))
+    yaml_path, _ = compat_column(tmp_path, 1 << 20, cic=128, cell=7.0e-3)
     return yaml_path
 
 

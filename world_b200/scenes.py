@@ -14,33 +14,107 @@ the shapes, sizes and value distributions of the workloads they name:
   jittered body-centred-cubic lattice (simple cubic tops out at 0.524), velocities
   N(0, 0.5 m/s) per component.
 
-Each returns (SimConfig, state[n, 6], radius[n]); masses come from physics.density
-(2500 kg/m^3) inside the library. The collision cell is the larger of 1.1 d and the
-largest contact distance (2 r_max), so the 27-cell stencil sees every contact.
+Each returns a Scene: state[n, 6], radius[n] and the configuration as a ConfigSpec
+(plain values under SimConfig's member names); `Scene.cfg` is the library's SimConfig
+built from it on first use. Masses come from physics.density (2500 kg/m^3), as
+grain_properties() states. The collision cell is the larger of 1.1 d and the largest
+contact distance (2 r_max), so the 27-cell stencil sees every contact.
+
+This module needs numpy only: it does not load libworld_b200.so until `Scene.cfg` is
+read, so CPU-side tools (the oracle's timed baseline) can build the same scenes.
 """
 from __future__ import annotations
 
+import copy
 import math
-from dataclasses import dataclass
+from dataclasses import dataclass, field
+from types import SimpleNamespace
+from typing import Any
 
 import numpy as np
-
-from .config import SimConfig
 
 D_REF = 5e-3          # mean diameter d (m)
 N_REF = 32768         # grains of the 1.0 x 1.0 x 0.5 m reference column
 
 
+class ConfigSpec:
+    """The SimConfig members the scene generators set, as plain Python values under
+    the same names (`spec.domain.x_min`, `spec.physics.friction`, `spec.dt`, ...);
+    every other member keeps the reference's default (src/sim_config.h:68-199).
+    `to_config()` gives the library's SimConfig with these values."""
+
+    _TOP = ("dt", "collision_grid_size_x", "collision_grid_size_y", "collision_grid_size_z",
+            "particles_per_cell", "density_grid_size_x", "density_grid_size_y",
+            "density_grid_size_z", "history", "neighbor_skin", "time_integrator",
+            "picard_iterations", "picard_tolerance", "kernel_timing", "particle_material",
+            "masses")
+    _DOMAIN = ("x_min", "x_max", "y_min", "y_max", "z_min", "z_max")
+    _PHYSICS = ("gravity", "particle_radius", "max_force", "floor_z", "ceiling_z",
+                "wall_x_min", "wall_x_max", "wall_y_min", "wall_y_max", "restitution",
+                "friction", "normal_stiffness", "tangential_stiffness", "density")
+
+    def __init__(self) -> None:
+        # reference defaults for the members the generators leave alone
+        self.particle_material = 1
+        self.masses = [0.0, 0.04]
+        self.neighbor_skin = 0.0
+        self.kernel_timing = False
+        self.domain = SimpleNamespace(**{k: 0.0 for k in self._DOMAIN})
+        self.physics = SimpleNamespace(**{k: 0.0 for k in self._PHYSICS})
+
+    def copy(self) -> "ConfigSpec":
+        return copy.deepcopy(self)
+
+    def to_config(self):
+        from .config import SimConfig   # loads the library
+        cfg = SimConfig()
+        for k in self._TOP:
+            setattr(cfg, k, getattr(self, k))
+        for k in self._DOMAIN:
+            setattr(cfg.domain, k, getattr(self.domain, k))
+        for k in self._PHYSICS:
+            setattr(cfg.physics, k, getattr(self.physics, k))
+        return cfg
+
+
 @dataclass
 class Scene:
-    cfg: SimConfig
+    spec: ConfigSpec
     state: np.ndarray    # (n, 6) float32
     radius: np.ndarray   # (n,) float32
     name: str
+    _cfg: Any = field(default=None, repr=False)
 
     @property
     def n(self) -> int:
         return int(self.state.shape[0])
+
+    @property
+    def cfg(self):
+        """The library's SimConfig for this scene (built once; changes made to it stay
+        with the scene)."""
+        if self._cfg is None:
+            self._cfg = self.spec.to_config()
+        return self._cfg
+
+
+def grain_properties(cfg, material: np.ndarray,
+                     radius: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """Per-grain (radius, mass) the library derives when none are given: the global
+    particle_radius, and mass from physics.density (4/3 pi r^3 rho, evaluated in
+    double and rounded once to float) when it is set, else the materials.masses table.
+    `cfg` is a SimConfig or a ConfigSpec."""
+    n = material.size
+    r = np.full(n, np.float32(cfg.physics.particle_radius), np.float32) if radius is None \
+        else np.asarray(radius, np.float32)
+    rho = cfg.physics.density
+    if rho > 0:
+        rd = r.astype(np.float64)
+        m = (np.float64(np.float32(rho)) * 4.0 / 3.0 * np.pi * rd * rd * rd).astype(np.float32)
+    else:
+        table = np.asarray(cfg.masses, np.float32)
+        m = table[material]
+    return r, m
 
 
 def _diameters(rng: np.random.Generator, n: int, d: float, kind: str) -> np.ndarray:
@@ -70,7 +144,7 @@ def _cylinder_sites(n: int, spacing: float, radius_xy: float, z0: float) -> np.n
     return sites[:n]
 
 
-def _apply_common(cfg: SimConfig, box: tuple[float, float, float], d_max: float, d_mean: float,
+def _apply_common(cfg: ConfigSpec, box: tuple[float, float, float], d_max: float, d_mean: float,
                   *, mu: float, restitution: float, k_n: float, density: float, dt: float,
                   history: bool, integrator: str, picard_iterations: int, picard_tol: float,
                   cic: int, cell_factor: float = 1.1) -> None:
@@ -132,7 +206,7 @@ def column_collapse(n: int = N_REF, *, diameters: str = "uniform", seed: int = 1
     pos = sites + jitter
     state = np.zeros((n, 6), np.float32)
     state[:, :3] = pos.astype(np.float32)
-    cfg = SimConfig()
+    cfg = ConfigSpec()
     _apply_common(cfg, box, d_max, d, mu=mu, restitution=restitution, k_n=k_n, density=density,
                   dt=dt, history=history, integrator=integrator,
                   picard_iterations=picard_iterations, picard_tol=picard_tol, cic=cic)
@@ -152,7 +226,7 @@ def perturbed_members(base: Scene, members: int, sigma: float = 50e-6,
         st = base.state.copy()
         st[:, :3] = (st[:, :3].astype(np.float64) +
                      rng.normal(0.0, sigma, size=(base.n, 3))).astype(np.float32)
-        out.append(Scene(base.cfg.copy(), st, base.radius.copy(), f"{base.name} member={m}"))
+        out.append(Scene(base.spec.copy(), st, base.radius.copy(), f"{base.name} member={m}"))
     return out
 
 
@@ -207,7 +281,7 @@ def dense_box(n: int = 1 << 24, *, phi: float = 0.55, seed: int = 2024, mu: floa
     state = np.zeros((n, 6), np.float32)
     state[:, :3] = pos.astype(np.float32)
     state[:, 3:] = rng.normal(0.0, 0.5, size=(n, 3)).astype(np.float32)
-    cfg = SimConfig()
+    cfg = ConfigSpec()
     _apply_common(cfg, box, d, d, mu=mu, restitution=restitution, k_n=k_n, density=density,
                   dt=dt, history=history, integrator="semi_implicit_euler",
                   picard_iterations=8, picard_tol=1e-6, cic=cic)

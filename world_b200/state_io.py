@@ -18,6 +18,7 @@ import numpy as np
 
 from ._lib import check, lib, ptr
 from .config import SimConfig
+from .scenes import grain_properties  # noqa: F401  (pure numpy; re-exported here)
 
 
 def initial_state(cfg: SimConfig) -> tuple[np.ndarray, np.ndarray]:
@@ -29,24 +30,6 @@ def initial_state(cfg: SimConfig) -> tuple[np.ndarray, np.ndarray]:
     material = np.empty(n.value, np.int32)
     check(lib.wd_initial_state(cfg.handle, ptr(state), ptr(material), n.value, ctypes.byref(n)))
     return state, material
-
-
-def grain_properties(cfg: SimConfig, material: np.ndarray,
-                     radius: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
-    """Per-grain (radius, mass) the library derives when none are given: the global
-    particle_radius, and mass from physics.density (4/3 pi r^3 rho) when it is set,
-    else the materials.masses table."""
-    n = material.size
-    r = np.full(n, np.float32(cfg.physics.particle_radius), np.float32) if radius is None \
-        else np.asarray(radius, np.float32)
-    rho = cfg.physics.density
-    if rho > 0:
-        rd = r.astype(np.float64)
-        m = (np.float64(np.float32(rho)) * 4.0 / 3.0 * np.pi * rd * rd * rd).astype(np.float32)
-    else:
-        table = np.asarray(cfg.masses, np.float32)
-        m = table[material]
-    return r, m
 
 
 def write_state_file(path: str | os.PathLike, state: np.ndarray) -> None:
