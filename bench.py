@@ -86,6 +86,12 @@ def parse_args():
                     help="steps from rest before the contact-bearing (settled) measurement")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the settled, batched and adjoint sub-measurements")
+    ap.add_argument("--save-after", type=int, default=0, metavar="K",
+                    help="with --checkpoint PATH: advance the workload K steps from rest, write "
+                         "the checkpoint (state file + sidecar with springs) and exit")
+    ap.add_argument("--checkpoint", default=None, metavar="PATH",
+                    help="start the workload from this checkpoint instead of from rest (or, "
+                         "with --save-after, write it)")
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="Verlet-list skin in m (simulation.neighbor_skin); negative: chosen by "
                          "the autotuner; 0: grid search every step, as the reference")
@@ -476,7 +482,21 @@ def run_ours(args) -> int:
     else:
         scene = scene_for(args.workload, n=args.grains, seed=12345 + rank)
         scene.cfg.neighbor_skin = max(args.skin, 0.0)
-        sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
+        if args.checkpoint and not args.save_after:
+            sim = ParticleDynamics.from_checkpoint(scene.cfg, args.checkpoint)
+        else:
+            sim = ParticleDynamics(scene.cfg, state=scene.state, radius=scene.radius)
+        if args.save_after:
+            # a contact-bearing starting point for profilers: K steps from rest, saved
+            if not args.checkpoint:
+                raise SystemExit("--save-after needs --checkpoint PATH")
+            sim.advance(args.save_after)
+            sim.write_checkpoint(args.checkpoint)
+            cnt = sim.get_history()[0]
+            print(json.dumps({"checkpoint": args.checkpoint, "steps": args.save_after,
+                              "grains": sim.n, "springs_per_grain": float(cnt.sum()) / sim.n}))
+            sim.close()
+            return 0
     sim.set_kernel_timing(args.direct)
     tuned = None
     if args.skin < 0:

@@ -250,6 +250,13 @@ int wd_compute_density_grid_device(wd_sim* sim, float* d_grid);
 /* compute_total_energy() (src/particle_dynamics.cu:296-308), summed in FP64. Like
  * the reference it re-runs the neighbor search on the current positions first. */
 int wd_compute_total_energy(wd_sim* sim, double* energy);
+/* Per-grain terms of compute_total_energy, by grain id (n doubles): kinetic, gravity
+ * and wall energy of the grain, the pair energy of its contacts with larger-id grains
+ * and the spring energy of its stored springs whose partner has a larger id (or is a
+ * wall). Summed over any partition of the grains they give the total once; the slab
+ * decomposition (world_b200/slab.py) sums its owned grains' and all-reduces. No
+ * counterpart in the reference (src/energy_kernel.cu:30-80 sums in one atomic). */
+int wd_grain_energies(wd_sim* sim, double* energies);
 /* Total momentum sum(m v) in FP64 (extension). */
 int wd_compute_momentum(wd_sim* sim, double* momentum3);
 
@@ -284,6 +291,14 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
  * autotuner's other choices); results do not depend on them. */
 int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant);
 int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant);
+/* Test hook for the bulk-staged contact kernel's bounded waits (no counterpart in the
+ * reference). wait_us: the limit of each wait for a stage of bulk copies (0: one
+ * second). stall != 0: each warp's first stage is made to expect 16 bytes that no copy
+ * delivers, so its wait runs out; the kernel then returns without finishing that warp's
+ * tiles, and the next synchronizing call returns WD_ERR_CUDA once with "did not
+ * complete within its wait limit" (the state of that step is invalid: restore one with
+ * wd_set_state). No copy is ever left in flight. Handles with Verlet lists only. */
+int wd_debug_stage_wait(wd_sim* sim, int32_t stall, int32_t wait_us);
 /* Verlet lists: steps so far whose contact kernel measured the exact displacement
  * since the build (reading the build positions). The other steps decide on a bound:
  * the last exact value plus the largest per-step displacement of each step since. */
@@ -323,11 +338,14 @@ int wd_kernels_per_step(const wd_sim* sim, int64_t* kernels);
  * node-centred grid [lo, hi] with size[a] nodes per axis, d_grid = 4*nodes floats.
  * The scratch (64-bit accumulators and channel bounds) is one static device array
  * sized for WD_NOALLOC_MAX_NODES nodes (8 MiB), held by every GPU that loads the
- * library until the process exits; larger grids return WD_ERR_CAPACITY. The first
- * call on each device looks that array up (cudaGetSymbolAddress) and should come
- * before any stream capture. Every call shares the array and clears it first, so
- * calls that overlap on the GPU (different streams or threads) race. Work is queued
- * on `stream` (cudaStream_t as void*, NULL = default stream). */
+ * library until the process exits; larger grids return WD_ERR_CAPACITY. Every call
+ * looks that array's address up in the current context (cudaGetSymbolAddress, host
+ * side only), so it stays valid after cudaDeviceReset; the first call on a device
+ * also loads the library's device code there and should come before any stream
+ * capture. Every call shares the array and clears it first, so calls that overlap on
+ * the GPU (different streams or threads) race. A NaN or infinite mass or momentum
+ * makes its whole channel NaN. Work is queued on `stream` (cudaStream_t as void*,
+ * NULL = default stream). */
 #define WD_NOALLOC_MAX_NODES (64 * 64 * 64)
 int wd_deposit_grid_noalloc(const float* d_state, const float* d_mass, int64_t n,
                             const float* lo3, const float* hi3, const int32_t* size3,

@@ -159,9 +159,15 @@ def test_copy_is_independent():
     assert a.physics.friction == pytest.approx(0.5)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference tree not present")
+def _reference_root() -> str:
+    """The reference tree the oracle's build recipe reads (oracle/build.py)."""
+    from oracle import build as oracle_build
+    return os.path.dirname(oracle_build.REFERENCE_SRC.rstrip("/"))
+
+
+@pytest.mark.skipif(not os.path.isdir(_reference_root()), reason="reference tree not present")
 def test_every_reference_yaml_loads_without_unknown_keys():
-    files = [f for f in glob.glob("/root/reference/**/*.yaml", recursive=True)]
+    files = [f for f in glob.glob(os.path.join(_reference_root(), "**", "*.yaml"), recursive=True)]
     assert files
     for f in files:
         cfg = SimConfig()

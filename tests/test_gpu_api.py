@@ -5,6 +5,8 @@ from __future__ import annotations
 
 import ctypes
 
+import os
+
 import numpy as np
 import pytest
 
@@ -175,7 +177,8 @@ def test_checkpoint_resume_is_bit_identical(tmp_path):
     a.advance(5)
     path = str(tmp_path / "ck.bin")
     a.write_checkpoint(path)
-    ck = read_checkpoint(path)
+    ck = read_checkpoint(path, verify=True)
+    assert not os.path.exists(path + ".tmp") and not os.path.exists(path + ".sidecar.tmp")
     np.testing.assert_array_equal(ck["state"].reshape(-1), a.get_state())
     assert ck["time"] == np.float32(a.time) and ck["dt"] == np.float32(8e-6)
     cnt, part, xi = a.get_history()
@@ -198,6 +201,11 @@ def test_checkpoint_resume_is_bit_identical(tmp_path):
     np.testing.assert_array_equal(read_state_file(str(tmp_path / "s.bin")).reshape(-1), a.get_state())
     frame = a.pack_frame([1.0, 2.0, 3.0, 4.0, 5.0])
     np.testing.assert_array_equal(frame[:3 * a.n], a.get_positions())
+    # a state file that is not the one the sidecar was written with is refused, even
+    # with the same grain count (a crash between the two renames leaves that pair)
+    a.write_state_file(path)
+    with pytest.raises(WorldError, match="another state file"):
+        ParticleDynamics.from_checkpoint(cfg, path)
     assert frame[3 * a.n] == np.float32(a.time)
     np.testing.assert_array_equal(frame[3 * a.n + 1:], [1, 2, 3, 4, 5])
     a.close(); b.close()

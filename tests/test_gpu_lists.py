@@ -294,3 +294,34 @@ def test_batched_picard_on_lists():
         b.advance(50)
         sims.append(b)
     _same(*sims)
+
+
+def test_bulk_staged_wait_runs_out_and_the_handle_recovers():
+    """The bulk-staged kernel's bounded wait: a stage made to expect bytes that no copy
+    delivers (wd_debug_stage_wait) runs out after 2 ms; the next synchronizing call
+    reports it once, and after a state restore the handle steps as a fresh one does."""
+    from world_b200 import WorldError
+    from world_b200._lib import check, lib
+    cfg, st, rad = packed_poly(n=3000, seed=21, mu=0.5)
+    cfg.neighbor_skin = 0.5e-3
+    cfg.kernel_timing = False
+    sim = ParticleDynamics(cfg, state=st, radius=rad)
+    sim.set_contact_kernel(256, 1)
+    sim.advance(10)
+    saved, springs = sim.get_state(), sim.get_history()
+    check(lib.wd_debug_stage_wait(sim.handle, 1, 2000))
+    sim.take_step()
+    with pytest.raises(WorldError, match="wait limit"):
+        sim.synchronize()
+    sim.synchronize()                       # reported once; the context is usable
+    check(lib.wd_debug_stage_wait(sim.handle, 0, 0))
+    sim.set_state(saved)
+    sim.set_history(*springs)
+    sim.advance(20)
+    fresh = ParticleDynamics(cfg, state=saved, radius=rad)
+    fresh.set_contact_kernel(256, 1)
+    fresh.set_history(*springs)
+    fresh.advance(20)
+    _same(sim, fresh)
+    sim.close()
+    fresh.close()

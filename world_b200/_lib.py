@@ -80,6 +80,7 @@ SIGNATURES = {
     "wd_list_exact_count": ([_p, _i64], c_int),
     "wd_get_tuning": ([_p, POINTER(c_float), POINTER(c_int32), POINTER(c_int32)], c_int),
     "wd_set_contact_kernel": ([_p, c_int32, c_int32], c_int),
+    "wd_debug_stage_wait": ([_p, c_int32, c_int32], c_int),
     "wd_set_state_async": ([_p, _p], c_int),
     "wd_get_positions_async": ([_p, _p], c_int),
     "wd_io_join": ([_p], c_int),
@@ -113,6 +114,7 @@ SIGNATURES = {
     "wd_compute_density_grid": ([_p, _p], c_int),
     "wd_compute_density_grid_device": ([_p, _p], c_int),
     "wd_compute_total_energy": ([_p, _d], c_int),
+    "wd_grain_energies": ([_p, _d], c_int),
     "wd_compute_momentum": ([_p, _d], c_int),
     "wd_is_stable": ([_p, _i32], c_int),
     "wd_compute_max_acceleration": ([_p, _f], c_int),

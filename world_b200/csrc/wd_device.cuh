@@ -35,6 +35,8 @@ enum Counter : int {
 struct DevParams {
     float lo[3], hi[3];        // domain box
     int grid[3];               // collision grid
+    float inv_len[3];          // 1 / (hi - lo) rounded to float, per axis (cell_axis)
+    float cell_err[3];         // (grid + 1) * 2^-20: cell_axis's fast-path margin
     int ppc;                   // particles_per_cell
     float gravity;
     float max_force;           // clamp (+inf: none)
@@ -72,16 +74,37 @@ __device__ __forceinline__ const DevParams& scene_params(const DevParams& P, con
 
 // reference src/find_neighbors_kernel.cu:11-22. __float2int_rz is cvt.rzi.s32.f32,
 // the conversion static_cast<int>(float) compiles to.
-__device__ __forceinline__ int cell_axis(float x, float lo, float hi, int g) {
+__device__ __forceinline__ int cell_axis_exact(float x, float lo, float hi, int g) {
     const float t = (x - lo) / (hi - lo) * static_cast<float>(g);
     return min(g - 1, max(0, __float2int_rz(t)));
 }
 
+// The same integer without the division where that is provably safe. With u = x - lo
+// (the same rounded difference), t' = (u * inv) * g, inv = 1/(hi - lo) rounded, differs
+// from the reference's t = (u / (hi - lo)) * g by at most 5 roundings of 2^-24 relative:
+// below (g + 1) 2^-21.4 for t' in [-0.5, g + 0.5), a third of `err` = (g + 1) 2^-20. So
+// where t' is farther than err from every integer, trunc(t) and floor(t') agree after
+// the clamp to [0, g - 1] (t' < -0.5 and t' >= g + 0.5 clamp alike); elsewhere, and
+// for NaN, the exact expression decides. About 2 err of all values take it.
+__device__ __forceinline__ int cell_axis(float x, float lo, float hi, int g, float inv, float err) {
+    const float t = ((x - lo) * inv) * static_cast<float>(g);
+    if (t >= -0.5f && t < static_cast<float>(g) + 0.5f) {
+        const float k = floorf(t);
+        const float f = t - k;
+        if (f >= err && f <= 1.f - err) return min(g - 1, max(0, static_cast<int>(k)));
+    } else if (t < -0.5f) {
+        return 0;
+    } else if (t >= static_cast<float>(g) + 0.5f) {
+        return g - 1;
+    }
+    return cell_axis_exact(x, lo, hi, g);
+}
+
 __device__ __forceinline__ void cell_coords(const DevParams& P, float x, float y, float z,
                                             int& cx, int& cy, int& cz) {
-    cx = cell_axis(x, P.lo[0], P.hi[0], P.grid[0]);
-    cy = cell_axis(y, P.lo[1], P.hi[1], P.grid[1]);
-    cz = cell_axis(z, P.lo[2], P.hi[2], P.grid[2]);
+    cx = cell_axis(x, P.lo[0], P.hi[0], P.grid[0], P.inv_len[0], P.cell_err[0]);
+    cy = cell_axis(y, P.lo[1], P.hi[1], P.grid[1], P.inv_len[1], P.cell_err[1]);
+    cz = cell_axis(z, P.lo[2], P.hi[2], P.grid[2], P.inv_len[2], P.cell_err[2]);
 }
 
 // reference src/find_neighbors_kernel.cu:27-30 (x slowest, z fastest).

@@ -10,6 +10,7 @@
 // the field is bit-identical run to run and is the correctly rounded sum up to the
 // 2^-62-relative quantum. Grains are visited in cell order, so neighbouring lanes hit
 // the same nodes; identical nodes inside a warp are combined before the atomic.
+#include <cfloat>
 #include <cmath>
 
 #include "wd_kernels.h"
@@ -148,6 +149,12 @@ k_deposit_finish(int n, int64_t nodes, const uint32_t* __restrict__ bounds,
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= 4 * nodes) return;
     const int c = static_cast<int>(t / nodes);
+    // a NaN or infinite mass or momentum makes its whole channel NaN (the bound is the
+    // largest |value| by its bits, so it is not finite exactly when some value is not)
+    if (!(__uint_as_float(bounds[c]) <= FLT_MAX)) {
+        out[t] = __uint_as_float(0x7fc00000u);
+        return;
+    }
     const double inv = 1.0 / channel_scale(n, bounds[c]);
     out[t] = static_cast<float>(static_cast<double>(static_cast<long long>(acc[t])) * inv);
 }
@@ -256,6 +263,10 @@ k_deposit_finish_batch(const DevParams* __restrict__ params, int scenes, int64_t
     const DevParams& Q = params[lo];
     const int64_t nodes = static_cast<int64_t>(Q.dgrid[0]) * Q.dgrid[1] * Q.dgrid[2];
     const int c = static_cast<int>((t - 4 * static_cast<int64_t>(Q.node_base)) / nodes);
+    if (!(__uint_as_float(bounds[4 * lo + c]) <= FLT_MAX)) {   // non-finite input: NaN channel
+        out[t] = __uint_as_float(0x7fc00000u);
+        return;
+    }
     const double inv = 1.0 / channel_scale(Q.n, bounds[4 * lo + c]);
     out[t] = static_cast<float>(static_cast<double>(static_cast<long long>(acc[t])) * inv);
 }
@@ -303,7 +314,6 @@ void launch_deposit_batch(int n, const float4* pos, const float4* vel, SceneTab 
 // allocate). Inputs are the caller's own device arrays in the reference's AoS
 // layout; the scratch is the static array below, one per device, never freed.
 // ---------------------------------------------------------------------------------
-#include <mutex>
 #include <string>
 
 #include "../../include/world_b200.h"
@@ -315,9 +325,6 @@ constexpr long long kNoAllocNodes = WD_NOALLOC_MAX_NODES;
 // 4 channels of 64-bit accumulators, then 2 words holding the four 32-bit bounds.
 static __device__ __align__(256) unsigned long long g_deposit_scratch[4 * kNoAllocNodes + 2];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
 
 __global__ void __launch_bounds__(wd::kBlock)
 k_deposit_bounds_aos(int n, const float* __restrict__ state, const float* __restrict__ mass,
@@ -413,20 +420,14 @@ k_deposit_aos(int n, const float* __restrict__ state, const float* __restrict__ 
             }
 }
 
-// Device address of this device's scratch array, looked up once per device.
+// Device address of the scratch array in the current device's context. Looked up on
+// every call (a host-side table lookup, no allocation and no device work), so the
+// address stays right after a cudaDeviceReset or when another context is made current.
 cudaError_t scratch_for_current_device(unsigned long long** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_deposit_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_deposit_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = p;
-    }
-    *out = static_cast<unsigned long long*>(g_scratch_addr[dev]);
+    *out = static_cast<unsigned long long*>(p);
     return cudaSuccess;
 }
 

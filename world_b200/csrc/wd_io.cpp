@@ -5,13 +5,16 @@
 //
 // A checkpoint is that file plus a sidecar "<path>.sidecar" holding what the state file
 // lacks for a bit-identical resume (the reference saves none of it):
-//   char magic[8] = "WDCKPT01"; uint32 version = 1; uint32 flags (bit 0: history)
-//   int64 n; float32 time; float32 dt
+//   char magic[8] = "WDCKPT01"; uint32 version = 2; uint32 flags (bit 0: history)
+//   int64 n; float32 time; float32 dt; uint64 state_hash (version 2 only: 64-bit
+//   FNV-1a of the state file's bytes, so a sidecar never pairs with another state)
 //   float32 radius[n]; float32 mass[n]; int32 material[n]
 //   history only: int32 count[n]; int32 partner[n * 24]; float32 xi[n * 24 * 3]
 // all little-endian, arrays by grain id. The neighbor order is canonical (cell key,
 // then grain id), so it needs no saving: the first search of the resumed handle
-// rebuilds it.
+// rebuilds it. Both files are written under temporary names and renamed into place,
+// the state file first; a crash between the two renames leaves a new state file with
+// the old sidecar, which the hash rejects. Version-1 sidecars (no hash) still load.
 //
 // Broadcast frame (src/broadcast.cpp:95-108): 3n position floats by grain id, then
 // sim time, real-time ratio, find-neighbors / compute-rhs / take-step / unpack times.
@@ -27,7 +30,7 @@
 namespace {
 
 constexpr char kMagic[8] = {'W', 'D', 'C', 'K', 'P', 'T', '0', '1'};
-constexpr uint32_t kVersion = 1;
+constexpr uint32_t kVersion = 2;
 constexpr int kCap = WD_HIST_CAP;
 
 int fail(int code, const std::string& msg) {
@@ -47,6 +50,21 @@ struct File {
     bool get(T* p, size_t count) { return std::fread(p, sizeof(T), count, f) == count; }
 };
 
+uint64_t fnv1a(uint64_t h, const void* data, size_t bytes) {
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    for (size_t k = 0; k < bytes; ++k) {
+        h ^= p[k];
+        h *= 0x100000001b3ull;
+    }
+    return h;
+}
+constexpr uint64_t kFnvBasis = 0xcbf29ce484222325ull;
+
+uint64_t state_hash(int32_t count, const std::vector<float>& state) {
+    return fnv1a(fnv1a(kFnvBasis, &count, sizeof(count)), state.data(),
+                 state.size() * sizeof(float));
+}
+
 bool is_batch(const wd_sim* sim) {
     int32_t scenes = 1;
     wd_scene_count(sim, &scenes);
@@ -57,18 +75,39 @@ bool is_batch(const wd_sim* sim) {
 
 extern "C" {
 
-int wd_write_state_file(wd_sim* sim, const char* path) {
-    if (!sim || !path) return fail(WD_ERR_INVALID, "wd_write_state_file: NULL argument");
+namespace {
+
+// The state file's bytes for `sim`: its grain count and 6n floats.
+int read_state(wd_sim* sim, const char* who, int32_t* count, std::vector<float>* state) {
     int64_t n = 0;
     int rc = wd_get_n(sim, &n);
     if (rc) return rc;
-    if (n > INT32_MAX) return fail(WD_ERR_INVALID, "wd_write_state_file: n does not fit int32");
-    std::vector<float> state(static_cast<size_t>(6) * n);
-    rc = wd_get_state(sim, state.data());
+    if (n > INT32_MAX) return fail(WD_ERR_INVALID, std::string(who) + ": n does not fit int32");
+    state->resize(static_cast<size_t>(6) * n);
+    rc = wd_get_state(sim, state->data());
     if (rc) return rc;
+    *count = static_cast<int32_t>(n);
+    return WD_OK;
+}
+
+bool write_state_bytes(const std::string& path, int32_t count, const std::vector<float>& state) {
     File out(path, "wb");
-    const int32_t count = static_cast<int32_t>(n);
-    if (!out.f || !out.put(&count, 1) || !out.put(state.data(), state.size()))
+    const bool ok = out.f && out.put(&count, 1) && out.put(state.data(), state.size());
+    if (!out.f) return false;
+    const bool closed = std::fclose(out.f) == 0;
+    out.f = nullptr;
+    return ok && closed;
+}
+
+}  // namespace
+
+int wd_write_state_file(wd_sim* sim, const char* path) {
+    if (!sim || !path) return fail(WD_ERR_INVALID, "wd_write_state_file: NULL argument");
+    int32_t count = 0;
+    std::vector<float> state;
+    const int rc = read_state(sim, "wd_write_state_file", &count, &state);
+    if (rc) return rc;
+    if (!write_state_bytes(path, count, state))
         return fail(WD_ERR_IO, std::string("wd_write_state_file: cannot write ") + path);
     return WD_OK;
 }
@@ -76,10 +115,11 @@ int wd_write_state_file(wd_sim* sim, const char* path) {
 int wd_write_checkpoint(wd_sim* sim, const char* path) {
     if (!sim || !path) return fail(WD_ERR_INVALID, "wd_write_checkpoint: NULL argument");
     if (is_batch(sim)) return fail(WD_ERR_INVALID, "wd_write_checkpoint: not for a batch of scenes");
-    int rc = wd_write_state_file(sim, path);
+    int32_t count32 = 0;
+    std::vector<float> state;
+    int rc = read_state(sim, "wd_write_checkpoint", &count32, &state);
     if (rc) return rc;
-    int64_t n = 0;
-    wd_get_n(sim, &n);
+    const int64_t n = count32;
     float time = 0.f, dt = 0.f;
     wd_get_time(sim, &time);
     wd_get_dt(sim, &dt);
@@ -96,16 +136,35 @@ int wd_write_checkpoint(wd_sim* sim, const char* path) {
     bool history = false;
     for (int32_t c : count) history |= c > 0;
     const uint32_t flags = history ? 1u : 0u;
+    const uint64_t hash = state_hash(count32, state);
+    const std::string state_tmp = std::string(path) + ".tmp";
     const std::string side = std::string(path) + ".sidecar";
-    File out(side, "wb");
-    bool ok = out.f && out.put(kMagic, 8) && out.put(&kVersion, 1) && out.put(&flags, 1) &&
-              out.put(&n, 1) && out.put(&time, 1) && out.put(&dt, 1) &&
-              out.put(radius.data(), radius.size()) && out.put(mass.data(), mass.size()) &&
-              out.put(material.data(), material.size());
-    if (ok && history)
-        ok = out.put(count.data(), count.size()) && out.put(partner.data(), partner.size()) &&
-             out.put(xi.data(), xi.size());
-    if (!ok) return fail(WD_ERR_IO, "wd_write_checkpoint: cannot write " + side);
+    const std::string side_tmp = side + ".tmp";
+    if (!write_state_bytes(state_tmp, count32, state))
+        return fail(WD_ERR_IO, "wd_write_checkpoint: cannot write " + state_tmp);
+    {
+        File out(side_tmp, "wb");
+        bool ok = out.f && out.put(kMagic, 8) && out.put(&kVersion, 1) && out.put(&flags, 1) &&
+                  out.put(&n, 1) && out.put(&time, 1) && out.put(&dt, 1) && out.put(&hash, 1) &&
+                  out.put(radius.data(), radius.size()) && out.put(mass.data(), mass.size()) &&
+                  out.put(material.data(), material.size());
+        if (ok && history)
+            ok = out.put(count.data(), count.size()) && out.put(partner.data(), partner.size()) &&
+                 out.put(xi.data(), xi.size());
+        if (out.f) {
+            ok = (std::fclose(out.f) == 0) && ok;
+            out.f = nullptr;
+        }
+        if (!ok) {
+            std::remove(state_tmp.c_str());
+            std::remove(side_tmp.c_str());
+            return fail(WD_ERR_IO, "wd_write_checkpoint: cannot write " + side_tmp);
+        }
+    }
+    if (std::rename(state_tmp.c_str(), path) != 0)
+        return fail(WD_ERR_IO, std::string("wd_write_checkpoint: cannot rename into ") + path);
+    if (std::rename(side_tmp.c_str(), side.c_str()) != 0)
+        return fail(WD_ERR_IO, "wd_write_checkpoint: cannot rename into " + side);
     return WD_OK;
 }
 
@@ -129,11 +188,19 @@ int wd_create_from_checkpoint(const wd_config* cfg, const char* path, wd_sim** o
     if (!sc.f || !sc.get(magic, 8) || std::memcmp(magic, kMagic, 8) != 0 || !sc.get(&version, 1) ||
         !sc.get(&flags, 1) || !sc.get(&sn, 1) || !sc.get(&time, 1) || !sc.get(&dt, 1))
         return fail(WD_ERR_IO, "wd_create_from_checkpoint: missing or bad sidecar " + side);
-    if (version != kVersion)
+    if (version != 1 && version != kVersion)
         return fail(WD_ERR_IO, "wd_create_from_checkpoint: sidecar version " + std::to_string(version));
     if (sn != n)
         return fail(WD_ERR_IO, "wd_create_from_checkpoint: sidecar is for " + std::to_string(sn) +
                                    " grains, state file has " + std::to_string(n));
+    if (version >= 2) {
+        uint64_t hash = 0;
+        if (!sc.get(&hash, 1))
+            return fail(WD_ERR_IO, "wd_create_from_checkpoint: short sidecar " + side);
+        if (hash != state_hash(count, state))
+            return fail(WD_ERR_IO, "wd_create_from_checkpoint: " + side +
+                                       " was written with another state file than " + path);
+    }
     std::vector<float> radius(n), mass(n);
     std::vector<int32_t> material(n);
     if (!sc.get(radius.data(), radius.size()) || !sc.get(mass.data(), mass.size()) ||

@@ -143,9 +143,13 @@ void launch_force(const DevParams& P, const ForceArgs& a, bool picard, Skip skip
 // tests). Picard builds earlier, at kPicardBuildAt, so that its iterates rarely leave.
 constexpr float kListValid = 0.49f;
 constexpr float kPicardBuildAt = 0.30f;
+// kLcStallTest / kLcWaitUs: the bulk-staged contact kernel's wait test. A nonzero
+// kLcStallTest makes each warp's first stage expect 16 bytes that no copy delivers (no
+// copy is issued for it), so its bounded wait runs out; kLcWaitUs is that wait's limit
+// in microseconds (0: one second).
 enum ListCtrl {
     kLcDisp = 0, kLcOverflow = 1, kLcForce = 2, kLcDecision = 3, kLcViol = 4, kLcRedo = 5,
-    kLcStep = 6, kLcExact = 7, kLcBound = 8, kLcWords = 10
+    kLcStep = 6, kLcExact = 7, kLcBound = 8, kLcStallTest = 10, kLcWaitUs = 11, kLcWords = 12
 };
 struct ListArgs {
     const float4* pos; const float4* vel; const int* ids;  // state of the step

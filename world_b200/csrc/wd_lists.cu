@@ -530,12 +530,12 @@ __device__ __forceinline__ uint64_t global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded wait for a phase: false after about a second without completion.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for a phase: false after limit_ns without completion.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     while (!mbar_try_wait(bar, parity))
-        if (global_ns() - t0 > 1000000000ull) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     return true;
 }
 
@@ -573,6 +573,9 @@ k_force_list_staged(DevParams P0, ListArgs A) {
     const int first = blockIdx.x * kStageWarps + w;
     const bool exact = A.list_ctrl[kLcExact] != 0u;
     const bool order_out = A.list_ctrl[kLcDecision] != 0u;  // first step after a build
+    const uint32_t wait_us = A.list_ctrl[kLcWaitUs];
+    const uint64_t limit_ns = wait_us ? 1000ull * wait_us : 1000000000ull;
+    const bool stall_test = A.list_ctrl[kLcStallTest] != 0u;
     SlotStage* S = stage[w];
     uint64_t* bar = bars[w];
     // tiles of iterations it (cur, in stage it & 1) and it + 1 (nxt), in registers
@@ -581,7 +584,10 @@ k_force_list_staged(DevParams P0, ListArgs A) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         mbar_init_fence();
-        if (cur < whole) stage_issue<HIST, BATCH>(A, cur, exact, S[0], &bar[0]);
+        if (cur < whole) {
+            if (stall_test) mbar_expect_tx(&bar[0], 16u);   // nothing will arrive
+            else stage_issue<HIST, BATCH>(A, cur, exact, S[0], &bar[0]);
+        }
         if (nxt < whole) stage_issue<HIST, BATCH>(A, nxt, exact, S[1], &bar[1]);
     }
     __syncwarp();
@@ -596,7 +602,7 @@ k_force_list_staged(DevParams P0, ListArgs A) {
         float4 pi = make_float4(0.f, 0.f, 0.f, 0.f), vi = pi, xb = pi;
         int id = 0, cnt = 0, hcnt_in = 0, scene = 0;
         if (t < whole) {
-            const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar[st], (it >> 1) & 1));
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar[st], (it >> 1) & 1, limit_ns));
             if (!ok) {
                 failed = true;
                 break;
@@ -640,8 +646,8 @@ k_force_list_staged(DevParams P0, ListArgs A) {
         // (bounded); the step is left unfinished for the host to report
         if (lane == 0) {
             atomicAdd(&A.counters[kCntStageTimeout], 1ull);
-            if (cur < whole) mbar_wait(&bar[it & 1], (it >> 1) & 1);
-            if (nxt < whole) mbar_wait(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+            if (cur < whole) mbar_wait(&bar[it & 1], (it >> 1) & 1, limit_ns);
+            if (nxt < whole) mbar_wait(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1, limit_ns);
         }
     } else {
         list_disp_report<false>(A.list_ctrl, exact, disp_bits, step_bits);

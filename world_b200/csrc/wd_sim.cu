@@ -374,6 +374,10 @@ DevParams make_params(const wd::Config& c, int n, float dt) {
         P.lo[a] = c.dom_lo[a];
         P.hi[a] = c.dom_hi[a];
         P.grid[a] = c.grid[a];
+        // cell_axis's fast path: the float box length as the kernels round it
+        const float len = P.hi[a] - P.lo[a];
+        P.inv_len[a] = static_cast<float>(1.0 / static_cast<double>(len));
+        P.cell_err[a] = static_cast<float>(std::ldexp(static_cast<double>(P.grid[a]) + 1.0, -20));
     }
     P.ppc = c.particles_per_cell;
     P.gravity = c.gravity;
@@ -888,9 +892,12 @@ int sync_stream(wd_sim* s) {
         unsigned long long stalls = 0;
         WD_CUDA(cudaMemcpy(&stalls, s->counters + wd::kCntStageTimeout, sizeof(stalls),
                            cudaMemcpyDeviceToHost));
-        if (stalls)
+        if (stalls) {
+            // reported once: the handle stays usable (the caller restores a state)
+            WD_CUDA(cudaMemset(s->counters + wd::kCntStageTimeout, 0, sizeof(stalls)));
             return fail(WD_ERR_CUDA, "contact kernel: a bulk copy into shared memory did not "
                                      "complete within its wait limit; the state is invalid");
+        }
     }
     return WD_OK;
 }
@@ -1692,6 +1699,27 @@ int wd_compute_scene_energies(wd_sim* sim, double* energies) {
     return sync_stream(sim);
 }
 
+int wd_grain_energies(wd_sim* sim, double* energies) {
+    if (!sim || !energies) return fail(WD_ERR_INVALID, "wd_grain_energies: NULL argument");
+    int rc = ondemand_search(sim);
+    if (rc) return rc;
+    wd::launch_energy(sim->P, tab(sim, sim->sceneC), sim->posC, sim->velC, sim->idsC,
+                      sim->sb.table, sim->hist[sim->hist_cur], sim->hcnt_slot, sim->sb.src,
+                      segments(sim), sim->grain_vals, sim->partials, sim->scene_sums, sim->stream);
+    WD_CUDA(cudaGetLastError());
+    const size_t n = static_cast<size_t>(sim->n);
+    std::vector<double> by_slot(n);
+    std::vector<int32_t> ids(n);
+    WD_CUDA(cudaMemcpyAsync(by_slot.data(), sim->grain_vals, n * sizeof(double),
+                            cudaMemcpyDeviceToHost, sim->stream));
+    WD_CUDA(cudaMemcpyAsync(ids.data(), sim->idsC, n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            sim->stream));
+    rc = sync_stream(sim);
+    if (rc) return rc;
+    for (size_t k = 0; k < n; ++k) energies[ids[k]] = by_slot[k];
+    return WD_OK;
+}
+
 int wd_compute_total_energy(wd_sim* sim, double* energy) {
     if (!sim || !energy) return fail(WD_ERR_INVALID, "wd_compute_total_energy: NULL argument");
     std::vector<double> e(sim->scenes);
@@ -2083,6 +2111,19 @@ int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant) {
     sim->force_minb = variant <= 2 ? variant : (variant == 64 ? 4 : 5);
     sim->graph_dirty = true;
     clear_adj_graphs(sim);
+    return WD_OK;
+}
+
+int wd_debug_stage_wait(wd_sim* sim, int32_t stall, int32_t wait_us) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_debug_stage_wait: NULL handle");
+    if (!sim->list_ctrl)
+        return fail(WD_ERR_INVALID, "wd_debug_stage_wait: the handle has no Verlet lists");
+    if (wait_us < 0) return fail(WD_ERR_INVALID, "wd_debug_stage_wait: wait_us must be >= 0");
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    const uint32_t words[2] = {stall ? 1u : 0u, static_cast<uint32_t>(wait_us)};
+    WD_CUDA(cudaMemcpy(sim->list_ctrl + wd::kLcStallTest, words, sizeof(words),
+                       cudaMemcpyHostToDevice));
     return WD_OK;
 }
 

@@ -270,6 +270,14 @@ class ParticleDynamics:
         check(lib.wd_compute_total_energy(self._h, ctypes.byref(e)))
         return float(e.value)
 
+    def grain_energies(self) -> np.ndarray:
+        """Per-grain energy terms by grain id (float64): each pair's and each spring's
+        energy is carried by the smaller-id grain of the pair, so any partition of the
+        grains sums to compute_total_energy()."""
+        out = np.empty(self.n, np.float64)
+        check(lib.wd_grain_energies(self._h, ptr(out)))
+        return out
+
     def compute_momentum(self) -> np.ndarray:
         out = (ctypes.c_double * 3)()
         check(lib.wd_compute_momentum(self._h, out))

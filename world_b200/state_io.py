@@ -5,8 +5,9 @@ surrogate/decode_particles.py:355-361): little-endian int32 n, then n*6 float32 
 out [x, y, z, vx, vy, vz] per grain. Grains get `initialization.particle_material`.
 
 Checkpoint sidecar ("<state file>.sidecar", written by wd_write_checkpoint):
-"WDCKPT01", uint32 version 1, uint32 flags (bit 0: springs), int64 n, float32 time,
-float32 dt, float32 radius[n], float32 mass[n], int32 material[n], and with springs
+"WDCKPT01", uint32 version 2, uint32 flags (bit 0: springs), int64 n, float32 time,
+float32 dt, uint64 state_hash (64-bit FNV-1a of the state file's bytes; absent in
+version 1), float32 radius[n], float32 mass[n], int32 material[n], and with springs
 int32 count[n], int32 partner[n*24], float32 xi[n*24*3]; little-endian, by grain id.
 """
 from __future__ import annotations
@@ -54,11 +55,21 @@ def read_state_file(path: str | os.PathLike) -> np.ndarray:
 
 
 CKPT_MAGIC = b"WDCKPT01"
+
+
+def state_hash(data: bytes) -> int:
+    """64-bit FNV-1a of a state file's bytes (the checkpoint sidecar's state_hash)."""
+    h = 0xcbf29ce484222325
+    for b in data:
+        h = ((h ^ b) * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+    return h
 HIST_CAP = 24
 
 
-def read_checkpoint(path: str | os.PathLike) -> dict:
-    """The state file at path and its sidecar as arrays (a reader for tooling)."""
+def read_checkpoint(path: str | os.PathLike, verify: bool = False) -> dict:
+    """The state file at path and its sidecar as arrays (a reader for tooling). With
+    `verify`, the sidecar's state_hash is checked against the state file (a pure-Python
+    hash: seconds per MB; the library's loader always checks it)."""
     state = read_state_file(path)
     n = state.shape[0]
     with open(str(path) + ".sidecar", "rb") as f:
@@ -66,7 +77,7 @@ def read_checkpoint(path: str | os.PathLike) -> dict:
     if raw[:8] != CKPT_MAGIC:
         raise ValueError(f"{path}.sidecar: bad magic {raw[:8]!r}")
     version, flags = (int(v) for v in np.frombuffer(raw[8:16], "<u4"))
-    if version != 1:
+    if version not in (1, 2):
         raise ValueError(f"{path}.sidecar: version {version}")
     sn = int(np.frombuffer(raw[16:24], "<i8")[0])
     if sn != n:
@@ -74,6 +85,13 @@ def read_checkpoint(path: str | os.PathLike) -> dict:
     time, dt = (float(v) for v in np.frombuffer(raw[24:32], "<f4"))
     o = 32
     out = {"state": state, "time": np.float32(time), "dt": np.float32(dt)}
+    if version >= 2:
+        out["state_hash"] = int(np.frombuffer(raw[32:40], "<u8")[0])
+        if verify:
+            with open(path, "rb") as f:
+                if state_hash(f.read()) != out["state_hash"]:
+                    raise ValueError(f"{path}.sidecar was written with another state file")
+        o = 40
     for name, dtype, count in (("radius", "<f4", n), ("mass", "<f4", n), ("material", "<i4", n)):
         out[name] = np.frombuffer(raw[o:o + 4 * count], dtype).copy()
         o += 4 * count
