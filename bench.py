@@ -10,8 +10,11 @@ dt = 1e-5 s, 453 x 453 x 226 collision grid, 128^3 CIC grid; synthetic seeded in
 (world_b200/scenes.py). A step is one take_step() over all grains.
 
 value  -- device time of K steps (CUDA events on the library's stream around each
-          step; a 512 MiB write queued on the same stream before every step flushes
-          L2 and is not timed), max over ranks; grains x ranks x K / time.
+          step; before every step, untimed and on the same stream, a 512 MiB write
+          flushes L2 and a 512 MiB read of another buffer then replaces the flush's
+          dirty lines, so the step starts from a cold and clean L2 and does not pay
+          the flush's own write-backs), max over ranks; grains x ranks x K / time.
+          `write_flush` repeats the measurement with the write alone (dirty L2).
 e2e    -- the same metric through the C ABI with host buffers: each step
           wd_set_state_async() from pinned host memory, wd_step(1),
           wd_get_positions_async() to pinned host memory, all inside the timed region
@@ -86,6 +89,8 @@ def parse_args():
                     help="steps from rest before the contact-bearing (settled) measurement")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the settled, batched and adjoint sub-measurements")
+    ap.add_argument("--field-reps", type=int, default=5,
+                    help="timed CIC deposits and energy reductions of the headline state")
     ap.add_argument("--save-after", type=int, default=0, metavar="K",
                     help="with --checkpoint PATH: advance the workload K steps from rest, write "
                          "the checkpoint (state file + sidecar with springs) and exit")
@@ -127,7 +132,8 @@ def workload_config(spec, workload: str, grains: int, scenes=None) -> dict:
                            spec.collision_grid_size_z],
         "cic_grid": spec.density_grid_size_x,
         "dt": spec.dt,
-        "l2": "flushed (512 MiB write) before every timed step, flush not timed",
+        "l2": "flushed before every timed step (512 MiB write, then a 512 MiB read of "
+              "another buffer so that no dirty line of the flush remains), flush not timed",
     }
     if scenes is not None:
         out["scenes"] = scenes
@@ -297,8 +303,28 @@ def run_reference(args) -> int:
 
 
 # ------------------------------------------------------------------ GPU side -----
+class L2Flush:
+    """Untimed L2 flush queued before a step: a 512 MiB write; with `clean`, then a
+    512 MiB read of a second buffer, whose clean lines replace the write's dirty ones
+    (else the step pays the write-back of the flush's data)."""
+
+    def __init__(self, clean: bool = True):
+        import torch
+        words = 512 * 1024 * 1024 // 4
+        self.buf = torch.empty(words, dtype=torch.float32, device="cuda")
+        self.clean = clean
+        self.rbuf = torch.zeros(words, dtype=torch.float32, device="cuda") if clean else None
+        self.out = torch.empty((), dtype=torch.float32, device="cuda")
+
+    def __call__(self, k: int) -> None:
+        import torch
+        self.buf.fill_(float(k))
+        if self.clean:
+            torch.sum(self.rbuf, dim=0, out=self.out)
+
+
 def _timed_steps(sim, stream, flush, steps: int) -> float:
-    """Device time (ms) of `steps` steps: each an L2 flush (512 MiB write) queued on the
+    """Device time (ms) of `steps` steps: each an L2 flush (L2Flush) queued on the
     library's stream, then the step bracketed by events on that stream. Nothing syncs
     the host inside the loop, so launches run ahead of the GPU and the events time only
     the steps."""
@@ -308,7 +334,7 @@ def _timed_steps(sim, stream, flush, steps: int) -> float:
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         for k in range(steps):
-            flush.fill_(float(k))
+            flush(k)
             ev[k][0].record(stream)
             sim.take_step()
             ev[k][1].record(stream)
@@ -332,7 +358,7 @@ def _contact_roofline(sim, stream, flush, spec, phase_steps: int, direct: bool) 
     exact0 = sim.list_exact_count()
     with torch.cuda.stream(stream):
         for k in range(phase_steps):
-            flush.fill_(float(k))
+            flush(k)
             sim.take_step()
     sim.synchronize()
     t1 = sim._timings()
@@ -382,6 +408,34 @@ def _contact_roofline(sim, stream, flush, spec, phase_steps: int, direct: bool) 
             "kernel_ms": kernel_ms, "search_ms": search_ms,
             "history_entries_per_grain": entries / n,
             "mean_list_length": mean_list if lists else None}
+
+
+def _fields(sim, stream, flush, reps: int) -> dict:
+    """The CIC deposit into a device grid (wd_compute_density_grid_device) and the total
+    energy (wd_compute_total_energy: a search and gather of the current state, the FP64
+    per-grain terms and their sums) of the current state, each bracketed by events on the
+    library's stream after an L2 flush; medians over `reps`."""
+    import torch
+    from world_b200._lib import check, lib, ptr
+    nodes = sim.density_grid_nodes()
+    grid = torch.empty(4 * nodes, dtype=torch.float32, device="cuda")
+    dep, en = [], []
+    for k in range(reps):
+        for fn, acc in ((lambda: check(lib.wd_compute_density_grid_device(sim.handle, ptr(grid)))
+                         , dep), (sim.compute_total_energy, en)):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush(k)
+                a.record(stream)
+                fn()
+                b.record(stream)
+            b.synchronize()
+            acc.append(a.elapsed_time(b))
+    return {"deposit_ms": statistics.median(dep), "energy_ms": statistics.median(en),
+            "cic_nodes": nodes, "reps": reps,
+            "note": "energy includes the search and gather of the current state and an "
+                    "8-byte copy to the host"}
 
 
 def _settled(sim, scene, stream, flush, args, plain_value: float, done: int,
@@ -511,7 +565,7 @@ def run_ours(args) -> int:
     lists = skin > 0
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush(clean=True)
 
     sim.advance(args.warmup)
     sim.synchronize()
@@ -529,6 +583,10 @@ def run_ours(args) -> int:
     local_ms = _timed_steps(sim, stream, flush, args.steps)
     barrier()
     clocks = sampler.stop() if sampler else None
+    # the same K steps after a write-only flush (dirty L2), for comparison
+    write_flush = L2Flush(clean=False)
+    wf_ms = max_over_ranks(_timed_steps(sim, stream, write_flush, args.steps))
+    del write_flush
     radix_searches = sim.radix_search_count()[0] - radix0
     builds, _, mean_list = sim.list_stats()
     builds -= builds0
@@ -547,6 +605,7 @@ def run_ours(args) -> int:
 
     roof = _contact_roofline(sim, stream, flush, scene.spec, args.phase_steps, args.direct)
     roof["traffic"] = profiled_traffic(args.workload, roof["symbol"])
+    fields = _fields(sim, stream, flush, args.field_reps) if args.field_reps > 0 else None
 
     # e2e through the C ABI with pinned host buffers: every step uploads its state and
     # downloads its positions; the asynchronous calls overlap the upload of one step
@@ -591,9 +650,9 @@ def run_ours(args) -> int:
         and args.grains is None
     settled = batched = adjoint = None
     if extras:
-        # steps from rest so far: warm-up, timed, roofline pass, and the last e2e step
-        # (each e2e step restarts from the same uploaded state)
-        done = args.warmup + args.steps + args.phase_steps + 1
+        # steps from rest so far: warm-up, both timed passes, roofline pass, and the last
+        # e2e step (each e2e step restarts from the same uploaded state)
+        done = args.warmup + 2 * args.steps + args.phase_steps + 1
         settled = _settled(sim, scene, stream, flush, args, value, done, args.settled_steps)
     sim.close()
     if extras:
@@ -628,6 +687,11 @@ def run_ours(args) -> int:
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
                     "d2h_bytes_per_step": 12 * n, "steps": args.e2e_steps},
             "clocks": clocks,
+            "write_flush": {"value": all_grains * args.steps / (wf_ms / 1e3),
+                            "ms_per_step": wf_ms / args.steps,
+                            "l2": "512 MiB write only before every step: the step also writes "
+                                  "back the flush's dirty lines"},
+            "fields": fields,
             "gpu_launches": launches,
             "radix_searches_timed": radix_searches,
             "neighbor_lists": {"skin_m": skin, "builds_timed": builds,

@@ -236,3 +236,18 @@ def test_async_io_loop_matches_the_synchronous_one():
         np.testing.assert_array_equal(x, y)
     np.testing.assert_array_equal(a.get_state(), b.get_state())
     a.close(); b.close()
+
+
+def test_grain_energies_sum_to_the_total_over_any_partition():
+    from test_gpu_parity import packed_poly
+    cfg, st, rad = packed_poly(n=2000, seed=8, mu=0.5)
+    sim = ParticleDynamics(cfg, state=st, radius=rad)
+    sim.advance(30)
+    e = sim.grain_energies()
+    total = sim.compute_total_energy()
+    assert e.shape == (sim.n,)
+    assert float(np.sum(e)) == pytest.approx(total, rel=1e-12)
+    rng = np.random.default_rng(0)
+    part = rng.integers(0, 3, sim.n)
+    assert sum(float(np.sum(e[part == k])) for k in range(3)) == pytest.approx(total, rel=1e-12)
+    sim.close()

@@ -348,17 +348,38 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
             if (cnt > 0) cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
             bool ordered = true;
             if (cnt <= kNbrCap) {
-                // the list, in its build order, while the contacts arrive in canonical order
+                // scan: which entries are contacts, four entries' loads in flight at a
+                // time (index loads, then the partners' positions), one bit each
+                unsigned long long hits = 0ull;
+                for (int e0 = 0; e0 < cnt; e0 += 4) {
+                    int jj[4];
+                    float4 pp[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        jj[u] = e0 + u < cnt ? __ldg(&A.nbr[static_cast<int64_t>(e0 + u) * n + s]) : s;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) pp[u] = __ldg(&A.pos[jj[u]]);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        float3 d;
+                        const float ns = pair_norm_sq(pi, pp[u], d);
+                        const bool hit = e0 + u < cnt && !(ns > cut) &&
+                                         pair_dist(sqrtf(ns), ri, pp[u].w) < 0.f;
+                        hits |= hit ? (1ull << (e0 + u)) : 0ull;
+                    }
+                }
+                // the contacts, in list order, while they arrive in canonical order (the
+                // partner's values are re-read: L1 hits, same arithmetic as the scan)
                 unsigned long long last = 0ull;
-                for (int e = 0; e < cnt; ++e) {
+                while (hits) {
+                    const int e = __ffsll(static_cast<long long>(hits)) - 1;
+                    hits &= hits - 1ull;
                     const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
                     const float4 pj = __ldg(&A.pos[j]);
                     float3 d;
                     const float ns = pair_norm_sq(pi, pj, d);
-                    if (ns > cut) continue;
                     const float norm = sqrtf(ns);
                     const float dist = pair_dist(norm, ri, pj.w);
-                    if (!(dist < 0.f)) continue;
                     const int jd = __ldg(&A.ids[j]);
                     const unsigned long long key = visit_key(P, cx, cy, cz, pj, jd);
                     if (key < last) {
