@@ -10,11 +10,8 @@ dt = 1e-5 s, 453 x 453 x 226 collision grid, 128^3 CIC grid; synthetic seeded in
 (world_b200/scenes.py). A step is one take_step() over all grains.
 
 value  -- device time of K steps (CUDA events on the library's stream around each
-          step; before every step, untimed and on the same stream, a 512 MiB write
-          flushes L2 and a 512 MiB read of another buffer then replaces the flush's
-          dirty lines, so the step starts from a cold and clean L2 and does not pay
-          the flush's own write-backs), max over ranks; grains x ranks x K / time.
-          `write_flush` repeats the measurement with the write alone (dirty L2).
+          step; a 512 MiB write queued on the same stream before every step flushes
+          L2 and is not timed), max over ranks; grains x ranks x K / time.
 e2e    -- the same metric through the C ABI with host buffers: each step
           wd_set_state_async() from pinned host memory, wd_step(1),
           wd_get_positions_async() to pinned host memory, all inside the timed region
@@ -89,6 +86,8 @@ def parse_args():
                     help="steps from rest before the contact-bearing (settled) measurement")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the settled, batched and adjoint sub-measurements")
+    ap.add_argument("--settled-only", action="store_true",
+                    help="of the sub-measurements, run the settled one only")
     ap.add_argument("--field-reps", type=int, default=5,
                     help="timed CIC deposits and energy reductions of the headline state")
     ap.add_argument("--save-after", type=int, default=0, metavar="K",
@@ -132,8 +131,7 @@ def workload_config(spec, workload: str, grains: int, scenes=None) -> dict:
                            spec.collision_grid_size_z],
         "cic_grid": spec.density_grid_size_x,
         "dt": spec.dt,
-        "l2": "flushed before every timed step (512 MiB write, then a 512 MiB read of "
-              "another buffer so that no dirty line of the flush remains), flush not timed",
+        "l2": "flushed (512 MiB write) before every timed step, flush not timed",
     }
     if scenes is not None:
         out["scenes"] = scenes
@@ -304,23 +302,14 @@ def run_reference(args) -> int:
 
 # ------------------------------------------------------------------ GPU side -----
 class L2Flush:
-    """Untimed L2 flush queued before a step: a 512 MiB write; with `clean`, then a
-    512 MiB read of a second buffer, whose clean lines replace the write's dirty ones
-    (else the step pays the write-back of the flush's data)."""
+    """Untimed L2 flush queued before a step: a 512 MiB write (larger than L2)."""
 
-    def __init__(self, clean: bool = True):
+    def __init__(self):
         import torch
-        words = 512 * 1024 * 1024 // 4
-        self.buf = torch.empty(words, dtype=torch.float32, device="cuda")
-        self.clean = clean
-        self.rbuf = torch.zeros(words, dtype=torch.float32, device="cuda") if clean else None
-        self.out = torch.empty((), dtype=torch.float32, device="cuda")
+        self.buf = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def __call__(self, k: int) -> None:
-        import torch
         self.buf.fill_(float(k))
-        if self.clean:
-            torch.sum(self.rbuf, dim=0, out=self.out)
 
 
 def _timed_steps(sim, stream, flush, steps: int) -> float:
@@ -406,6 +395,7 @@ def _contact_roofline(sim, stream, flush, spec, phase_steps: int, direct: bool) 
             "measuring_step_fraction": exact_frac if lists else None,
             "build_step_fraction": build_frac if lists else None,
             "kernel_ms": kernel_ms, "search_ms": search_ms,
+            "build_ms": (search_ms / build_frac) if (lists and build_frac > 0) else None,
             "history_entries_per_grain": entries / n,
             "mean_list_length": mean_list if lists else None}
 
@@ -467,7 +457,7 @@ def _settled(sim, scene, stream, flush, args, plain_value: float, done: int,
             "roofline": {k: roof[k] for k in ("achieved", "peak", "frac", "kernel",
                                                "algorithmic_bytes_per_launch", "kernel_ms",
                                                "measuring_step_fraction",
-                                               "build_step_fraction")},
+                                               "build_step_fraction", "build_ms")},
             "autotuned": tuned}
 
 
@@ -565,7 +555,7 @@ def run_ours(args) -> int:
     lists = skin > 0
     n = sim.n
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
-    flush = L2Flush(clean=True)
+    flush = L2Flush()
 
     sim.advance(args.warmup)
     sim.synchronize()
@@ -583,10 +573,6 @@ def run_ours(args) -> int:
     local_ms = _timed_steps(sim, stream, flush, args.steps)
     barrier()
     clocks = sampler.stop() if sampler else None
-    # the same K steps after a write-only flush (dirty L2), for comparison
-    write_flush = L2Flush(clean=False)
-    wf_ms = max_over_ranks(_timed_steps(sim, stream, write_flush, args.steps))
-    del write_flush
     radix_searches = sim.radix_search_count()[0] - radix0
     builds, _, mean_list = sim.list_stats()
     builds -= builds0
@@ -650,12 +636,12 @@ def run_ours(args) -> int:
         and args.grains is None
     settled = batched = adjoint = None
     if extras:
-        # steps from rest so far: warm-up, both timed passes, roofline pass, and the last
-        # e2e step (each e2e step restarts from the same uploaded state)
-        done = args.warmup + 2 * args.steps + args.phase_steps + 1
+        # steps from rest so far: warm-up, timed, roofline pass, and the last e2e step
+        # (each e2e step restarts from the same uploaded state)
+        done = args.warmup + args.steps + args.phase_steps + 1
         settled = _settled(sim, scene, stream, flush, args, value, done, args.settled_steps)
     sim.close()
-    if extras:
+    if extras and not args.settled_only:
         batched = {w: _batched(w, args, flush, value) for w in BATCHED_WORKLOADS}
         adjoint = adjoint_measure(args, plain_value=value)
 
@@ -673,7 +659,7 @@ def run_ours(args) -> int:
         roofline = {k: roof[k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic",
                                          "kernel", "peak_source", "algorithmic_bytes_per_launch",
                                          "measuring_step_fraction", "build_step_fraction",
-                                         "kernel_ms", "search_ms")}
+                                         "kernel_ms", "search_ms", "build_ms")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -687,10 +673,6 @@ def run_ours(args) -> int:
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
                     "d2h_bytes_per_step": 12 * n, "steps": args.e2e_steps},
             "clocks": clocks,
-            "write_flush": {"value": all_grains * args.steps / (wf_ms / 1e3),
-                            "ms_per_step": wf_ms / args.steps,
-                            "l2": "512 MiB write only before every step: the step also writes "
-                                  "back the flush's dirty lines"},
             "fields": fields,
             "gpu_launches": launches,
             "radix_searches_timed": radix_searches,

@@ -238,3 +238,53 @@ def cic(x, v, mass, lo, hi, size):
                 contrib = torch.where(live[:, None], chan * ww[:, None], torch.zeros_like(chan))
                 out = out.index_add(1, node, contrib.T)
     return out.reshape(4, *size)
+
+
+def adjoint_along(model: TorchModel, traj, springs, theta, loss_of_end):
+    """The FP64 adjoint of a window along a given trajectory: traj[t] (n, 6) is the state
+    entering step t (t = 0 .. T, traj[T] the end), springs[t] the (sorted keys, springs)
+    entering step t. Each step's vector-Jacobian product is evaluated at those states,
+    with the step's own contact decisions there, and chained back from
+    loss_of_end(x_T, v_T). Returns (dL/dv0, dL/dx0, dL/dtheta)."""
+    steps = len(traj) - 1
+    xT = traj[-1][:, :3].clone().requires_grad_(True)
+    vT = traj[-1][:, 3:].clone().requires_grad_(True)
+    loss_of_end(xT, vT).backward()
+    gx = xT.grad if xT.grad is not None else torch.zeros_like(xT)
+    gv = vT.grad if vT.grad is not None else torch.zeros_like(vT)
+    g_keys, g_xi = None, None
+    g_th = torch.zeros(3, dtype=torch.float64, device=theta.device)
+    for t in reversed(range(steps)):
+        x = traj[t][:, :3].clone().requires_grad_(True)
+        v = traj[t][:, 3:].clone().requires_grad_(True)
+        keys_t, xi_t = springs[t]
+        xi_t = xi_t.clone().requires_grad_(True)
+        th = theta.clone().requires_grad_(True)
+        x1, v1, keys1, xi1, _ = step(model, x, v, keys_t, xi_t, th[0], th[1], th[2])
+        outs, grads = [x1, v1], [gx, gv]
+        if g_xi is not None and xi1.numel() and g_keys.numel():
+            at = torch.searchsorted(g_keys, keys1).clamp(max=g_keys.numel() - 1)
+            hit = (g_keys[at] == keys1)[:, None]
+            outs.append(xi1)
+            grads.append(torch.where(hit, g_xi[at], torch.zeros_like(xi1)))
+        torch.autograd.backward(outs, grads)
+        gx = x.grad if x.grad is not None else torch.zeros_like(x)
+        gv = v.grad if v.grad is not None else torch.zeros_like(v)
+        g_keys = keys_t
+        g_xi = xi_t.grad if xi_t.grad is not None else torch.zeros_like(xi_t)
+        if th.grad is not None:
+            g_th = g_th + th.grad
+    return gv, gx, g_th
+
+
+def record_trajectory(model: TorchModel, x0, v0, springs0, theta, steps: int):
+    """The FP64 run's own states and springs entering each step (for adjoint_along)."""
+    x, v = x0, v0
+    keys, xi = springs0
+    traj, sprs = [torch.cat([x, v], 1)], []
+    with torch.no_grad():
+        for _ in range(steps):
+            sprs.append((keys, xi))
+            x, v, keys, xi, _ = step(model, x, v, keys, xi, theta[0], theta[1], theta[2])
+            traj.append(torch.cat([x, v], 1))
+    return traj, sprs

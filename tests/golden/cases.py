@@ -82,6 +82,11 @@ CASES = {
     # packing pressed into a corner: floor and two walls in contact, with friction
     "packed_walls": dict(kind="packed", n=1331, spacing_r=1.95, seed=5, vel_sigma=0.2,
                          solver="semi_implicit_euler", picard=3, steps=1, near_walls=True),
+    # restitution 0.6 (the differentiable window's target run): the damping coefficient
+    # the library derives from ln e on the host must match the reference's per-contact
+    # device logf to the bit
+    "packed_e06": dict(kind="packed", n=2197, spacing_r=1.9, seed=17, vel_sigma=0.1,
+                       solver="semi_implicit_euler", picard=3, steps=1, restitution=0.6),
 }
 
 PACKED_PARAMS = dict(dt=1e-4, gx=50, gy=50, gz=50, ppc=16, dg=16, lo=-0.5, hi=0.5,
@@ -94,6 +99,7 @@ def case_inputs(name: str, state_path: str) -> tuple[str | None, np.ndarray | No
     if c["kind"] == "cube":
         return None, None
     p = dict(PACKED_PARAMS)
+    p.update({k: c[k] for k in ("restitution", "friction") if k in c})
     state = packed_state(c["n"], p["radius"], p["lo"], p["hi"], c["spacing_r"], c["seed"],
                          c["vel_sigma"], c.get("near_walls", False))
     text = BASE_YAML.format(state_path=state_path, solver=c["solver"], picard=c["picard"], **p)

@@ -3,8 +3,8 @@
 Runs the reference's ParticleDynamics, compiled from its unmodified sources for
 sm_100a by oracle/build.py into oracle/_ref/libref_world.so, on a B200:
 
-    python tests/golden/make_golden.py [OUT_DIR]  # writes OUT_DIR/<case>.npz
-                                                  # (default: tests/golden)
+    python tests/golden/make_golden.py [OUT_DIR [CASE ...]]  # writes OUT_DIR/<case>.npz
+                                              # (default: tests/golden, every case)
 
 Per case it stores the initial state, the state and rhs after the case's steps, the
 candidate set of every grain (the reference's device_neighbors rows, sorted: the
@@ -74,8 +74,9 @@ def main() -> int:
         print("oracle/_ref/libref_world.so missing: run python oracle/build.py where the "
               "reference tree is present", file=sys.stderr)
         return 1
+    names = sys.argv[2:] or list(CASES)
     with tempfile.TemporaryDirectory() as tmp:
-        for name in CASES:
+        for name in names:
             rec = run_case(name, tmp)
             path = os.path.join(out_dir, f"{name}.npz")
             np.savez_compressed(path, **rec)

@@ -79,3 +79,28 @@ def test_torch_cic_matches_numpy_cic():
     want = adjoint_ref.cic(x, v, m, lo, hi, size)
     got = AT.cic(torch.tensor(x), torch.tensor(v), torch.tensor(m), lo, hi, size)
     np.testing.assert_allclose(got.numpy(), want, rtol=1e-12, atol=1e-12)
+
+
+def test_adjoint_along_a_trajectory_equals_autograd_through_the_window():
+    """Chaining per-step vector-Jacobian products at the recorded states (what the C4 test
+    does along the library's trajectory) equals autograd through the frozen window when
+    the states are the window's own."""
+    cfg, st, rad, mass, model, (mu, e, k), empty = _setup(n=300, seed=13)
+    steps = 15
+    x0 = torch.tensor(st[:, :3], dtype=torch.float64)
+    v0 = torch.tensor(st[:, 3:], dtype=torch.float64)
+    th = torch.tensor([mu, e, k], dtype=torch.float64)
+    rng = np.random.default_rng(2)
+    wx = torch.tensor(rng.normal(size=(model.n, 3)))
+    wv = torch.tensor(rng.normal(size=(model.n, 3)) * 1e-3)
+    _, _, pat = AT.run(model, x0, v0, empty, th[0], th[1], th[2], steps)
+    tv = v0.clone().requires_grad_(True)
+    tth = th.clone().requires_grad_(True)
+    xT, vT, _ = AT.run(model, x0, tv, empty, tth[0], tth[1], tth[2], steps, pattern=pat)
+    ((wx * xT).sum() + (wv * vT).sum()).backward()
+    traj, sprs = AT.record_trajectory(model, x0, v0, empty, th, steps)
+    gv, _, gth = AT.adjoint_along(model, traj, sprs, th,
+                                  lambda x, v: (wx * x).sum() + (wv * v).sum())
+    assert sum(int(s[0].numel()) for s in sprs) > 500        # springs carried through
+    np.testing.assert_allclose(gv.numpy(), tv.grad.numpy(), rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(gth.numpy(), tth.grad.numpy(), rtol=1e-9, atol=0)

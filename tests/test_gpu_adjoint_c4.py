@@ -7,12 +7,18 @@ falling without a single contact, so a window there would test free flight only)
 200-step window with checkpoints every 20 steps; loss = mean((rho_T - rho_target)^2) over
 the 64^3 CIC mass field, the target from the same window with mu = 0.4, e = 0.6.
 
-The library's FP32 gradients in (mu, e, k_n) and in v0 (every grain) are checked against
-  * central finite differences (h = 1e-4, relative for k_n) of the FP64 restatement
-    (tests/adjoint_torch.py) with its contact set and branches frozen, and
-  * the FP64 adjoint: torch.autograd through that same frozen FP64 window,
-within 1e-3 relative: the parameters each, v0 in three random directions and as a whole
-vector (relative L2 norm).
+Two FP64 checks (tests/adjoint_torch.py, a torch float64 restatement of the step):
+  * along the library's own FP32 trajectory: every step's vector-Jacobian product
+    evaluated in FP64 at the library's recorded state and springs of that step, chained
+    back from the loss. The library's FP32 gradients in (mu, e, k_n) and in v0 (every
+    grain) must agree within 1e-3 relative: the parameters each, v0 in three random
+    directions and as a whole vector (relative L2 norm);
+  * along the FP64 trajectory of the same window: torch.autograd through the frozen
+    FP64 window against its central finite differences (h = 1e-4, relative for k_n),
+    within 1e-3. This pins the restatement itself.
+The library's gradients are also printed against the FP64 trajectory's: 200 steps of a
+collapsing column amplify the rounding difference of the two trajectories (a few percent
+in dL/dmu on a B200), which is why the 1e-3 bar is taken along the library's own states.
 """
 from __future__ import annotations
 
@@ -62,7 +68,20 @@ def test_c4_window_gradients_match_fp64_adjoint_and_finite_differences():
                           device="cuda").reshape(size)
     sim.set_contact_params(mu, e, k)
 
+    # the library's own trajectory, step by step (the window below repeats it exactly)
+    model = AT.model_from_config(cfg, sc.radius, sim.grain_mass.copy())
+    sim.set_state(start)
+    sim.set_history(*springs)
+    traj, sprs = [], []
+    for t in range(steps + 1):
+        traj.append(torch.tensor(sim.get_state().reshape(-1, 6), dtype=torch.float64,
+                                 device="cuda"))
+        if t < steps:
+            sprs.append(AT.springs_from_rows(n, *sim.get_history()))
+            sim.take_step()
+
     # the library: FP32 forward window with checkpoints, hand-written reverse pass
+    sim.set_state(start)
     sim.set_history(*springs)
     xs = torch.tensor(start[:, :3], device="cuda")
     tv0 = torch.tensor(start[:, 3:], device="cuda", requires_grad=True)
@@ -73,16 +92,31 @@ def test_c4_window_gradients_match_fp64_adjoint_and_finite_differences():
     loss32.backward()
     g32_v0 = tv0.grad.double()
     g32_th = theta.grad.numpy().copy()
-    mass = sim.grain_mass.copy()
     sim.close()
 
-    # FP64: the same window recorded, then frozen
-    model = AT.model_from_config(cfg, sc.radius, mass)
+    # FP64 adjoint along the library's trajectory
+    m64 = model.mass
+    th0 = torch.tensor([mu, e, k], dtype=torch.float64, device="cuda")
+    ga_v0, _, ga_th = AT.adjoint_along(
+        model, traj, sprs, th0,
+        lambda x, v: ((AT.cic(x, v, m64, lo, hi, size)[0] - target) ** 2).mean())
+    ga_th = ga_th.cpu().numpy()
+    for a in range(3):
+        print(f"theta[{a}] along the library's states: library {g32_th[a]:.6e}  "
+              f"fp64 {ga_th[a]:.6e}")
+        assert _rel(g32_th[a], ga_th[a]) < RTOL
+    whole_along = float((g32_v0 - ga_v0).norm() / ga_v0.norm())
+    print(f"v0 gradient along the library's states, relative L2 difference: {whole_along:.3e}")
+    assert whole_along < RTOL
+    rng_a = np.random.default_rng(9)
+    for _ in range(3):
+        dv = torch.tensor(rng_a.normal(size=(n, 3)), device="cuda")
+        assert _rel(float((g32_v0 * dv).sum()), float((ga_v0 * dv).sum())) < RTOL
+
+    # FP64: the same window on its own trajectory, recorded, then frozen
     x0 = torch.tensor(start[:, :3], dtype=torch.float64, device="cuda")
     v0 = torch.tensor(start[:, 3:], dtype=torch.float64, device="cuda")
     sp0 = AT.springs_from_rows(n, *springs)
-    th0 = torch.tensor([mu, e, k], dtype=torch.float64, device="cuda")
-    m64 = model.mass
 
     with torch.no_grad():
         _, _, pat = AT.run(model, x0, v0, sp0, th0[0], th0[1], th0[2], steps)
@@ -108,19 +142,17 @@ def test_c4_window_gradients_match_fp64_adjoint_and_finite_differences():
             d = torch.zeros(3, dtype=torch.float64, device="cuda")
             d[a] = step
             fd = float((loss64(v0, th0 + d) - loss64(v0, th0 - d)) / (2 * step))
-            print(f"theta[{a}]: library {g32_th[a]:.6e}  fp64 adjoint {g64_th[a]:.6e}  fd {fd:.6e}")
+            print(f"theta[{a}] on the FP64 trajectory: library {g32_th[a]:.6e}  "
+                  f"fp64 adjoint {g64_th[a]:.6e}  fd {fd:.6e}")
             assert _rel(g64_th[a], fd) < RTOL
-            assert _rel(g32_th[a], fd) < RTOL
-            assert _rel(g32_th[a], g64_th[a]) < RTOL
         # v0 in random directions
         for _ in range(3):
             dv = torch.tensor(rng.normal(size=(n, 3)), device="cuda")
             fd = float((loss64(v0 + h * dv, th0) - loss64(v0 - h * dv, th0)) / (2 * h))
             a32 = float((g32_v0 * dv).sum())
             a64 = float((g64_v0 * dv).sum())
-            print(f"v0 direction: library {a32:.6e}  fp64 adjoint {a64:.6e}  fd {fd:.6e}")
+            print(f"v0 direction on the FP64 trajectory: library {a32:.6e}  "
+                  f"fp64 adjoint {a64:.6e}  fd {fd:.6e}")
             assert _rel(a64, fd) < RTOL
-            assert _rel(a32, fd) < RTOL
     whole = float((g32_v0 - g64_v0).norm() / g64_v0.norm())
-    print(f"v0 gradient, relative L2 difference library vs fp64 adjoint: {whole:.3e}")
-    assert whole < RTOL
+    print(f"v0 gradient, relative L2 difference library vs the FP64 trajectory: {whole:.3e}")

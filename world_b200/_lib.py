@@ -114,7 +114,7 @@ SIGNATURES = {
     "wd_compute_density_grid": ([_p, _p], c_int),
     "wd_compute_density_grid_device": ([_p, _p], c_int),
     "wd_compute_total_energy": ([_p, _d], c_int),
-    "wd_grain_energies": ([_p, _d], c_int),
+    "wd_grain_energies": ([_p, _p], c_int),
     "wd_compute_momentum": ([_p, _d], c_int),
     "wd_is_stable": ([_p, _i32], c_int),
     "wd_compute_max_acceleration": ([_p, _f], c_int),

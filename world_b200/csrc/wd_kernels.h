@@ -181,9 +181,12 @@ struct ListCopy {
     const float4* vel; const int* ids; const int* hcnt; const int* scene;
     float4* pos_out; float4* vel_out; int* ids_out; int* hcnt_out; int* scene_out;
 };
+// tiled: a single scene's build with each block's neighbour window staged in shared
+// memory (k_list_build_tiled); otherwise one thread per slot reading global memory.
 void launch_list_build(const DevParams& P, SceneTab T, const float4* pos, const int2* table,
                        int* nbr, int* nbr_cnt, float4* xbuild, uint32_t* list_ctrl,
-                       const ListCopy& cp, Skip skip, cudaStream_t st);
+                       const ListCopy& cp, Skip skip, unsigned long long* counters, bool tiled,
+                       cudaStream_t st);
 void launch_list_copy(int n, const float4* pos, const float4* vel, const int* ids,
                       const int* hcnt, const int* scene, float4* pos_out, float4* vel_out,
                       int* ids_out, int* hcnt_out, int* scene_out, Skip skip, cudaStream_t st);

@@ -676,6 +676,162 @@ k_force_list_staged(DevParams P0, ListArgs A) {
     list_tail_decide(A);
 }
 
+// ---- list build with the tile's neighbour window staged in shared memory ----------
+// One block per 256 consecutive sorted slots (single scene). Every grain's candidates
+// lie in its nine stencil rows (three z-consecutive cells of one column each, one slot
+// range per row); over the tile, row r's ranges lie inside [min lo_r, max hi_r). Those
+// nine hulls, merged where they overlap (consecutive columns of one x-plane are
+// consecutive in slot order), are copied into shared memory once by bulk copies
+// (cp.async.bulk, this GPU's memory into this CTA, completing on an mbarrier), and the
+// threads read their candidates there: 27 position loads per grain from L2 become a
+// few per grain. A window above kWinCap positions, or a copy that does not complete
+// within the bounded wait, falls back to global loads. Same lists, same order.
+constexpr int kWinCap = 2560;   // positions (40 KB): five blocks per SM
+
+__global__ void __launch_bounds__(kBlock)
+k_list_build_tiled(DevParams P, const float4* __restrict__ pos, const int2* __restrict__ table,
+                   int* __restrict__ nbr, int* __restrict__ nbr_cnt, float4* __restrict__ xbuild,
+                   uint32_t* __restrict__ ctrl, ListCopy cp, Skip skip,
+                   unsigned long long* __restrict__ counters) {
+    if (skipped(skip)) return;
+    __shared__ float4 win[kWinCap];
+    __shared__ int hull_lo[9], hull_hi[9], row_off[9];
+    __shared__ int staged;
+    __shared__ __align__(8) uint64_t bar;
+    const int n = P.n;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = s < n;
+    if (threadIdx.x < 9) {
+        hull_lo[threadIdx.x] = 0x7fffffff;
+        hull_hi[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int lo[9], hi[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        lo[r] = 0x7fffffff;
+        hi[r] = 0;
+    }
+    if (live) {
+        pi = pos[s];
+        cp.pos_out[s] = pi;
+        cp.vel_out[s] = cp.vel[s];
+        cp.ids_out[s] = cp.ids[s];
+        if (cp.hcnt) cp.hcnt_out[s] = cp.hcnt[s];
+        int cx, cy, cz;
+        cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const int nx = cx + r - 1;
+            if (nx >= 0 && nx < P.grid[0]) row_ranges(P, table, nx, cy, cz, lo + 3 * r, hi + 3 * r);
+        }
+    }
+    __syncthreads();   // hull initialisation and the barrier's init visible
+    if (live) {
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+            if (lo[r] < hi[r]) {
+                atomicMin(&hull_lo[r], lo[r]);
+                atomicMax(&hull_hi[r], hi[r]);
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // merge the nine hulls into disjoint ranges (ascending), stage them if they fit
+        int idx[9], m = 0;
+        for (int r = 0; r < 9; ++r)
+            if (hull_lo[r] < hull_hi[r]) idx[m++] = r;
+        for (int a = 1; a < m; ++a) {          // insertion sort by hull start
+            const int v = idx[a];
+            int b = a - 1;
+            while (b >= 0 && hull_lo[idx[b]] > hull_lo[v]) {
+                idx[b + 1] = idx[b];
+                --b;
+            }
+            idx[b + 1] = v;
+        }
+        int mlo[9], mhi[9], nm = 0, total = 0;
+        for (int a = 0; a < m; ++a) {
+            const int r = idx[a];
+            if (nm > 0 && hull_lo[r] <= mhi[nm - 1]) {
+                mhi[nm - 1] = max(mhi[nm - 1], hull_hi[r]);
+            } else {
+                mlo[nm] = hull_lo[r];
+                mhi[nm] = hull_hi[r];
+                ++nm;
+            }
+        }
+        for (int k = 0; k < nm; ++k) total += mhi[k] - mlo[k];
+        const bool fits = nm > 0 && total <= kWinCap;
+        staged = fits ? 1 : 0;
+        if (fits) {
+            int base[9];
+            int acc = 0;
+            for (int k = 0; k < nm; ++k) {
+                base[k] = acc;
+                acc += mhi[k] - mlo[k];
+            }
+            for (int a = 0; a < m; ++a) {
+                const int r = idx[a];
+                int k = 0;
+                while (!(hull_lo[r] >= mlo[k] && hull_hi[r] <= mhi[k])) ++k;
+                row_off[r] = base[k] - mlo[k];
+            }
+            mbar_expect_tx(&bar, static_cast<uint32_t>(total) * 16u);
+            for (int k = 0; k < nm; ++k)
+                bulk_g2s(&win[base[k]], pos + mlo[k], static_cast<uint32_t>(mhi[k] - mlo[k]) * 16u, &bar);
+        }
+    }
+    __syncthreads();
+    bool use_win = staged != 0;
+    if (use_win) {
+        const bool ok = mbar_wait(&bar, 0u, 1000000000ull);
+        if (!__syncthreads_and(ok)) {
+            if (threadIdx.x == 0) atomicAdd(&counters[kCntStageTimeout], 1ull);
+            use_win = false;
+        }
+    }
+    if (!live) return;
+    int cnt = 0;
+    auto visit = [&](int j, float4 pj) {
+        if (j == s) return;
+        float3 d;
+        const float ns = pair_norm_sq(pi, pj, d);
+        const float reach = (pi.w + pj.w) + P.skin;
+        if (ns < reach * reach) {
+            if (cnt < kNbrCap) nbr[static_cast<int64_t>(cnt) * n + s] = j;
+            ++cnt;
+        }
+    };
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        int j = lo[r];
+        const int e = hi[r];
+        if (use_win) {
+            if (j < e) {
+                const float4* w = win + row_off[r];
+                for (; j < e; ++j) visit(j, w[j]);
+            }
+        } else {
+            for (; e - j > 1; j += 2) {
+                const float4 a = __ldg(&pos[j]);
+                const float4 b = __ldg(&pos[j + 1]);
+                visit(j, a);
+                visit(j + 1, b);
+            }
+            if (j < e) visit(j, __ldg(&pos[j]));
+        }
+    }
+    nbr_cnt[s] = cnt;
+    xbuild[s] = pi;
+    if (cnt > kNbrCap) atomicOr(&ctrl[kLcOverflow], 1u);
+}
+
 // The last executed Picard iteration k wrote the B buffers when k is even and the
 // scratch buffers when k is odd (iterations alternate, starting in B).
 __global__ void __launch_bounds__(kBlock)
@@ -934,7 +1090,13 @@ void launch_list_decide(uint32_t* list_ctrl, float thr, bool always_exact,
 
 void launch_list_build(const DevParams& P, SceneTab T, const float4* pos, const int2* table,
                        int* nbr, int* nbr_cnt, float4* xbuild, uint32_t* list_ctrl,
-                       const ListCopy& cp, Skip skip, cudaStream_t st) {
+                       const ListCopy& cp, Skip skip, unsigned long long* counters, bool tiled,
+                       cudaStream_t st) {
+    if (tiled && !T.params) {
+        k_list_build_tiled<<<blocks_for(P.n), kBlock, 0, st>>>(P, pos, table, nbr, nbr_cnt, xbuild,
+                                                               list_ctrl, cp, skip, counters);
+        return;
+    }
     if (T.params)
         k_list_build<true><<<blocks_for(P.n), kBlock, 0, st>>>(P, T, pos, table, nbr, nbr_cnt,
                                                                 xbuild, list_ctrl, cp, skip);

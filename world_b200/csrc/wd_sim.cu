@@ -151,6 +151,7 @@ struct wd_sim {
     int* nbr_cnt = nullptr;
     float4* xbuild = nullptr;
     uint32_t* list_ctrl = nullptr;
+    bool build_tiled = true;    // list builds stage each block's neighbour window
     unsigned long long* list_len = nullptr;
     unsigned* tail_count = nullptr;  // block ticket of the contact kernel's fused decision
     bool need_build = false;         // host-side change: rebuild before the next step
@@ -552,7 +553,7 @@ void enqueue_list_build(wd_sim* s, wd::Skip gate, cudaStream_t st) {
                     s->posA, s->velA, s->idsA, hist ? s->hcnt_slot : nullptr,
                     batch ? s->sceneA : nullptr};
     wd::launch_list_build(P, tab(s, s->sceneB), s->posB, s->sb.table, s->nbr, s->nbr_cnt,
-                          s->xbuild, s->list_ctrl, cp, gate, st);
+                          s->xbuild, s->list_ctrl, cp, gate, s->counters, s->build_tiled, st);
 }
 
 // Inside a capture on st: an IF node on `cond` after everything captured so far, its
