@@ -345,6 +345,7 @@ def _contact_roofline(sim, stream, flush, spec, phase_steps: int, direct: bool) 
     t0 = sim._timings()
     builds0 = sim.list_stats()[0]
     exact0 = sim.list_exact_count()
+    resort0 = sim.list_resort_count()
     with torch.cuda.stream(stream):
         for k in range(phase_steps):
             flush(k)
@@ -353,6 +354,7 @@ def _contact_roofline(sim, stream, flush, spec, phase_steps: int, direct: bool) 
     t1 = sim._timings()
     sim.set_kernel_timing(direct)
     build_frac = (sim.list_stats()[0] - builds0) / phase_steps
+    resort_frac = (sim.list_resort_count() - resort0) / (phase_steps * sim.n)
     exact_frac = (sim.list_exact_count() - exact0) / phase_steps
     search_ms = float(t1[0] - t0[0]) / phase_steps
     contact_ms = float(t1[1] - t0[1]) / phase_steps
@@ -397,7 +399,8 @@ def _contact_roofline(sim, stream, flush, spec, phase_steps: int, direct: bool) 
             "kernel_ms": kernel_ms, "search_ms": search_ms,
             "build_ms": (search_ms / build_frac) if (lists and build_frac > 0) else None,
             "history_entries_per_grain": entries / n,
-            "mean_list_length": mean_list if lists else None}
+            "mean_list_length": mean_list if lists else None,
+            "resorted_grain_fraction": resort_frac if lists else None}
 
 
 def _fields(sim, stream, flush, reps: int) -> dict:
@@ -457,7 +460,8 @@ def _settled(sim, scene, stream, flush, args, plain_value: float, done: int,
             "roofline": {k: roof[k] for k in ("achieved", "peak", "frac", "kernel",
                                                "algorithmic_bytes_per_launch", "kernel_ms",
                                                "measuring_step_fraction",
-                                               "build_step_fraction", "build_ms")},
+                                               "build_step_fraction", "build_ms",
+                                               "resorted_grain_fraction")},
             "autotuned": tuned}
 
 
@@ -659,7 +663,8 @@ def run_ours(args) -> int:
         roofline = {k: roof[k] for k in ("bound", "achieved", "peak", "unit", "frac", "traffic",
                                          "kernel", "peak_source", "algorithmic_bytes_per_launch",
                                          "measuring_step_fraction", "build_step_fraction",
-                                         "kernel_ms", "search_ms", "build_ms")}
+                                         "kernel_ms", "search_ms", "build_ms",
+                                         "resorted_grain_fraction")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,

@@ -303,6 +303,10 @@ int wd_debug_stage_wait(wd_sim* sim, int32_t stall, int32_t wait_us);
  * since the build (reading the build positions). The other steps decide on a bound:
  * the last exact value plus the largest per-step displacement of each step since. */
 int wd_list_exact_count(wd_sim* sim, int64_t* steps);
+/* Lifetime count of (grain, step) pairs in which the list contact kernels found a
+ * grain's contacts out of the canonical visiting order (a cell crossing since the last
+ * build) and evaluated them in sorted order instead (no counterpart in the reference). */
+int wd_list_resort_count(wd_sim* sim, int64_t* grains);
 /* Backward Euler / Picard: iterations executed so far (iterations that a converged
  * step skipped are not counted), and, on Verlet lists, the steps whose iterate went
  * beyond the lists' validity bound and that were redone with the per-iteration search

@@ -78,6 +78,7 @@ SIGNATURES = {
     "wd_set_neighbor_skin": ([_p, c_float], c_int),
     "wd_picard_counts": ([_p, _i64, _i64], c_int),
     "wd_list_exact_count": ([_p, _i64], c_int),
+    "wd_list_resort_count": ([_p, _i64], c_int),
     "wd_get_tuning": ([_p, POINTER(c_float), POINTER(c_int32), POINTER(c_int32)], c_int),
     "wd_set_contact_kernel": ([_p, c_int32, c_int32], c_int),
     "wd_debug_stage_wait": ([_p, c_int32, c_int32], c_int),

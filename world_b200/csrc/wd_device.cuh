@@ -28,6 +28,7 @@ enum Counter : int {
     kCntPicardIters = 7,    // Picard iterations executed (contact-kernel launches that ran)
     kCntListExact = 8,      // list steps whose contact kernel read the build positions
     kCntStageTimeout = 9,   // bulk-staged contact kernel: stages that never completed
+    kCntListResort = 10,    // list contact kernels: grains whose contacts were re-ordered
     kNumCounters = 12,
 };
 

@@ -263,6 +263,42 @@ __device__ __forceinline__ void list_contacts_sorted(const DevParams& P, const L
     }
 }
 
+// The same for a grain whose contacts the scan found (bitmask over list entries): each
+// pass visits the contacts only, and takes the smallest visiting key above the last.
+template <bool HIST>
+__device__ __forceinline__ void list_contacts_sorted_mask(const DevParams& P, const ListArgs& A,
+                                                       int s, int n, unsigned long long hits,
+                                                       float4 pi, float3 vel, float mi, int cx,
+                                                       int cy, int cz, float3& f, HistRow& h) {
+    const float ri = pi.w;
+    long long done = -1;
+    for (;;) {
+        long long best = 0x7fffffffffffffffll;
+        int be = -1;
+        for (unsigned long long m = hits; m; m &= m - 1ull) {
+            const int e = __ffsll(static_cast<long long>(m)) - 1;
+            const int j = __ldg(&A.nbr[static_cast<int64_t>(e) * n + s]);
+            const long long key = static_cast<long long>(
+                visit_key(P, cx, cy, cz, __ldg(&A.pos[j]), __ldg(&A.ids[j])));
+            if (key > done && key < best) {
+                best = key;
+                be = e;
+            }
+        }
+        if (be < 0) break;
+        done = best;
+        const int j = __ldg(&A.nbr[static_cast<int64_t>(be) * n + s]);
+        const float4 pj = __ldg(&A.pos[j]);
+        float3 d;
+        const float ns = pair_norm_sq(pi, pj, d);
+        const float norm = sqrtf(ns);
+        const float dist = pair_dist(norm, ri, pj.w);
+        const float4 vj = __ldg(&A.vel[j]);
+        pair_force<HIST>(P, d, norm, dist, vel, mi, vj, static_cast<int>(best & 0xffffffffll),
+                         f, h, A.counters);
+    }
+}
+
 // The contacts of a grain whose list overflowed, from the run table of the build that
 // ran this step (the stencil walk of the searched kernel).
 template <bool HIST>
@@ -370,6 +406,7 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
                 }
                 // the contacts, in list order, while they arrive in canonical order (the
                 // partner's values are re-read: L1 hits, same arithmetic as the scan)
+                const unsigned long long all_hits = hits;
                 unsigned long long last = 0ull;
                 while (hits) {
                     const int e = __ffsll(static_cast<long long>(hits)) - 1;
@@ -395,7 +432,9 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
                     // canonical order
                     f = f_walls;
                     if (HIST) h.out_count = out_walls;
-                    list_contacts_sorted<HIST>(P, A, s, n, cnt, pi, vel, mi, cut, cx, cy, cz, f, h);
+                    atomicAdd(&A.counters[kCntListResort], 1ull);
+                    list_contacts_sorted_mask<HIST>(P, A, s, n, all_hits, pi, vel, mi, cx, cy, cz,
+                                                    f, h);
                 }
             } else {
                 // list overflow: this step built the lists, so the run table is fresh

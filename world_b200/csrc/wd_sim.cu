@@ -1963,6 +1963,11 @@ int wd_picard_counts(wd_sim* sim, int64_t* iterations, int64_t* redos) {
     return rc ? rc : read_counter(sim, wd::kCntPicardRedos, redos);
 }
 
+int wd_list_resort_count(wd_sim* sim, int64_t* grains) {
+    if (!sim || !grains) return fail(WD_ERR_INVALID, "wd_list_resort_count: NULL argument");
+    return read_counter(sim, wd::kCntListResort, grains);
+}
+
 int wd_list_exact_count(wd_sim* sim, int64_t* steps) {
     if (!sim || !steps) return fail(WD_ERR_INVALID, "wd_list_exact_count: NULL argument");
     return read_counter(sim, wd::kCntListExact, steps);

@@ -383,6 +383,13 @@ class ParticleDynamics:
         check(lib.wd_list_exact_count(self._h, ctypes.byref(v)))
         return int(v.value)
 
+    def list_resort_count(self) -> int:
+        """(grain, step) pairs so far whose contacts a cell crossing had re-ordered, so
+        that the list kernel evaluated them in sorted order."""
+        v = ctypes.c_int64()
+        check(lib.wd_list_resort_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
     def list_stats(self) -> tuple[int, int, float]:
         """(Verlet-list builds so far, kernels each build launches, mean list length)."""
         b = ctypes.c_int64()
