@@ -296,8 +296,10 @@ int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant);
  * second). stall != 0: each warp's first stage is made to expect 16 bytes that no copy
  * delivers, so its wait runs out; the kernel then returns without finishing that warp's
  * tiles, and the next synchronizing call returns WD_ERR_CUDA once with "did not
- * complete within its wait limit" (the state of that step is invalid: restore one with
- * wd_set_state). No copy is ever left in flight. Handles with Verlet lists only. */
+ * complete within its wait limit". The state of that step is invalid, slot order
+ * included: restore one with wd_set_state (which then starts from the grain-id order
+ * and no stored springs; wd_set_history restores those). No copy is ever left in
+ * flight. Handles with Verlet lists only. */
 int wd_debug_stage_wait(wd_sim* sim, int32_t stall, int32_t wait_us);
 /* Verlet lists: steps so far whose contact kernel measured the exact displacement
  * since the build (reading the build positions). The other steps decide on a bound:

@@ -38,6 +38,7 @@ def test_library_exports_every_declared_symbol():
     assert not missing, f"declared but not exported: {missing}"
     for s in declared_symbols():
         assert hasattr(lib, s)
+    assert not _lib.MISSING
 
 
 def test_python_binding_covers_the_header():

@@ -131,8 +131,16 @@ SIGNATURES = {
     "wd_debug_candidates": ([_p, _p, _p, _p, c_int64, _i64], c_int),
 }
 
+# A library built before an entry point existed loads too; calling that entry point
+# then raises AttributeError (tests/test_abi.py checks that the built library exports
+# every declared symbol).
+MISSING = []
 for _name, (_args, _res) in SIGNATURES.items():
-    _fn = getattr(lib, _name)
+    try:
+        _fn = getattr(lib, _name)
+    except AttributeError:
+        MISSING.append(_name)
+        continue
     _fn.argtypes = _args
     _fn.restype = _res
 

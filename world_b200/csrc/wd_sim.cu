@@ -152,6 +152,7 @@ struct wd_sim {
     float4* xbuild = nullptr;
     uint32_t* list_ctrl = nullptr;
     bool build_tiled = true;    // list builds stage each block's neighbour window
+    bool slots_invalid = false; // a contact step stopped part-way: slot order to reset
     unsigned long long* list_len = nullptr;
     unsigned* tail_count = nullptr;  // block ticket of the contact kernel's fused decision
     bool need_build = false;         // host-side change: rebuild before the next step
@@ -894,8 +895,11 @@ int sync_stream(wd_sim* s) {
         WD_CUDA(cudaMemcpy(&stalls, s->counters + wd::kCntStageTimeout, sizeof(stalls),
                            cudaMemcpyDeviceToHost));
         if (stalls) {
-            // reported once: the handle stays usable (the caller restores a state)
+            // reported once: the handle stays usable. The step stopped part-way, so even
+            // its slot order may be mixed (the first step after a build rewrites the
+            // ids); the next state upload starts from a fresh slot order.
             WD_CUDA(cudaMemset(s->counters + wd::kCntStageTimeout, 0, sizeof(stalls)));
+            s->slots_invalid = true;
             return fail(WD_ERR_CUDA, "contact kernel: a bulk copy into shared memory did not "
                                      "complete within its wait limit; the state is invalid");
         }
@@ -1429,8 +1433,43 @@ int wd_get_picard_stats(const wd_sim* sim_c, int32_t* iterations, float* residua
     return WD_OK;
 }
 
+// Slots back to grain-id order with each grain's radius, mass and scene (as at
+// creation) and no stored springs, after a step that stopped part-way.
+static int reset_slot_order(wd_sim* s) {
+    const int n = s->n;
+    std::vector<float4> pos(n), vel(n);
+    std::vector<int> ids(n);
+    for (int i = 0; i < n; ++i) {
+        pos[i] = make_float4(0.f, 0.f, 0.f, s->radius[i]);
+        vel[i] = make_float4(0.f, 0.f, 0.f, s->mass[i]);
+        ids[i] = i;
+    }
+    WD_CUDA(cudaStreamSynchronize(s->stream));
+    WD_CUDA(cudaMemcpy(s->posA, pos.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    WD_CUDA(cudaMemcpy(s->velA, vel.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    WD_CUDA(cudaMemcpy(s->idsA, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    WD_CUDA(cudaMemcpy(s->idsB, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (s->scenes > 1) {
+        std::vector<int> sc(n);
+        for (int k = 0; k < s->scenes; ++k)
+            for (int64_t i = s->scene_off[k]; i < s->scene_off[k + 1]; ++i) sc[i] = k;
+        WD_CUDA(cudaMemcpy(s->sceneA, sc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+        WD_CUDA(cudaMemcpy(s->sceneB, sc.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    }
+    if (s->P.history) {
+        WD_CUDA(cudaMemset(s->hcnt_slot, 0, sizeof(int) * n));
+        WD_CUDA(cudaMemset(s->hcnt_g, 0, sizeof(int) * n));
+    }
+    s->slots_invalid = false;
+    return WD_OK;
+}
+
 int wd_set_state_device(wd_sim* sim, const float* d_state) {
     if (!sim || !d_state) return fail(WD_ERR_INVALID, "wd_set_state_device: NULL argument");
+    if (sim->slots_invalid) {
+        const int rc = reset_slot_order(sim);
+        if (rc) return rc;
+    }
     wd::launch_state_from_aos(sim->n, d_state, sim->posA, sim->velA, sim->idsA, sim->stream);
     WD_CUDA(cudaGetLastError());
     WD_CUDA(request_list_build(sim));
