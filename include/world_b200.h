@@ -291,6 +291,12 @@ int wd_autotune(wd_sim* sim, int32_t steps, const char* cache_path, float* skin_
  * autotuner's other choices); results do not depend on them. */
 int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* variant);
 int wd_set_contact_kernel(wd_sim* sim, int32_t block, int32_t variant);
+/* Verlet-list build kernel (no counterpart in the reference): 0 (default) one thread per
+ * grain reading its candidates from global memory; 1 each block of 256 grains stages the
+ * union of its stencil rows in shared memory by bulk copies first (single scenes; the
+ * same lists). Measured on a B200, 2^20-grain collapsed column: 0.185 ms per build with
+ * 0, 0.24 ms with 1. */
+int wd_set_build_kernel(wd_sim* sim, int32_t tiled);
 /* Test hook for the bulk-staged contact kernel's bounded waits (no counterpart in the
  * reference). wait_us: the limit of each wait for a stage of bulk copies (0: one
  * second). stall != 0: each warp's first stage is made to expect 16 bytes that no copy

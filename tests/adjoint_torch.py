@@ -109,12 +109,9 @@ def candidate_pairs(model: TorchModel, x: torch.Tensor) -> tuple[torch.Tensor, t
     return torch.cat(I_all), torch.cat(J_all)
 
 
-def step(model: TorchModel, x, v, sp_keys, sp_xi, mu, e, k, pat=None, slip_from=None):
+def step(model: TorchModel, x, v, sp_keys, sp_xi, mu, e, k, pat=None):
     """One step. sp_keys (sorted) / sp_xi: the springs entering the step. Returns
-    (x', v', keys', springs', pattern); with `pat` the contacts and branches are frozen.
-    slip_from = (sorted keys, springs) that another run of this step produced: a contact
-    slips here when its spring there came out on the Coulomb cap (|k_t xi| within 1e-6
-    of mu |F_n|), so that ties at the cap take that run's branch."""
+    (x', v', keys', springs', pattern); with `pat` the contacts and branches are frozen."""
     n = model.n
     dev = x.device
     r, m = model.radius, model.mass
@@ -189,12 +186,6 @@ def step(model: TorchModel, x, v, sp_keys, sp_xi, mu, e, k, pat=None, slip_from=
     fmag = torch.sqrt((ft * ft).sum(1))
     if pat is None:
         rec["slip"] = fmag > limit
-        if slip_from is not None and slip_from[0].numel():
-            kn, xn_ = slip_from
-            at = torch.searchsorted(kn, keys).clamp(max=kn.numel() - 1)
-            found = kn[at] == keys
-            mag = kt * torch.sqrt((xn_[at] * xn_[at]).sum(1))
-            rec["slip"] = found & (mag >= limit * (1.0 - 1e-6))
     slip = rec["slip"]
     s = torch.where(slip, limit / torch.where(fmag > 0, fmag, torch.ones_like(fmag)),
                     torch.ones_like(fmag))[:, None]
@@ -252,11 +243,10 @@ def cic(x, v, mass, lo, hi, size):
 def adjoint_along(model: TorchModel, traj, springs, theta, loss_of_end):
     """The FP64 adjoint of a window along a given trajectory: traj[t] (n, 6) is the state
     entering step t (t = 0 .. T, traj[T] the end), springs[t] the (sorted keys, springs)
-    entering step t (t = 0 .. T; springs[T], when given, leave the last step). Each
-    step's vector-Jacobian product is evaluated at those states, with that trajectory's
-    stick/slip branches (read from the springs leaving the step) and its own contact
-    decisions there, and chained back from loss_of_end(x_T, v_T). Returns (dL/dv0,
-    dL/dx0, dL/dtheta)."""
+    entering step t (t = 0 .. T - 1; more entries are ignored). Each step's
+    vector-Jacobian product is evaluated at those states, with its own contact and
+    stick/slip decisions there, and chained back from loss_of_end(x_T, v_T). Returns
+    (dL/dv0, dL/dx0, dL/dtheta)."""
     steps = len(traj) - 1
     xT = traj[-1][:, :3].clone().requires_grad_(True)
     vT = traj[-1][:, 3:].clone().requires_grad_(True)
@@ -271,9 +261,7 @@ def adjoint_along(model: TorchModel, traj, springs, theta, loss_of_end):
         keys_t, xi_t = springs[t]
         xi_t = xi_t.clone().requires_grad_(True)
         th = theta.clone().requires_grad_(True)
-        nxt = springs[t + 1] if t + 1 < len(springs) else None
-        x1, v1, keys1, xi1, _ = step(model, x, v, keys_t, xi_t, th[0], th[1], th[2],
-                                     slip_from=nxt)
+        x1, v1, keys1, xi1, _ = step(model, x, v, keys_t, xi_t, th[0], th[1], th[2])
         outs, grads = [x1, v1], [gx, gv]
         if g_xi is not None and xi1.numel() and g_keys.numel():
             at = torch.searchsorted(g_keys, keys1).clamp(max=g_keys.numel() - 1)

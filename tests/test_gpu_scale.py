@@ -11,7 +11,7 @@
 * C1 exactly as benched (2^20 grains, lognormal diameters, springs and history): bit
   for bit against the oracle over 5 steps from rest and over 5 steps from the settled
   column (30,000 steps in), with the grid searched every step and on Verlet lists with
-  the per-lane and the bulk-staged contact kernels.
+  the per-lane and the bulk-staged contact kernels and the shared-memory list build.
 * C2, the 2^24-grain dense box (int64 offsets, 288 x 288 x 144 cells): 2 steps bit for
   bit against the oracle.
 * C3 Set B: the whole 256-scene design batch (9.5 M grains) for 2,000 steps; four
@@ -113,19 +113,22 @@ def test_c0_sets_and_step_match_reference(tmp_path, oracle_for, pre_roll):
 
 # ------------------------------------------------------------------ C1 ------------
 C1_MODES = {
-    "searched": (0.0, None),
-    "lists_per_lane": (0.15, (128, 64)),
-    "lists_bulk_staged": (0.15, (256, 1)),
+    "searched": (0.0, None, False),
+    "lists_per_lane": (0.15, (128, 64), False),
+    "lists_bulk_staged": (0.15, (256, 1), False),
+    "lists_tiled_build": (0.15, (128, 48), True),
 }
 
 
 def _c1_sim(state, radius, mode, springs=None):
     sc = scene_for("collapse_1m_sie_mu05", seed=12345)
-    skin_d, kernel = C1_MODES[mode]
+    skin_d, kernel, tiled = C1_MODES[mode]
     sc.cfg.neighbor_skin = skin_d * 5e-3
     sim = ParticleDynamics(sc.cfg, state=state, radius=radius)
     if kernel:
         sim.set_contact_kernel(*kernel)
+    if tiled:
+        sim.set_build_kernel(True)
     if springs is not None:
         sim.set_history(*springs)
     return sim

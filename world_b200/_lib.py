@@ -81,6 +81,7 @@ SIGNATURES = {
     "wd_list_resort_count": ([_p, _i64], c_int),
     "wd_get_tuning": ([_p, POINTER(c_float), POINTER(c_int32), POINTER(c_int32)], c_int),
     "wd_set_contact_kernel": ([_p, c_int32, c_int32], c_int),
+    "wd_set_build_kernel": ([_p, c_int32], c_int),
     "wd_debug_stage_wait": ([_p, c_int32, c_int32], c_int),
     "wd_set_state_async": ([_p, _p], c_int),
     "wd_get_positions_async": ([_p, _p], c_int),

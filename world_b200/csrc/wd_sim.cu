@@ -151,7 +151,7 @@ struct wd_sim {
     int* nbr_cnt = nullptr;
     float4* xbuild = nullptr;
     uint32_t* list_ctrl = nullptr;
-    bool build_tiled = true;    // list builds stage each block's neighbour window
+    bool build_tiled = false;   // list builds stage each block's neighbour window
     bool slots_invalid = false; // a contact step stopped part-way: slot order to reset
     unsigned long long* list_len = nullptr;
     unsigned* tail_count = nullptr;  // block ticket of the contact kernel's fused decision
@@ -2141,6 +2141,15 @@ int wd_get_tuning(const wd_sim* sim, float* skin, int32_t* block, int32_t* varia
     if (block) *block = sim->force_minb <= 2 ? wd::kBlock : sim->force_block;
     if (variant)
         *variant = sim->force_minb <= 2 ? sim->force_minb : (sim->force_minb == 4 ? 64 : 48);
+    return WD_OK;
+}
+
+int wd_set_build_kernel(wd_sim* sim, int32_t tiled) {
+    if (!sim) return fail(WD_ERR_INVALID, "wd_set_build_kernel: NULL handle");
+    int rc = sync_stream(sim);
+    if (rc) return rc;
+    sim->build_tiled = tiled != 0;
+    sim->graph_dirty = true;
     return WD_OK;
 }
 

@@ -369,6 +369,11 @@ class ParticleDynamics:
         do not depend on them."""
         check(lib.wd_set_contact_kernel(self._h, int(block), int(variant)))
 
+    def set_build_kernel(self, tiled: bool) -> None:
+        """Verlet-list build kernel: per-grain global loads (default) or each block's
+        neighbour window staged in shared memory by bulk copies; the same lists."""
+        check(lib.wd_set_build_kernel(self._h, 1 if tiled else 0))
+
     def picard_counts(self) -> tuple[int, int]:
         """(Picard iterations executed, list-mode steps redone with the per-iteration
         search) so far."""
