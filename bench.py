@@ -350,6 +350,7 @@ def _build_cost(sim, stream, flush, steps: int) -> dict | None:
     if sim.tuning()["neighbor_skin_m"] <= 0:
         return None
     with_b, without = [], []
+    radix0 = sim.radix_search_count()[0]
     for k in range(steps):
         b0 = sim.list_stats()[0]
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -360,9 +361,10 @@ def _build_cost(sim, stream, flush, steps: int) -> dict | None:
             b.record(stream)
         b.synchronize()
         (with_b if sim.list_stats()[0] > b0 else without).append(a.elapsed_time(b))
+    radix = sim.radix_search_count()[0] - radix0
     if not with_b or not without:
-        return {"steps": steps, "builds": len(with_b), "build_ms": None}
-    return {"steps": steps, "builds": len(with_b),
+        return {"steps": steps, "builds": len(with_b), "radix_builds": radix, "build_ms": None}
+    return {"steps": steps, "builds": len(with_b), "radix_builds": radix,
             "step_ms_without_build": statistics.mean(without),
             "build_ms": statistics.mean(with_b) - statistics.mean(without)}
 

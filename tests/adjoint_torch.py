@@ -52,6 +52,14 @@ def model_from_config(cfg, radius, mass, device="cuda") -> TorchModel:
         kt_fixed=float(ph.tangential_stiffness))
 
 
+def model_as(model: TorchModel, dtype) -> TorchModel:
+    """The same model with radius and mass in `dtype`: with float32 states and springs,
+    step() and adjoint_along() then evaluate every step in float32."""
+    return TorchModel(radius=model.radius.to(dtype), mass=model.mass.to(dtype), dt=model.dt,
+                      gravity=model.gravity, wall_lo=model.wall_lo, wall_hi=model.wall_hi,
+                      max_force=model.max_force, kt_fixed=model.kt_fixed)
+
+
 def damping(e, k, m):
     """reference src/compute_rhs_kernel.cu:41-47 for 0 < e < 1."""
     L = torch.log(e)
@@ -254,7 +262,7 @@ def adjoint_along(model: TorchModel, traj, springs, theta, loss_of_end):
     gx = xT.grad if xT.grad is not None else torch.zeros_like(xT)
     gv = vT.grad if vT.grad is not None else torch.zeros_like(vT)
     g_keys, g_xi = None, None
-    g_th = torch.zeros(3, dtype=torch.float64, device=theta.device)
+    g_th = torch.zeros(3, dtype=theta.dtype, device=theta.device)
     for t in reversed(range(steps)):
         x = traj[t][:, :3].clone().requires_grad_(True)
         v = traj[t][:, 3:].clone().requires_grad_(True)

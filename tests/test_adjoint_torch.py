@@ -104,3 +104,26 @@ def test_adjoint_along_a_trajectory_equals_autograd_through_the_window():
     assert sum(int(s[0].numel()) for s in sprs) > 500        # springs carried through
     np.testing.assert_allclose(gv.numpy(), tv.grad.numpy(), rtol=1e-9, atol=1e-12)
     np.testing.assert_allclose(gth.numpy(), tth.grad.numpy(), rtol=1e-9, atol=0)
+
+
+def test_adjoint_along_in_float32_stays_near_float64():
+    """The float32 evaluation of the chain (the C4 test's measure of what FP32 arithmetic
+    does to a window's adjoint) runs in float32 throughout and, on a short window, lands
+    near the float64 one."""
+    cfg, st, rad, mass, model, (mu, e, k), empty = _setup(n=300, seed=13)
+    steps = 15
+    x0 = torch.tensor(st[:, :3], dtype=torch.float64)
+    v0 = torch.tensor(st[:, 3:], dtype=torch.float64)
+    th = torch.tensor([mu, e, k], dtype=torch.float64)
+    rng = np.random.default_rng(3)
+    wx = torch.tensor(rng.normal(size=(model.n, 3)))
+    wv = torch.tensor(rng.normal(size=(model.n, 3)) * 1e-3)
+    traj, sprs = AT.record_trajectory(model, x0, v0, empty, th, steps)
+    loss = lambda x, v: (wx * x.double()).sum() + (wv * v.double()).sum()  # noqa: E731
+    gv, _, gth = AT.adjoint_along(model, traj, sprs, th, loss)
+    m32 = AT.model_as(model, torch.float32)
+    gv32, _, gth32 = AT.adjoint_along(m32, [t.float() for t in traj],
+                                      [(kk, xi.float()) for kk, xi in sprs], th.float(), loss)
+    assert gv32.dtype == torch.float32 and gth32.dtype == torch.float32
+    assert float((gv32.double() - gv).norm() / gv.norm()) < 1e-4
+    np.testing.assert_allclose(gth32.double().numpy(), gth.numpy(), rtol=1e-3)

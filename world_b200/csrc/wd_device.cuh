@@ -151,6 +151,7 @@ struct HistRow {
     int in_count;
     float4* out;        // new row
     int out_count;
+    int cursor = 0;     // where the next search of the old row starts
 };
 
 // Stored spring of `partner` in a row (zero if the contact is new).
@@ -158,6 +159,23 @@ __device__ __forceinline__ float3 find_spring(const float4* row, int count, int 
     for (int k = 0; k < count; ++k) {
         const float4 e = row[k];
         if (__float_as_int(e.w) == partner) return make_float3(e.x, e.y, e.z);
+    }
+    return make_float3(0.f, 0.f, 0.f);
+}
+
+// The same search started at the entry after the last match, wrapping around. A row
+// holds each partner at most once, so the entry found is the one above; the row was
+// written in the order the contacts were visited, and the next step visits the same
+// contacts in the same order, so a lasting contact is found at its first probe.
+__device__ __forceinline__ float3 find_spring(HistRow& h, int partner) {
+    int k = h.cursor;
+    for (int t = 0; t < h.in_count; ++t, ++k) {
+        if (k >= h.in_count) k = 0;
+        const float4 e = h.in[k];
+        if (__float_as_int(e.w) == partner) {
+            h.cursor = k + 1;
+            return make_float3(e.x, e.y, e.z);
+        }
     }
     return make_float3(0.f, 0.f, 0.f);
 }
@@ -190,7 +208,7 @@ __device__ __forceinline__ float3 spring_step(const DevParams& P, float3 vt, flo
 __device__ __forceinline__ void spring_friction(const DevParams& P, float3& f, float3 vt,
                                                 float3 nrm, float limit, int partner,
                                                 HistRow& h, unsigned long long* counters) {
-    float3 xi = find_spring(h.in, h.in_count, partner);
+    float3 xi = find_spring(h, partner);
     const float3 ft = spring_step(P, vt, nrm, limit, xi);
     f.x = f.x + ft.x;
     f.y = f.y + ft.y;
@@ -343,7 +361,7 @@ __device__ __forceinline__ void pair_force(const DevParams& P, float3 d, float n
                                            float dist, float3 vel, float mi, float4 vj,
                                            int partner, float3& f, HistRow& h,
                                            unsigned long long* counters) {
-    float3 xi = HIST ? find_spring(h.in, h.in_count, partner) : make_float3(0.f, 0.f, 0.f);
+    float3 xi = HIST ? find_spring(h, partner) : make_float3(0.f, 0.f, 0.f);
     const PairTerms q = pair_terms<HIST>(P, d, norm, dist, vel, mi, vj, xi);
     pair_accumulate<HIST>(f, q);
     if (HIST) {

@@ -76,6 +76,30 @@ __device__ __forceinline__ double channel_scale(int n, uint32_t bound_bits) {
     return ldexp(1.0, 62 - e);
 }
 
+// Adds up q over each run of adjacent lanes that hold the same key: a segmented inclusive
+// scan by shuffles (one step per doubling of the longest run in the warp), after which the
+// last lane of each run holds the run's total. Returns true on that lane. Grains arrive in
+// cell order, so lanes that deposit on one node are mostly adjacent; a node that comes back
+// later in the warp forms a second run with its own atomic. The values are integers, so the
+// node totals do not depend on how the lanes are grouped.
+__device__ __forceinline__ bool run_totals(long long key, long long (&q)[4]) {
+    const int lane = threadIdx.x & 31;
+    const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+    const bool last = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    if (heads == 0xffffffffu) return true;
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+    const unsigned longest = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(lane - start + 1));
+    for (unsigned d = 1; d < longest; d <<= 1) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const long long t = __shfl_up_sync(0xffffffffu, q[c], d);
+            if (lane - static_cast<int>(d) >= start) q[c] += t;
+        }
+    }
+    return last;
+}
+
 __global__ void __launch_bounds__(kBlock)
 k_deposit(int n, const float4* __restrict__ pos, const float4* __restrict__ vel,
           DepositGeom g, const uint32_t* __restrict__ bounds,
@@ -119,22 +143,9 @@ k_deposit(int n, const float4* __restrict__ pos, const float4* __restrict__ vel,
                     for (int a = 0; a < 3; ++a)
                         q[a + 1] = __double2ll_rn(static_cast<double>(mom[a] * w) * scale[a + 1]);
                 }
-                // combine lanes that hit the same node, then one atomic per node
-                const unsigned peers = __match_any_sync(0xffffffffu, node);
-                const int leader = __ffs(peers) - 1;
-                const int lane = threadIdx.x & 31;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    long long sum = 0;
-                    unsigned rest = peers;
-                    while (rest) {
-                        const int src = __ffs(rest) - 1;
-                        rest &= rest - 1u;
-                        sum += __shfl_sync(peers, q[c], src);
-                    }
-                    q[c] = sum;
-                }
-                if (live && lane == leader) {
+                // combine adjacent lanes that hit the same node, then one atomic per run
+                const bool tail = run_totals(node, q);
+                if (live && tail) {
 #pragma unroll
                     for (int c = 0; c < 4; ++c)
                         if (q[c] != 0)
@@ -217,7 +228,7 @@ k_deposit_batch(int n, const float4* __restrict__ pos, const float4* __restrict_
                 const long long node =
                     live ? (static_cast<long long>(ix[cx]) * Q.dgrid[1] + iy[cy]) * Q.dgrid[2] + iz[cz]
                          : -1ll;
-                // lanes combine only within one scene: key the match on (scene, node)
+                // lanes combine only within one scene: key the runs on (scene, node)
                 const long long key = live ? (static_cast<long long>(sc) << 40) | node : -1ll;
                 long long q[4] = {0, 0, 0, 0};
                 if (live) {
@@ -226,21 +237,9 @@ k_deposit_batch(int n, const float4* __restrict__ pos, const float4* __restrict_
                     for (int k = 0; k < 3; ++k)
                         q[k + 1] = __double2ll_rn(static_cast<double>(mom[k] * w) * scale[k + 1]);
                 }
-                const unsigned peers = __match_any_sync(0xffffffffu, key);
-                const int leader = __ffs(peers) - 1;
-                const int lane = threadIdx.x & 31;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    long long sum = 0;
-                    unsigned rest = peers;
-                    while (rest) {
-                        const int src = __ffs(rest) - 1;
-                        rest &= rest - 1u;
-                        sum += __shfl_sync(peers, q[c], src);
-                    }
-                    q[c] = sum;
-                }
-                if (live && lane == leader) {
+                // combine adjacent lanes that hit the same node, then one atomic per run
+                const bool tail = run_totals(key, q);
+                if (live && tail) {
 #pragma unroll
                     for (int c = 0; c < 4; ++c)
                         if (q[c] != 0)
@@ -397,21 +396,9 @@ k_deposit_aos(int n, const float* __restrict__ state, const float* __restrict__ 
                     for (int a = 0; a < 3; ++a)
                         q[a + 1] = __double2ll_rn(static_cast<double>(mom[a] * w) * scale[a + 1]);
                 }
-                const unsigned peers = __match_any_sync(0xffffffffu, node);
-                const int leader = __ffs(peers) - 1;
-                const int lane = threadIdx.x & 31;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    long long sum = 0;
-                    unsigned rest = peers;
-                    while (rest) {
-                        const int src = __ffs(rest) - 1;
-                        rest &= rest - 1u;
-                        sum += __shfl_sync(peers, q[c], src);
-                    }
-                    q[c] = sum;
-                }
-                if (live && lane == leader) {
+                // combine adjacent lanes that hit the same node, then one atomic per run
+                const bool tail = wd::run_totals(node, q);
+                if (live && tail) {
 #pragma unroll
                     for (int c = 0; c < 4; ++c)
                         if (q[c] != 0)
