@@ -70,6 +70,47 @@ def test_lists_equal_search_in_a_collapsing_column():
     assert lst.list_stats()[0] < 400
 
 
+@pytest.mark.parametrize("axis", [0, 1, 2])
+@pytest.mark.parametrize("skin", [1.5e-3, 2.5e-3])
+def test_lists_hold_pairs_two_cells_apart(axis, skin):
+    """Cells exactly one grain diameter wide (5 mm): two grains in cells two apart along
+    an axis, 5.5 mm between centres, closing at 2 m/s. They are closer than
+    r_i + r_j + skin at the build, meet 25 steps later, long before either has moved
+    0.49 skin, so the lists must hold the pair although the 27-cell stencil does not
+    reach it. The list run must equal the searched one, collision included."""
+    cfg = SimConfig()
+    L = 0.05
+    for ax in "xyz":
+        setattr(cfg.domain, f"{ax}_min", -L)
+        setattr(cfg.domain, f"{ax}_max", L)
+    ph = cfg.physics
+    ph.wall_x_min = ph.wall_y_min = ph.floor_z = -L
+    ph.wall_x_max = ph.wall_y_max = ph.ceiling_z = L
+    ph.gravity = 0.0
+    ph.normal_stiffness = 1e5
+    ph.max_force = 250.0
+    ph.restitution = 0.5
+    ph.friction = 0.5
+    ph.density = 2500.0
+    ph.particle_radius = 2.5e-3
+    cfg.history = True
+    cfg.collision_grid_size_x = cfg.collision_grid_size_y = cfg.collision_grid_size_z = 20
+    cfg.particles_per_cell = 16
+    cfg.dt = 1e-5
+    cfg.density_grid_size_x = cfg.density_grid_size_y = cfg.density_grid_size_z = 8
+    cfg.kernel_timing = False
+    state = np.zeros((2, 6), np.float32)
+    state[:, :3] = 2.5e-3                      # the middle of cell 10 on the other axes
+    state[0, axis], state[1, axis] = -0.3e-3, 5.2e-3   # cells 9 and 11
+    state[0, 3 + axis], state[1, 3 + axis] = 1.0, -1.0
+    radius = np.full(2, 2.5e-3, np.float32)
+    ref, lst = _pair(cfg, state, radius, 100, skin)
+    _same(ref, lst)
+    v = ref.get_state().reshape(-1, 6)
+    assert v[0, 3 + axis] < 0.9 and v[1, 3 + axis] > -0.9     # they did collide
+    assert lst.list_stats()[0] < 100
+
+
 def test_builds_follow_the_displacement_bound():
     """Grains drifting at 0.5 m/s without contacts or gravity: the decision on the
     displacement bound builds every 0.49 skin / (v dt) = 98 steps, as the exact criterion
@@ -219,6 +260,23 @@ def test_every_contact_kernel_variant_is_exact(variant, block):
         b.advance(100)
         sb.append(b)
     _same(*sb)
+
+
+def test_contact_kernel_switches_mid_run():
+    """Switching the list contact kernel between steps (per-lane at 48 and 64
+    registers, cooperative, bulk-staged, and back) leaves the run equal to the searched
+    one."""
+    cfg, st, rad = packed_poly(n=2500, seed=31, mu=0.5)
+    cfg.kernel_timing = False
+    ref = ParticleDynamics(cfg, state=st, radius=rad)
+    c = cfg.copy()
+    c.neighbor_skin = 0.5e-3
+    var = ParticleDynamics(c, state=st, radius=rad)
+    for block, variant in ((128, 48), (256, 0), (128, 64), (256, 1), (256, 0), (128, 48)):
+        var.set_contact_kernel(block, variant)
+        var.advance(40)
+    ref.advance(240)
+    _same(ref, var)
 
 
 def test_bulk_staged_kernel_over_many_tiles():

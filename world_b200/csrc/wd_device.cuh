@@ -38,6 +38,8 @@ struct DevParams {
     int grid[3];               // collision grid
     float inv_len[3];          // 1 / (hi - lo) rounded to float, per axis (cell_axis)
     float cell_err[3];         // (grid + 1) * 2^-20: cell_axis's fast-path margin
+    float cell_len[3];         // cell width (hi - lo) / grid, rounded down
+    float cell_min;            // the smallest of the three
     int ppc;                   // particles_per_cell
     float gravity;
     float max_force;           // clamp (+inf: none)

@@ -98,6 +98,74 @@ __device__ __forceinline__ void list_tail_decide(const ListArgs& A) {
     }
 }
 
+// Grains in cells two apart along an axis are more than a cell width apart, so the 27
+// stencil cells hold every contact; but when 2 r_max + skin exceeds a cell width, a pair
+// two cells apart can be closer than r_i + r_j + skin and meet before the next build.
+// A build then walks the outer shell of the 5 x 5 x 5 block too, cell by cell where its
+// box lies within the grain's reach r_i + r_max + skin (only grains near a face of their
+// cell, so few). Each shell cell is visited in the pass of the first axis along which
+// it lies two cells away; its grains follow the stencil's in the list.
+template <typename Visit>
+__device__ __forceinline__ void list_far_shell(const DevParams& P, const int2* __restrict__ table,
+                                               const float4* __restrict__ pos, float4 pi,
+                                               int cx, int cy, int cz, Visit& visit) {
+    const float reach_max = (pi.w + P.rmax) + P.skin;
+    // the grain's offset in its cell per axis (the fast path's t minus the index) and the
+    // cell mapping's rounding margin, in cells
+    const float f0 = ((pi.x - P.lo[0]) * P.inv_len[0]) * static_cast<float>(P.grid[0]) -
+                     static_cast<float>(cx);
+    const float f1 = ((pi.y - P.lo[1]) * P.inv_len[1]) * static_cast<float>(P.grid[1]) -
+                     static_cast<float>(cy);
+    const float f2 = ((pi.z - P.lo[2]) * P.inv_len[2]) * static_cast<float>(P.grid[2]) -
+                     static_cast<float>(cz);
+    // distance from the grain to the box of cell c + o along axis a, shortened by the
+    // margin (a NaN offset gives 0: every cell in reach)
+    auto gap = [&](int a, int o) {
+        const float f = a == 0 ? f0 : (a == 1 ? f1 : f2);
+        const float g = o == 0 ? 0.f
+                      : o == 1 ? 1.f - f
+                      : o == -1 ? f
+                      : o == 2 ? 2.f - f
+                               : 1.f + f;
+        const float m = 2.f * (a == 0 ? P.cell_err[0] : (a == 1 ? P.cell_err[1] : P.cell_err[2])) + 1e-4f;
+        const float len = a == 0 ? P.cell_len[0] : (a == 1 ? P.cell_len[1] : P.cell_len[2]);
+        return fmaxf(0.f, g - m) * len;
+    };
+    const float r2 = (reach_max * reach_max) * 1.0001f;
+    // a cell two away along two axes is at least sqrt(2) cell widths (less the margins)
+    // away: in reach only for a reach above about 1.4 cells
+    // (an offset f lies in [-err, 1 + err] and the margin is 2 err + 1e-4 cells)
+    const float w = P.cell_min * (1.f - 3.f * fmaxf(P.cell_err[0], fmaxf(P.cell_err[1], P.cell_err[2])) - 1e-4f);
+    const bool two_axes = r2 > 2.f * w * w;
+    for (int a = 0; a < 3; ++a) {
+        // b < c: the other two axes; an axis before a stays within one cell (a is the
+        // first axis at which the cell lies two away)
+        const int b = a == 0 ? 1 : 0, c = a == 2 ? 1 : 2;
+        for (int side = -2; side <= 2; side += 4) {
+            const float ga = gap(a, side);
+            if (ga * ga > r2) continue;
+            const int bl = (b < a || !two_axes) ? -1 : -2;
+            const int cl = (c < a || !two_axes) ? -1 : -2;
+            for (int ob = bl; ob <= -bl; ++ob) {
+                const float gb = gap(b, ob);
+                if (ga * ga + gb * gb > r2) continue;
+                for (int oc = cl; oc <= -cl; ++oc) {
+                    const float gc = gap(c, oc);
+                    if (ga * ga + gb * gb + gc * gc > r2) continue;
+                    const int nx = cx + (a == 0 ? side : ob);
+                    const int ny = cy + (a == 0 ? ob : (a == 1 ? side : oc));
+                    const int nz = cz + (a == 2 ? side : oc);
+                    if (nx < 0 || nx >= P.grid[0] || ny < 0 || ny >= P.grid[1] || nz < 0 ||
+                        nz >= P.grid[2])
+                        continue;
+                    const int2 e = __ldg(&table[P.cell_base + flat_cell(P, nx, ny, nz)]);
+                    for (int j = e.x; j < e.y; ++j) visit(j, __ldg(&pos[j]));
+                }
+            }
+        }
+    }
+}
+
 // The list of every grain, from the run table of the build's sorted state: the
 // contact kernel's stencil walk with the skin added to the contact distance. The sorted
 // state is copied back into the step's buffers on the way.
@@ -159,6 +227,7 @@ k_list_build(DevParams P0, SceneTab T, const float4* __restrict__ pos,
         }
         if (j < e) visit(j, __ldg(&pos[j]));
     }
+    if ((pi.w + P.rmax) + P.skin > P.cell_min) list_far_shell(P, table, pos, pi, cx, cy, cz, visit);
     nbr_cnt[s] = cnt;
     xbuild[s] = pi;
     if (cnt > kNbrCap) atomicOr(&ctrl[kLcOverflow], 1u);
@@ -865,6 +934,12 @@ k_list_build_tiled(DevParams P, const float4* __restrict__ pos, const int2* __re
             }
             if (j < e) visit(j, __ldg(&pos[j]));
         }
+    }
+    if ((pi.w + P.rmax) + P.skin > P.cell_min) {
+        // the outer shell, from global memory (the window holds the stencil only)
+        int cx, cy, cz;
+        cell_coords(P, pi.x, pi.y, pi.z, cx, cy, cz);
+        list_far_shell(P, table, pos, pi, cx, cy, cz, visit);
     }
     nbr_cnt[s] = cnt;
     xbuild[s] = pi;

@@ -380,7 +380,9 @@ DevParams make_params(const wd::Config& c, int n, float dt) {
         const float len = P.hi[a] - P.lo[a];
         P.inv_len[a] = static_cast<float>(1.0 / static_cast<double>(len));
         P.cell_err[a] = static_cast<float>(std::ldexp(static_cast<double>(P.grid[a]) + 1.0, -20));
+        P.cell_len[a] = static_cast<float>(static_cast<double>(len) / P.grid[a] * (1.0 - 1e-6));
     }
+    P.cell_min = std::min(P.cell_len[0], std::min(P.cell_len[1], P.cell_len[2]));
     P.ppc = c.particles_per_cell;
     P.gravity = c.gravity;
     const bool compat_k = !(c.normal_stiffness > 0.f);
