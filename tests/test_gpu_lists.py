@@ -262,6 +262,26 @@ def test_every_contact_kernel_variant_is_exact(variant, block):
     _same(*sb)
 
 
+def test_builds_are_launched_from_the_device():
+    """In a graph-launched list step the build is not a conditional node: the step graph
+    holds the contact kernel and a one-thread kernel that tail-launches the build's
+    device graphs (search head, then the mover or radix path) when the contact kernel
+    decided a build. Builds happen, and the run equals the searched one."""
+    cfg, st, rad = packed_poly(n=2500, seed=32, mu=0.5)
+    cfg.kernel_timing = False
+    ref = ParticleDynamics(cfg, state=st, radius=rad)
+    c = cfg.copy()
+    c.neighbor_skin = 0.3e-3
+    lst = ParticleDynamics(c, state=st, radius=rad)
+    ref.advance(200)
+    lst.advance(200)
+    _same(ref, lst)
+    builds, kernels_each, _ = lst.list_stats()
+    assert lst.kernels_per_step() == 2
+    assert kernels_each == 6
+    assert 2 <= builds < 200
+
+
 def test_contact_kernel_switches_mid_run():
     """Switching the list contact kernel between steps (per-lane at 48 and 64
     registers, cooperative, bulk-staged, and back) leaves the run equal to the searched

@@ -26,10 +26,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-fmad=false",
                      "-Xcompiler", "-fPIC,-O2,-fno-fast-math", "-Xptxas", "-O3",
                      f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
+RDC_SOURCES = {"wd_launch.cu"}
 BIN = os.path.join(HERE, "bin")
 DRIVERS = ["dataset", "chaos"]
 SOURCES = ["wd_search.cu", "wd_contact.cu", "wd_lists.cu", "wd_fields.cu", "wd_ensemble.cu",
-           "wd_adjoint.cu",
+           "wd_adjoint.cu", "wd_launch.cu",
            "wd_sim.cu",
            "wd_config.cpp", "wd_io.cpp"]
 
@@ -48,8 +49,11 @@ def _compile(src: str, extra: list[str]) -> str:
     deps.append(os.path.join(ROOT, "include", "world_b200.h"))
     if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
         return out
-    cmd = [nvcc()] + CUDA_FLAGS + extra + ["-x", "cu" if src.endswith(".cu") else "c++",
-                                           "-c", path, "-o", out]
+    # relocatable device code only where the device runtime is called (the list build's
+    # device-side graph launches); elsewhere it would put the call ABI on every kernel
+    rdc = ["-rdc=true"] if src in RDC_SOURCES else []
+    cmd = [nvcc()] + CUDA_FLAGS + rdc + extra + ["-x", "cu" if src.endswith(".cu") else "c++",
+                                                 "-c", path, "-o", out]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
@@ -63,7 +67,9 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
         objs = list(ex.map(lambda s: _compile(s, extra), SOURCES))
     if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs):
         return LIB
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+    # -rdc=true at the link runs the device link of wd_launch.cu against the device runtime
+    cmd = [nvcc()] + ARCH + ["-rdc=true", "-shared", "-o", LIB] + objs + [
+        "-lcudadevrt", "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed: {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")

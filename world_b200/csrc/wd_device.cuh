@@ -29,6 +29,7 @@ enum Counter : int {
     kCntListExact = 8,      // list steps whose contact kernel read the build positions
     kCntStageTimeout = 9,   // bulk-staged contact kernel: stages that never completed
     kCntListResort = 10,    // list contact kernels: grains whose contacts were re-ordered
+    kCntLaunchFail = 11,    // device-side launches of a list build's graphs that failed
     kNumCounters = 12,
 };
 

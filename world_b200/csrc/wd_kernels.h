@@ -172,6 +172,16 @@ struct ListArgs {
     // last block (threshold on max |x - x_build|, block ticket, the build's IF node)
     float thr; unsigned* tail_count; int use_cond; cudaGraphConditionalHandle cond;
 };
+// Device-side launches of the list build's graphs (wd_launch.cu, the one translation
+// unit built with relocatable device code for the device runtime): one thread
+// tail-launches `graph` when *flag is nonzero (the step's build decision), or `on_zero`
+// / `on_one` by *flag (the search's path). The launched graph runs once the graph that
+// holds the launching kernel has completed; later work of the stream waits for it. A
+// failed launch counts in counters[kCntLaunchFail].
+void launch_graph_if(const uint32_t* flag, cudaGraphExec_t graph, unsigned long long* counters,
+                     cudaStream_t st);
+void launch_graph_pick(const int* flag, cudaGraphExec_t on_zero, cudaGraphExec_t on_one,
+                       unsigned long long* counters, cudaStream_t st);
 void launch_list_decide(uint32_t* list_ctrl, float thr, bool always_exact,
                         unsigned long long* counters,
                         bool use_cond, cudaGraphConditionalHandle cond, cudaStream_t st);

@@ -214,6 +214,13 @@ struct wd_sim {
     std::vector<int32_t> material;
 
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // list mode (semi-implicit Euler): the list build as device-launchable graphs per
+    // step parity -- the search head (keys, mover sort), then the mover path (merge) or
+    // the radix path, each followed by the gather and the listing; the contact kernel
+    // tail-launches the head when it decides a build, the mover kernel the rest
+    cudaGraphExec_t dev_head[2] = {nullptr, nullptr};
+    cudaGraphExec_t dev_mover[2] = {nullptr, nullptr};
+    cudaGraphExec_t dev_radix[2] = {nullptr, nullptr};
     bool graph_dirty = true;
     int kernels_per_step = 0;
 
@@ -236,6 +243,12 @@ void destroy_graphs(wd_sim* s) {
     for (auto& g : s->graph) {
         if (g) cudaGraphExecDestroy(g);
         g = nullptr;
+    }
+    for (cudaGraphExec_t* set : {s->dev_head, s->dev_mover, s->dev_radix}) {
+        for (int q = 0; q < 2; ++q) {
+            if (set[q]) cudaGraphExecDestroy(set[q]);
+            set[q] = nullptr;
+        }
     }
     s->graph_dirty = true;
 }
@@ -542,11 +555,18 @@ cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
 // neighbors of the sorted state, copy it back to A. `gate` skips it all when the
 // step's decision says no build (direct launches); in a graph it is the body of an
 // IF node and runs ungated.
+void enqueue_list_build_tail(wd_sim* s, wd::Skip gate, cudaStream_t st);
+
 void enqueue_list_build(wd_sim* s, wd::Skip gate, cudaStream_t st) {
+    wd::launch_search(s->P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, gate, nullptr, 0,
+                      s->counters, st);
+    enqueue_list_build_tail(s, gate, st);
+}
+
+// The build after the search: gather into the new order, list, copy back.
+void enqueue_list_build_tail(wd_sim* s, wd::Skip gate, cudaStream_t st) {
     const DevParams& P = s->P;
     const bool hist = P.history != 0, batch = s->scenes > 1;
-    wd::launch_search(P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, gate, nullptr, 0,
-                      s->counters, st);
     wd::launch_gather(P, s->sb, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr, nullptr,
                       nullptr, nullptr, false, hist ? s->hcnt_slot : nullptr,
                       hist ? s->hcnt_g : nullptr, batch ? s->sceneA : nullptr,
@@ -722,20 +742,103 @@ cudaError_t enqueue_step_list_picard(wd_sim* s, int parity, cudaStream_t st, boo
 }
 
 // One list-mode step: decide, build if needed, contacts + integration from A into B.
+// The buffers a list step's build works on: the step's new state (B) as the build's
+// input (A), gathered through the C buffers; the step's input (A, the rhs getter's
+// velocities and ids) stays as it is. Restored when the view ends.
+struct BuildView {
+    wd_sim* s;
+    float4 *pa, *pb, *va, *vb;
+    int *ia, *ib, *ha, *hb, *sa, *sbn;
+    explicit BuildView(wd_sim* w)
+        : s(w), pa(w->posA), pb(w->posB), va(w->velA), vb(w->velB), ia(w->idsA), ib(w->idsB),
+          ha(w->hcnt_slot), hb(w->hcnt_g), sa(w->sceneA), sbn(w->sceneB) {
+        s->posA = pb; s->velA = vb; s->idsA = ib; s->hcnt_slot = hb; s->sceneA = sbn;
+        s->posB = s->posC; s->velB = s->velC; s->idsB = s->idsC; s->hcnt_g = ha;
+        s->sceneB = s->sceneC;
+    }
+    ~BuildView() {
+        s->posA = pa; s->posB = pb; s->velA = va; s->velB = vb; s->idsA = ia; s->idsB = ib;
+        s->hcnt_slot = ha; s->hcnt_g = hb; s->sceneA = sa; s->sceneB = sbn;
+    }
+};
+
+// One device-launchable graph: what `body` enqueues, captured on the auxiliary stream,
+// instantiated for device launch and uploaded.
+template <class Body>
+cudaError_t capture_device_graph(wd_sim* s, cudaGraphExec_t* out, Body body) {
+    *out = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s->aux_stream, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return e;
+    body(s->aux_stream);
+    const cudaError_t be = cudaGetLastError();
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(s->aux_stream, &g);
+    if (be != cudaSuccess || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return be != cudaSuccess ? be : e;
+    }
+    e = cudaGraphInstantiate(out, g, cudaGraphInstantiateFlagDeviceLaunch);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return e;
+    }
+    return cudaGraphUpload(*out, s->aux_stream);
+}
+
+// The list build of the step graph of parity q as device graphs (see dev_head), on the
+// buffers that graph's build sees. On failure none is kept and the step graph holds
+// the build in a conditional node instead.
+cudaError_t capture_device_builds(wd_sim* s, int q) {
+    const DevParams& P = s->P;
+    const wd::Skip none{nullptr, 0.f};
+    BuildView view(s);
+    cudaError_t e = capture_device_graph(s, &s->dev_mover[q], [&](cudaStream_t st) {
+        wd::launch_search_merge(P, s->idsA, s->sb, none, st);
+        enqueue_list_build_tail(s, none, st);
+    });
+    if (e == cudaSuccess)
+        e = capture_device_graph(s, &s->dev_radix[q], [&](cudaStream_t st) {
+            wd::launch_search_radix(P, s->idsA, s->sb, none, st);
+            enqueue_list_build_tail(s, none, st);
+        });
+    if (e == cudaSuccess)
+        e = capture_device_graph(s, &s->dev_head[q], [&](cudaStream_t st) {
+            wd::launch_search_head(P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, none, nullptr,
+                                   0, false, 0, s->counters, st);
+            // the path the mover kernel picked (ctrl[1]: the radix sort)
+            wd::launch_graph_pick(s->sb.ctrl + 1, s->dev_mover[q], s->dev_radix[q], s->counters,
+                                  st);
+        });
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->aux_stream);
+    if (e != cudaSuccess) {
+        for (cudaGraphExec_t* x : {&s->dev_head[q], &s->dev_mover[q], &s->dev_radix[q]}) {
+            if (*x) cudaGraphExecDestroy(*x);
+            *x = nullptr;
+        }
+        cudaGetLastError();
+    }
+    return e;
+}
+
+// One list-mode step: decide, build if needed, contacts + integration from A into B.
 cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool capture,
                               cudaEvent_t mid = nullptr) {
     if (s->picard) return enqueue_step_list_picard(s, parity, st, capture, mid);
     const DevParams& P = s->P;
     const bool hist = P.history != 0, batch = s->scenes > 1;
+    // in a graph, the build is either tail-launched from the device (its graphs exist)
+    // or an IF node that the contact kernel switches
+    const bool device_build = capture && s->dev_head[parity] != nullptr;
     cudaGraphConditionalHandle cond = 0;
-    if (capture) {
+    if (capture && !device_build) {
         const cudaError_t e = capture_cond(st, &cond);
         if (e != cudaSuccess) return e;
     }
     wd::ListArgs a{};
     a.thr = wd::kListValid * P.skin;
     a.tail_count = s->tail_count;
-    a.use_cond = capture ? 1 : 0;
+    a.use_cond = capture && !device_build ? 1 : 0;
     a.cond = cond;
     a.pos = s->posA; a.vel = s->velA; a.ids = s->idsA; a.table = s->sb.table;
     a.pos_out = s->posB; a.vel_out = s->velB; a.ids_out = s->idsB; a.acc_out = s->acc;
@@ -750,20 +853,18 @@ cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool captu
     a.scene_out = s->sceneB;
     wd::launch_force_list(P, a, st, s->force_block, s->force_minb);
     if (mid) cudaEventRecord(mid, st);
-    // the build the kernel's last block decided on, of the new state in B, gathered
-    // through the C buffers: the step's input (A, the rhs getter's velocities and ids)
-    // stays as it is
-    float4 *pa = s->posA, *pb = s->posB, *va = s->velA, *vb = s->velB;
-    int *ia = s->idsA, *ib = s->idsB, *ha = s->hcnt_slot, *hb = s->hcnt_g;
-    int *sa = s->sceneA, *sbn = s->sceneB;
-    s->posA = pb; s->velA = vb; s->idsA = ib; s->hcnt_slot = hb; s->sceneA = sbn;
-    s->posB = s->posC; s->velB = s->velC; s->idsB = s->idsC; s->hcnt_g = ha;
-    s->sceneB = s->sceneC;
+    if (device_build) {
+        // the build the kernel's last block decided on (kLcDecision), from the device
+        wd::launch_graph_if(s->list_ctrl + wd::kLcDecision, s->dev_head[parity], s->counters, st);
+        return cudaGetLastError();
+    }
+    // the build the kernel's last block decided on, of the new state in B
     cudaError_t e = cudaSuccess;
-    if (capture) e = capture_if_build(s, st, cond);
-    else enqueue_list_build(s, wd::Skip{s->list_ctrl + wd::kLcDecision, 0.5f}, st);
-    s->posA = pa; s->posB = pb; s->velA = va; s->velB = vb; s->idsA = ia; s->idsB = ib;
-    s->hcnt_slot = ha; s->hcnt_g = hb; s->sceneA = sa; s->sceneB = sbn;
+    {
+        BuildView view(s);
+        if (capture) e = capture_if_build(s, st, cond);
+        else enqueue_list_build(s, wd::Skip{s->list_ctrl + wd::kLcDecision, 0.5f}, st);
+    }
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -792,6 +893,9 @@ int build_graphs(wd_sim* s) {
         // list mode: capture the graph of parity q with the buffers it will see
         const bool swapped = s->lists && s->lpar != parity;
         if (swapped) swap_state(s);
+        // semi-implicit Euler on lists: the build as device-launched graphs (kept only
+        // when they instantiate; otherwise the step graph holds an IF node)
+        if (s->lists && !s->picard) capture_device_builds(s, parity);
         WD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         const cudaError_t ce = enqueue_any_step(s, parity, s->stream, true);
         const cudaError_t ee = cudaStreamEndCapture(s->stream, &g);
@@ -891,6 +995,18 @@ int ondemand_search(wd_sim* s) {
 int sync_stream(wd_sim* s) {
     WD_CUDA(cudaStreamSynchronize(s->stream));
     WD_CUDA(cudaGetLastError());
+    if (s->lists && !s->picard) {
+        // a list build whose device-side graph launch failed did not run
+        unsigned long long failed = 0;
+        WD_CUDA(cudaMemcpy(&failed, s->counters + wd::kCntLaunchFail, sizeof(failed),
+                           cudaMemcpyDeviceToHost));
+        if (failed) {
+            WD_CUDA(cudaMemset(s->counters + wd::kCntLaunchFail, 0, sizeof(failed)));
+            WD_CUDA(request_list_build(s));
+            return fail(WD_ERR_CUDA, "list build: a device-side graph launch failed; the "
+                                     "steps since the last synchronisation are invalid");
+        }
+    }
     if (s->lists && (s->force_minb == 1 || s->force_minb == 2)) {
         // the bulk-staged contact kernel flags stages that never arrived (bounded waits)
         unsigned long long stalls = 0;
@@ -2016,8 +2132,13 @@ int wd_list_exact_count(wd_sim* sim, int64_t* steps) {
 
 int wd_list_stats(wd_sim* sim, int64_t* builds, int32_t* kernels_each, double* mean_length) {
     if (!sim) return fail(WD_ERR_INVALID, "wd_list_stats: NULL handle");
-    if (kernels_each)
-        *kernels_each = sim->lists ? 2 + (1 + 3 * sim->sb.passes) + 1 + 2 : 0;
+    if (kernels_each) {
+        // device-launched builds: the head (keys, mover sort, path pick) and the mover
+        // path (merge, gather, listing); in a conditional node or direct launches: every
+        // search kernel (the radix ones return at once when idle), gather and listing
+        const bool device = sim->dev_head[0] != nullptr || sim->dev_head[1] != nullptr;
+        *kernels_each = !sim->lists ? 0 : device ? 6 : 2 + (1 + 3 * sim->sb.passes) + 1 + 2;
+    }
     if (builds) {
         int rc = read_counter(sim, wd::kCntListBuilds, builds);
         if (rc) return rc;
