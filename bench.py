@@ -107,7 +107,7 @@ def parse_args():
     ap.add_argument("--direct", action="store_true",
                     help="launch each step's kernels directly instead of as one CUDA graph "
                          "(for per-kernel profilers, which cannot see inside graphs with "
-                         "conditional nodes)")
+                         "conditional nodes or device-launched graphs)")
     return ap.parse_args()
 
 

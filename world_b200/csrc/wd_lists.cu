@@ -34,8 +34,8 @@ __device__ __forceinline__ bool skipped(const Skip& s) {
     return s.prev_res != nullptr && s.tol > 0.f && __uint_as_float(*s.prev_res) < s.tol;
 }
 
-// One thread: decide whether this step builds and switch the build's conditional node
-// (graph mode). The decision needs a bound B on max |x - x_build| of the current state:
+// One thread: decide whether this step builds (the decision word, kLcDecision) and
+// switch the build's conditional node where the graph holds one. The decision needs a bound B on max |x - x_build| of the current state:
 // the exact maximum when the last contact kernel measured it (it then read the build
 // positions), otherwise the previous bound plus the largest displacement of the last
 // step (triangle inequality), so that most steps read no build positions. The measured
@@ -81,7 +81,9 @@ __global__ void k_list_decide(uint32_t* __restrict__ ctrl, float thr, int always
 
 // The decision fused into the tail of a semi-implicit Euler list kernel: the last block
 // to finish (every block's displacement atomics done) decides whether the lists are
-// rebuilt before the next step and switches the build's conditional node. All threads
+// rebuilt before the next step: it switches the build's conditional node where the step
+// graph holds one, or leaves the decision word to the kernel that launches the build's
+// graphs from the device (wd_launch.cu). All threads
 // of every block call it. The barrier orders the block's atomics before thread 0's
 // fence and ticket (the grid-barrier pattern: one fence per block, not per thread).
 __device__ __forceinline__ void list_tail_decide(const ListArgs& A) {
