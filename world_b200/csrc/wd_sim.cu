@@ -1986,11 +1986,16 @@ int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
     if (!sim || !kernels) return fail(WD_ERR_INVALID, "wd_kernels_per_step: NULL argument");
     // keys, mover kernel, merge, gather, contact per search; a search that takes the
     // radix path adds 1 + 3 per pass (wd_radix_search_count)
-    // list mode: the contact kernel (its last block decides the next build); builds add
+    // list mode: the contact kernel (its last block decides the next build) and, in graph
+    // mode, the kernel that launches a decided build from the device; builds add
     // wd_list_stats' count (Picard: the decision, the iterations, the last iterate's
     // copy, the redo check)
-    *kernels = sim->lists ? (sim->picard ? sim->picard_iters + 3 : 1)
-                          : static_cast<int64_t>(5) * sim->picard_iters;
+    if (sim->lists && !sim->picard) {
+        const bool device = sim->dev_head[0] != nullptr || sim->dev_head[1] != nullptr;
+        *kernels = device ? 2 : 1;
+    } else {
+        *kernels = sim->lists ? sim->picard_iters + 3 : static_cast<int64_t>(5) * sim->picard_iters;
+    }
     return WD_OK;
 }
 
