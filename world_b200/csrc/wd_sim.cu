@@ -221,6 +221,12 @@ struct wd_sim {
     cudaGraphExec_t dev_head[2] = {nullptr, nullptr};
     cudaGraphExec_t dev_mover[2] = {nullptr, nullptr};
     cudaGraphExec_t dev_radix[2] = {nullptr, nullptr};
+    // searched semi-implicit Euler steps: the step graph holds the search head (keys,
+    // mover sort) and a kernel that tail-launches the rest of the step as one of two
+    // device-launchable graphs: the mover path (merge) or the radix path, each followed
+    // by the gather and the contact kernel
+    cudaGraphExec_t dev_step_mover[2] = {nullptr, nullptr};
+    cudaGraphExec_t dev_step_radix[2] = {nullptr, nullptr};
     bool graph_dirty = true;
     int kernels_per_step = 0;
 
@@ -244,7 +250,8 @@ void destroy_graphs(wd_sim* s) {
         if (g) cudaGraphExecDestroy(g);
         g = nullptr;
     }
-    for (cudaGraphExec_t* set : {s->dev_head, s->dev_mover, s->dev_radix}) {
+    for (cudaGraphExec_t* set : {s->dev_head, s->dev_mover, s->dev_radix, s->dev_step_mover,
+                                 s->dev_step_radix}) {
         for (int q = 0; q < 2; ++q) {
             if (set[q]) cudaGraphExecDestroy(set[q]);
             set[q] = nullptr;
@@ -500,6 +507,39 @@ cudaError_t enqueue_search(wd_sim* s, wd::Skip skip, uint32_t* zero_res, int zer
 // travel with the state in slot order (committed in hcnt_slot, gathered into hcnt_g,
 // or for Picard into the permuted step-start snapshots hcnt_snap). `mid`, when given,
 // is recorded between the search and the contact kernel (semi-implicit Euler only).
+// The arguments of a searched step's contact kernel (state B -> A).
+wd::ForceArgs step_force_args(wd_sim* s, int parity) {
+    const bool batch = s->scenes > 1;
+    wd::ForceArgs fa{};
+    fa.pos = s->posB; fa.vel = s->velB; fa.ids = s->idsB; fa.table = s->sb.table;
+    fa.pos_out = s->posA; fa.vel_out = s->velA; fa.ids_out = s->idsA; fa.acc_out = s->acc;
+    fa.hist_in = s->hist[parity];
+    fa.hist_out = s->hist[parity ^ 1];
+    fa.hcnt_out = s->hcnt_slot;
+    fa.counters = s->counters;
+    fa.scene_params = batch ? s->d_scene_P : nullptr;
+    fa.scene = s->sceneB;
+    fa.scene_out = s->sceneA;
+    return fa;
+}
+
+// A searched semi-implicit Euler step after its search: gather into the new order (B),
+// then the contact kernel (B -> A).
+void enqueue_step_tail(wd_sim* s, int parity, cudaStream_t st, cudaEvent_t mid) {
+    const DevParams& P = s->P;
+    const bool hist = P.history != 0, batch = s->scenes > 1;
+    const wd::Skip none{nullptr, 0.f};
+    wd::launch_gather(P, s->sb, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr, nullptr,
+                      nullptr, nullptr, false, hist ? s->hcnt_slot : nullptr,
+                      hist ? s->hcnt_g : nullptr, batch ? s->sceneA : nullptr,
+                      batch ? s->sceneB : nullptr, true, s->counters, s->scene_overflow,
+                      s->d_scene_P, none, st);
+    if (mid) cudaEventRecord(mid, st);
+    wd::ForceArgs fa = step_force_args(s, parity);
+    fa.hcnt_in = s->hcnt_g;
+    wd::launch_force(P, fa, false, none, st, s->force_block);
+}
+
 cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
                          cudaEvent_t mid = nullptr) {
     const DevParams& P = s->P;
@@ -517,15 +557,17 @@ cudaError_t enqueue_step(wd_sim* s, int parity, cudaStream_t st, bool capture,
     fa.scene_out = s->sceneA;
     const wd::Skip none{nullptr, 0.f};
     if (!s->picard) {
+        if (capture && s->dev_step_mover[parity] != nullptr) {
+            // the search head here, the rest of the step tail-launched from the device
+            wd::launch_search_head(P, tab(s, s->sceneA), s->posA, s->idsA, s->sb, none, nullptr,
+                                   0, false, 0, s->counters, st);
+            wd::launch_graph_pick(s->sb.ctrl + 1, s->dev_step_mover[parity],
+                                  s->dev_step_radix[parity], s->counters, st);
+            return cudaGetLastError();
+        }
         cudaError_t e = enqueue_search(s, none, nullptr, 0, capture, st);
         if (e != cudaSuccess) return e;
-        wd::launch_gather(P, s->sb, s->posA, s->velA, s->posB, s->velB, s->idsB, nullptr, nullptr,
-                          nullptr, nullptr, false, hist ? s->hcnt_slot : nullptr,
-                          hist ? s->hcnt_g : nullptr, batch ? s->sceneA : nullptr,
-                          batch ? s->sceneB : nullptr, true, s->counters, s->scene_overflow, s->d_scene_P, none, st);
-        if (mid) cudaEventRecord(mid, st);
-        fa.hcnt_in = s->hcnt_g;
-        wd::launch_force(P, fa, false, none, st, s->force_block);
+        enqueue_step_tail(s, parity, st, mid);
         return cudaGetLastError();
     }
     for (int k = 0; k < s->picard_iters; ++k) {
@@ -821,6 +863,31 @@ cudaError_t capture_device_builds(wd_sim* s, int q) {
     return e;
 }
 
+// The rest of a searched step of parity q as device graphs (see dev_step_mover). On
+// failure none is kept and the step graph holds the radix path in a conditional node.
+cudaError_t capture_device_search_steps(wd_sim* s, int q) {
+    const DevParams& P = s->P;
+    const wd::Skip none{nullptr, 0.f};
+    cudaError_t e = capture_device_graph(s, &s->dev_step_mover[q], [&](cudaStream_t st) {
+        wd::launch_search_merge(P, s->idsA, s->sb, none, st);
+        enqueue_step_tail(s, q, st, nullptr);
+    });
+    if (e == cudaSuccess)
+        e = capture_device_graph(s, &s->dev_step_radix[q], [&](cudaStream_t st) {
+            wd::launch_search_radix(P, s->idsA, s->sb, none, st);
+            enqueue_step_tail(s, q, st, nullptr);
+        });
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->aux_stream);
+    if (e != cudaSuccess) {
+        for (cudaGraphExec_t* x : {&s->dev_step_mover[q], &s->dev_step_radix[q]}) {
+            if (*x) cudaGraphExecDestroy(*x);
+            *x = nullptr;
+        }
+        cudaGetLastError();
+    }
+    return e;
+}
+
 // One list-mode step: decide, build if needed, contacts + integration from A into B.
 cudaError_t enqueue_step_list(wd_sim* s, int parity, cudaStream_t st, bool capture,
                               cudaEvent_t mid = nullptr) {
@@ -896,6 +963,7 @@ int build_graphs(wd_sim* s) {
         // semi-implicit Euler on lists: the build as device-launched graphs (kept only
         // when they instantiate; otherwise the step graph holds an IF node)
         if (s->lists && !s->picard) capture_device_builds(s, parity);
+        if (!s->lists && !s->picard) capture_device_search_steps(s, parity);
         WD_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         const cudaError_t ce = enqueue_any_step(s, parity, s->stream, true);
         const cudaError_t ee = cudaStreamEndCapture(s->stream, &g);
@@ -1993,6 +2061,10 @@ int wd_kernels_per_step(const wd_sim* sim_c, int64_t* kernels) {
     if (sim->lists && !sim->picard) {
         const bool device = sim->dev_head[0] != nullptr || sim->dev_head[1] != nullptr;
         *kernels = device ? 2 : 1;
+    } else if (!sim->lists && !sim->picard) {
+        // the searched step: with its tail launched from the device, the path-pick kernel
+        const bool device = sim->dev_step_mover[0] != nullptr || sim->dev_step_mover[1] != nullptr;
+        *kernels = device ? 6 : 5;
     } else {
         *kernels = sim->lists ? sim->picard_iters + 3 : static_cast<int64_t>(5) * sim->picard_iters;
     }
