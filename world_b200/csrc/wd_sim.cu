@@ -245,6 +245,8 @@ void clear_adj_graphs(wd_sim* s) {
 }
 
 void destroy_graphs(wd_sim* s) {
+    // steps still in flight may yet tail-launch the device graphs: let them finish first
+    if (s->stream) cudaStreamSynchronize(s->stream);
     clear_adj_graphs(s);
     for (auto& g : s->graph) {
         if (g) cudaGraphExecDestroy(g);
