@@ -28,7 +28,8 @@ cpu_baseline -- the oracle port (C, OpenMP on all host cores) on a bounded sampl
           of the same workload, rank 0 at N = 1 only.
 settled / batched / adjoint -- (N = 1, default workload) the same metric in the
           contact-bearing regime (the same column after 30,000 steps, when it has
-          collapsed onto the floor), for the two batched ensembles, and the reverse
+          collapsed onto the floor), for the two batched ensembles (from rest, and
+          after the same 30,000 steps beside the settled column), and the reverse
           pass's cost, each beside the plain step measured above on the same GPU.
 
 --impl reference: the reference's step has no CPU implementation (it is CUDA only),
@@ -503,9 +504,12 @@ def _settled(sim, scene, stream, flush, args, plain_value: float, done: int,
             "autotuned": tuned}
 
 
-def _batched(workload: str, args, flush, plain_value: float) -> dict:
+def _batched(workload: str, args, flush, plain_value: float,
+             settled_plain: float | None = None) -> dict:
     """One batched ensemble on this GPU: every scene in one SceneBatch, the autotuner's
-    schedule, K timed steps with the L2 flushed before each."""
+    schedule, K timed steps with the L2 flushed before each; then the same batch once
+    its columns have collapsed (`settled_steps` steps from rest, re-tuned), K timed steps
+    against the plain column's settled value."""
     import torch
     from world_b200 import SceneBatch
     from world_b200.scenes import ensemble_for
@@ -523,6 +527,20 @@ def _batched(workload: str, args, flush, plain_value: float) -> dict:
            "ms_per_step": ms / args.steps, "steps": args.steps, "over_plain": value / plain_value,
            "setup_seconds": setup_s, "schedule": batch.tuning(),
            "mean_list_length": batch.list_stats()[2]}
+    if settled_plain:
+        t0 = time.perf_counter()
+        batch.advance(max(0, args.settled_steps - args.warmup - args.steps))
+        batch.synchronize()
+        preroll_s = time.perf_counter() - t0
+        if args.skin < 0:
+            batch.autotune(steps=20)
+        batch.advance(args.warmup)
+        ms = _timed_steps(batch, stream, flush, args.steps)
+        v = batch.n * args.steps / (ms / 1e3)
+        out["settled"] = {"value": v, "ms_per_step": ms / args.steps,
+                          "after_steps": args.settled_steps, "pre_roll_seconds": preroll_s,
+                          "over_plain_settled": v / settled_plain, "schedule": batch.tuning(),
+                          "mean_list_length": batch.list_stats()[2]}
     batch.close()
     return out
 
@@ -684,7 +702,8 @@ def run_ours(args) -> int:
         settled = _settled(sim, scene, stream, flush, args, value, done, args.settled_steps)
     sim.close()
     if extras and not args.settled_only:
-        batched = {w: _batched(w, args, flush, value) for w in BATCHED_WORKLOADS}
+        batched = {w: _batched(w, args, flush, value, settled["value"] if settled else None)
+                   for w in BATCHED_WORKLOADS}
         adjoint = adjoint_measure(args, plain_value=value)
 
     cpu = None

@@ -292,6 +292,12 @@ __device__ __forceinline__ void list_disp_report(uint32_t* ctrl, bool exact, uin
     }
 }
 
+// Asks L1 for the line holding p; nothing is read into registers, so a later __ldg of
+// p finds it on chip without holding registers in between.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // The contacts of a grain whose list entries a cell crossing re-ordered, in canonical
 // order: each pass takes the smallest visiting key above the last. (Inlined: an
 // out-of-line call copies the parameter structs to local memory at kernel entry, which
@@ -406,7 +412,7 @@ __device__ __forceinline__ void list_contacts_table(const DevParams& P, const Li
 // (warp-uniform). order_out: write the slot's id (and scene) too. Between builds
 // the slot order is fixed and the ids of both state buffers agree, so only the first
 // step after a build (whose gather reordered one buffer) and Picard write them.
-template <bool HIST, bool BATCH, bool PICARD>
+template <bool HIST, bool BATCH, bool PICARD, bool PREFETCH = false>
 __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& A, int s, int n,
                                            int scene, float4 pi, float4 vi, int id, int cnt,
                                            float4 xb, int hcnt_in, bool exact, bool order_out,
@@ -442,6 +448,8 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
             h.in_count = hcnt_in;
             h.out = A.hist_out + static_cast<int64_t>(id) * kHistCap;
             h.out_count = 0;
+            // the first stored spring is probed first: on its way while the list is scanned
+            if (PREFETCH && hcnt_in > 0) prefetch_l1(h.in);
         }
         wall_forces<HIST>(P, pos, vel, ri, mi, f, h, A.counters);
         // the list contacts, skipped as a whole by warps in which no grain has a list
@@ -473,6 +481,11 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
                         const bool hit = e0 + u < cnt && !(ns > cut) &&
                                          pair_dist(sqrtf(ns), ri, pp[u].w) < 0.f;
                         hits |= hit ? (1ull << (e0 + u)) : 0ull;
+                        // the contact's partner id and velocity are read after the scan
+                        if (PREFETCH && hit) {
+                            prefetch_l1(&A.ids[jj[u]]);
+                            prefetch_l1(&A.vel[jj[u]]);
+                        }
                     }
                 }
                 // the contacts, in list order, while they arrive in canonical order (the
@@ -543,7 +556,10 @@ __device__ __forceinline__ void list_grain(const DevParams& P0, const ListArgs& 
 }
 
 // MINB resident blocks per SM: 5 caps registers at 48 (more warps, a few spills), 4 at
-// 64 (no spills); the autotuner picks.
+// 64 (no spills); the autotuner picks. The 64-register form also prefetches, into L1,
+// each contact's partner id and velocity when the scan finds it, and the grain's first
+// stored spring (measured: 2% on a settled column; at 48 registers the prefetches'
+// addresses added spills and cost more than they saved).
 // PICARD: one backward-Euler / Picard iteration (src/backward_euler_picard_kernel.cu:4-17):
 // forces at the iterate (pos, vel), integration from the step-start state (xn, vn), the
 // residual max |x_{k+1} - x_k|; an iterate that has left the lists' validity bound marks
@@ -581,9 +597,9 @@ k_force_list(DevParams P0, ListArgs A) {
         }
         const bool warp_listed = __any_sync(0xffffffffu, cnt != 0);
         if (live)
-            list_grain<HIST, BATCH, PICARD>(P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in,
-                                            exact, order_out, warp_listed, disp_bits, step_bits,
-                                            res_bits, viol);
+            list_grain<HIST, BATCH, PICARD, MINB == 4 && !PICARD>(
+                P0, A, s, n, scene, pi, vi, id, cnt, xb, hcnt_in, exact, order_out, warp_listed,
+                disp_bits, step_bits, res_bits, viol);
     }
     list_disp_report<PICARD>(A.list_ctrl, exact, disp_bits, step_bits);
     if (!PICARD) list_tail_decide(A);
